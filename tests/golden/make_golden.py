@@ -1,0 +1,294 @@
+"""Generate golden vectors by running the reference's own 1D solvers in FP64.
+
+Run from the repository root in a container where the reference tree is
+mounted (default ``/root/reference``; override with ``INC_REFERENCE``):
+
+    python tests/golden/make_golden.py
+
+It imports ``solvers/solver_1d.py`` from the reference (never copied), runs it
+with ``torch.set_default_dtype(torch.float64)`` on seeded inputs, and writes
+``tests/golden/*.npz``.  The files are small and committed: the GPU test box
+has no reference tree.
+
+The only change to the reference's behaviour is the Burgers ``step`` arity
+fix: the shipped ``step`` calls ``u, source = self._apply_corrections(u, source)``
+(solver_1d.py:188) against a one-argument ``_apply_corrections`` (solver_1d.py:116)
+and raises ``TypeError``.  ``_FixedBurgers`` below builds the step from the
+reference's own methods with ``source = self._apply_corrections(source)``.
+SSP-RK3 is composed from the same methods (the reference only has Euler).
+"""
+from __future__ import annotations
+
+import math
+import os
+import sys
+from types import SimpleNamespace
+
+import numpy as np
+import torch
+
+REF = os.environ.get("INC_REFERENCE", "/root/reference")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+
+def _import_reference():
+    if REF not in sys.path:
+        sys.path.insert(0, REF)
+    from solvers.solver_1d import BurgersSolverTorch, KSSolverTorch, weno_reconstruction
+    return BurgersSolverTorch, KSSolverTorch, weno_reconstruction
+
+
+BurgersSolverTorch, KSSolverTorch, weno_reconstruction = _import_reference()
+
+
+class _FixedBurgers(BurgersSolverTorch):
+    """Reference solver with the ``_apply_corrections`` call fixed."""
+
+    def rhs_at(self, u, t):
+        saved = self.t
+        self.t = t
+        source = self._compute_source(u)
+        self.t = saved
+        source = self._apply_corrections(source)
+        return self.calc_nonlinear(u) + self.calc_linear(u) + source
+
+    def step(self, u):
+        if self.adaptive_CFL is not None:
+            return self.step_adaptive(u)
+        u_new = u + self.dt * self.rhs_at(u, self.t)
+        self.t += self.dt
+        return u_new
+
+    def step_rk3(self, u):
+        dt, t = self.dt, self.t
+        u1 = u + dt * self.rhs_at(u, t)
+        u2 = 0.75 * u + 0.25 * (u1 + dt * self.rhs_at(u1, t + dt))
+        u3 = (1.0 / 3.0) * u + (2.0 / 3.0) * (u2 + dt * self.rhs_at(u2, t + 0.5 * dt))
+        self.t = t + dt
+        return u3
+
+    def step_adaptive(self, u):
+        target, substeps = self.dt, 0
+        while target > 0:
+            max_u = torch.max(torch.abs(u))
+            allowed = self.adaptive_CFL * self.dx / max_u.item() if max_u.item() > 0 else target
+            dt_local = min(target, allowed)
+            u = u + dt_local * self.rhs_at(u, self.t)
+            self.t += dt_local
+            target -= dt_local
+            if int(math.ceil(target / dt_local)) > 1000:
+                break
+            substeps += 1
+        self.substeps = substeps
+        return u
+
+
+def burgers_params(rng, B, N, *, eq="viscosity", conv="WENO", nu_rows=False, J=3,
+                   adaptive=None, dt=0.01, L=2 * math.pi):
+    x = torch.arange(N, dtype=torch.float64) * (L / N)
+    p = SimpleNamespace(resolution=N, dt=dt, x=x, adaptive_CFL=adaptive, L=L,
+                        nu=(torch.from_numpy(rng.uniform(0.005, 0.05, (B, 1))) if nu_rows else 0.01),
+                        device="cpu", convection_term=conv, equation_type=eq, batch_size=B,
+                        beta=torch.from_numpy(rng.uniform(-0.5, 0.5, (B, 1))), J=J,
+                        A=torch.from_numpy(rng.uniform(-0.5, 0.5, (B, 1, J))),
+                        omega=torch.from_numpy(rng.uniform(-0.4, 0.4, (B, 1, J))),
+                        phi=torch.from_numpy(rng.uniform(0, 2 * math.pi, (B, 1, J))),
+                        l=torch.from_numpy(rng.integers(1, 4, (B, 1, J)).astype(np.float64)))
+    return p
+
+
+def sines_u0(rng, B, N, K=5, L=2 * math.pi):
+    x = np.arange(N) * (L / N)
+    a = rng.uniform(-0.5, 0.5, (B, K))
+    ph = rng.uniform(0, 2 * math.pi, (B, K))
+    k = np.arange(1, K + 1)
+    return (a[:, :, None] * np.sin(k[None, :, None] * x[None, None, :] * (2 * math.pi / L)
+                                   + ph[:, :, None])).sum(1)
+
+
+def p_to_dict(prefix, p):
+    d = {f"{prefix}N": p.resolution, f"{prefix}dt": p.dt, f"{prefix}L": p.L,
+         f"{prefix}x": p.x.numpy(), f"{prefix}conv": p.convection_term,
+         f"{prefix}eq": p.equation_type,
+         f"{prefix}nu": (p.nu.numpy() if torch.is_tensor(p.nu) else np.float64(p.nu)),
+         f"{prefix}beta": p.beta.numpy(), f"{prefix}A": p.A.numpy(),
+         f"{prefix}omega": p.omega.numpy(), f"{prefix}phi": p.phi.numpy(),
+         f"{prefix}l": p.l.numpy(),
+         f"{prefix}cfl": (np.float64(p.adaptive_CFL) if p.adaptive_CFL is not None else np.float64(np.nan))}
+    return d
+
+
+def make_burgers():
+    rng = np.random.default_rng(1234)
+    out = {}
+    # Per-op: WENO reconstruction both directions, nonlinear and linear terms.
+    f = rng.standard_normal((3, 16))
+    out["weno_f"] = f
+    out["weno_left"] = weno_reconstruction(torch.from_numpy(f), "left").numpy()
+    out["weno_right"] = weno_reconstruction(torch.from_numpy(f), "right").numpy()
+    p = burgers_params(rng, 3, 32)
+    solver = _FixedBurgers(p)
+    u = torch.from_numpy(sines_u0(rng, 3, 32))
+    out["op_u"] = u.numpy()
+    out["op_nonlinear_weno"] = solver.calc_nonlinear_weno(u).numpy()
+    out["op_linear"] = solver.calc_linear(u).numpy()
+
+    cases = [
+        ("euler_visc", dict(eq="viscosity"), "euler", False),
+        ("euler_learning", dict(eq="learning", nu_rows=True), "euler", True),
+        ("euler_linear_fdm", dict(eq="linear", conv="FDM"), "euler", True),
+        ("rk3_visc", dict(eq="viscosity"), "rk3", False),
+        ("rk3_learning_s", dict(eq="learning", nu_rows=True), "rk3", True),
+        ("rk3_linear", dict(eq="linear"), "rk3", True),
+        ("adaptive_visc", dict(eq="viscosity", adaptive=0.2, dt=0.05), "euler", False),
+    ]
+    names = []
+    for name, kw, scheme, with_s in cases:
+        B, N, steps = 4, 64, 5
+        p = burgers_params(rng, B, N, **kw)
+        u0 = sines_u0(rng, B, N)
+        s = 0.1 * rng.standard_normal((B, N)) if with_s else None
+        t0 = rng.uniform(0, 1, (B, 1))
+        solver = _FixedBurgers(p)
+        solver.t = torch.from_numpy(t0.copy())
+        solver.correction_s = torch.from_numpy(s) if s is not None else None
+        u = torch.from_numpy(u0)
+        frames = []
+        for _ in range(steps):
+            u = solver.step_rk3(u) if scheme == "rk3" else solver.step(u)
+            frames.append(u.numpy().copy())
+        out.update(p_to_dict(f"{name}.", p))
+        out[f"{name}.scheme"] = scheme
+        out[f"{name}.u0"] = u0
+        out[f"{name}.t0"] = t0
+        out[f"{name}.s"] = s if s is not None else np.zeros(0)
+        out[f"{name}.frames"] = np.stack(frames, 1)
+        if kw.get("adaptive") is not None:
+            out[f"{name}.substeps"] = np.int64(solver.substeps)
+        names.append(name)
+    out["cases"] = np.array(names)
+
+    # Gradients by torch autograd through the (fixed) reference, one and three steps.
+    gnames = []
+    for name, scheme, eq, steps in [("g_euler", "euler", "learning", 1), ("g_rk3", "rk3", "linear", 1),
+                                    ("g_rk3_3", "rk3", "viscosity", 3), ("g_euler_fdm3", "euler", "linear", 3)]:
+        B, N = 3, 32
+        p = burgers_params(rng, B, N, eq=eq, conv=("FDM" if "fdm" in name else "WENO"), nu_rows=True)
+        u0 = torch.from_numpy(sines_u0(rng, B, N)).requires_grad_(True)
+        s = torch.from_numpy(0.1 * rng.standard_normal((B, N))).requires_grad_(True)
+        w = torch.from_numpy(rng.standard_normal((B, steps, N)))
+        solver = _FixedBurgers(p)
+        solver.t = torch.from_numpy(rng.uniform(0, 1, (B, 1)))
+        t0 = solver.t.numpy().copy()
+        solver.correction_s = s
+        u, frames = u0, []
+        for _ in range(steps):
+            u = solver.step_rk3(u) if scheme == "rk3" else solver.step(u)
+            frames.append(u)
+        loss = (torch.stack(frames, 1) * w).sum()
+        gu, gs = torch.autograd.grad(loss, (u0, s))
+        out.update(p_to_dict(f"{name}.", p))
+        out[f"{name}.scheme"] = scheme
+        out[f"{name}.steps"] = np.int64(steps)
+        out[f"{name}.u0"] = u0.detach().numpy()
+        out[f"{name}.t0"] = t0
+        out[f"{name}.s"] = s.detach().numpy()
+        out[f"{name}.w"] = w.numpy()
+        out[f"{name}.loss"] = np.float64(loss.item())
+        out[f"{name}.grad_u"] = gu.numpy()
+        out[f"{name}.grad_s"] = gs.numpy()
+        gnames.append(name)
+    out["grad_cases"] = np.array(gnames)
+    np.savez_compressed(os.path.join(OUT, "burgers_golden.npz"), **out)
+
+
+def ks_u0(rng, B, N, L):
+    x = np.arange(N) * (L / N)
+    k = np.arange(1, 9)
+    a = rng.standard_normal((B, 8)) / k
+    ph = rng.uniform(0, 2 * math.pi, (B, 8))
+    return (a[:, :, None] * np.cos(2 * math.pi * k[None, :, None] * x[None, None, :] / L
+                                   + ph[:, :, None])).sum(1)
+
+
+def make_ks():
+    rng = np.random.default_rng(4321)
+    out = {}
+    names = []
+    cases = [
+        ("etrk2_same_L", "ETRK2", 64, [64.0] * 4, 0.25, True, False, 4),
+        ("etrk2_ragged_L", "ETRK2", 64, [48.0, 64.0, 80.0, 100.0, 22.0], 0.1, True, True, 3),
+        ("etd1_small_dt", "ETD1", 32, [32.0, 40.0, 50.0], 0.05, True, True, 3),
+        ("etrk2_n128_nos", "ETRK2", 128, [100.0, 100.0], 0.2, False, False, 3),
+    ]
+    for name, scheme, N, Ls, dt, with_s, with_cu, steps in cases:
+        B = len(Ls)
+        ds = torch.tensor(Ls)
+        sp = SimpleNamespace(resolution=N, dt=dt, device="cpu", domain_size=ds,
+                             alpha=torch.zeros(B), time_scheme=scheme)
+        solver = KSSolverTorch(sp)
+        u0 = np.stack([ks_u0(rng, 1, N, L)[0] for L in Ls])
+        s = 0.01 * rng.standard_normal((B, N)) if with_s else None
+        cu = 0.01 * rng.standard_normal((B, N)) if with_cu else None
+        solver.correction_s = torch.from_numpy(s) if s is not None else None
+        solver.correction_u = torch.from_numpy(cu) if cu is not None else None
+        u = torch.from_numpy(u0)
+        frames = []
+        for _ in range(steps):
+            u = solver.step(u, ds)
+            frames.append(u.numpy().copy())
+        out[f"{name}.scheme"] = scheme
+        out[f"{name}.N"] = np.int64(N)
+        out[f"{name}.L"] = np.array(Ls)
+        out[f"{name}.dt"] = np.float64(dt)
+        out[f"{name}.u0"] = u0
+        out[f"{name}.s"] = s if s is not None else np.zeros(0)
+        out[f"{name}.cu"] = cu if cu is not None else np.zeros(0)
+        out[f"{name}.frames"] = np.stack(frames, 1)
+        # single substeps, straight from the reference's etd1_step / etrk2_step
+        sub = solver.etrk2_step if scheme == "ETRK2" else solver.etd1_step
+        out[f"{name}.substep"] = sub(torch.from_numpy(u0), ds).numpy()
+        names.append(name)
+    out["cases"] = np.array(names)
+
+    gnames = []
+    for name, scheme, N, Ls, dt, steps in [("g_etrk2", "ETRK2", 64, [64.0, 64.0, 50.0], 0.25, 1),
+                                           ("g_etrk2_3", "ETRK2", 32, [40.0, 40.0], 0.2, 3),
+                                           ("g_etd1", "ETD1", 32, [30.0, 36.0], 0.05, 2)]:
+        B = len(Ls)
+        ds = torch.tensor(Ls)
+        sp = SimpleNamespace(resolution=N, dt=dt, device="cpu", domain_size=ds,
+                             alpha=torch.zeros(B), time_scheme=scheme)
+        solver = KSSolverTorch(sp)
+        u0 = torch.from_numpy(np.stack([ks_u0(rng, 1, N, L)[0] for L in Ls])).requires_grad_(True)
+        s = torch.from_numpy(0.01 * rng.standard_normal((B, N))).requires_grad_(True)
+        w = torch.from_numpy(rng.standard_normal((B, steps, N)))
+        solver.correction_s = s
+        u, frames = u0, []
+        for _ in range(steps):
+            u = solver.step(u, ds)
+            frames.append(u)
+        loss = (torch.stack(frames, 1) * w).sum()
+        gu, gs = torch.autograd.grad(loss, (u0, s))
+        out[f"{name}.scheme"] = scheme
+        out[f"{name}.N"] = np.int64(N)
+        out[f"{name}.L"] = np.array(Ls)
+        out[f"{name}.dt"] = np.float64(dt)
+        out[f"{name}.steps"] = np.int64(steps)
+        out[f"{name}.u0"] = u0.detach().numpy()
+        out[f"{name}.s"] = s.detach().numpy()
+        out[f"{name}.w"] = w.numpy()
+        out[f"{name}.loss"] = np.float64(loss.item())
+        out[f"{name}.grad_u"] = gu.numpy()
+        out[f"{name}.grad_s"] = gs.numpy()
+        gnames.append(name)
+    out["grad_cases"] = np.array(gnames)
+    np.savez_compressed(os.path.join(OUT, "ks_golden.npz"), **out)
+
+
+if __name__ == "__main__":
+    torch.set_default_dtype(torch.float64)
+    make_burgers()
+    make_ks()
+    for f in ("burgers_golden.npz", "ks_golden.npz"):
+        print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
