@@ -1,0 +1,581 @@
+// Burgers WENO5-LF / FDM time stepper for sm_100a: device code and kernels.
+//
+// Layout: u is [rows][n] FP32.  A row is owned by a group of TPR consecutive
+// lanes of one warp (TPR <= 32); lane g of the group holds the CPT contiguous
+// cells [g*CPT, g*CPT+CPT) in registers (n = TPR*CPT).  Periodic halos (3 cells
+// each side) and the per-row Lax-Friedrichs alpha = max|u| move by warp
+// shuffles, so the forward path uses no shared memory and no block barrier.
+//
+// Reference (tum-pbs/INC solvers/solver_1d.py):
+//   weno_reconstruction :4-42, calc_nonlinear_weno :129-142,
+//   calc_nonlinear_FDM :125-127, calc_linear :144-146, _compute_delta :74-85,
+//   _compute_source :104-114, _apply_corrections :116-123, step :181-195.
+#pragma once
+#include <string.h>
+
+#include "common.cuh"
+
+namespace inc {
+namespace burgers {
+
+constexpr float kEps = 1e-6f;  // solver_1d.py:5
+
+// ---------------------------------------------------------------------------
+// WENO5 reconstruction on a 5-point window g0..g4.
+// 'left' (RIGHT=false): f+ at i+1/2 from f[i-2..i+2]   (solver_1d.py:14-22).
+// 'right' (RIGHT=true): f- from f[i-1..i+3]            (solver_1d.py:24-33).
+// The two share q0..q2, beta0 and beta1 on the window; they differ only in the
+// second term of beta2: (3g2 - 4g3 + g4) for left, (g2 - 4g3 + 3g4) for right.
+// ---------------------------------------------------------------------------
+struct Weno {
+    float q0, q1, q2, s0, s1, s2, a0, a1, a2, inv_sum, h;
+    float d0, e0, d1, e1, d2, e2;
+};
+
+template <bool RIGHT>
+INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& w) {
+    w.q0 = fmaf(1.f / 3.f, g0, fmaf(-7.f / 6.f, g1, (11.f / 6.f) * g2));
+    w.q1 = fmaf(-1.f / 6.f, g1, fmaf(5.f / 6.f, g2, (1.f / 3.f) * g3));
+    w.q2 = fmaf(1.f / 3.f, g2, fmaf(5.f / 6.f, g3, (-1.f / 6.f) * g4));
+    w.d0 = fmaf(-2.f, g1, g0) + g2;
+    w.e0 = fmaf(-4.f, g1, g0) + 3.f * g2;
+    w.d1 = fmaf(-2.f, g2, g1) + g3;
+    w.e1 = g1 - g3;
+    w.d2 = fmaf(-2.f, g3, g2) + g4;
+    w.e2 = RIGHT ? (fmaf(-4.f, g3, g2) + 3.f * g4) : (fmaf(-4.f, g3, 3.f * g2) + g4);
+    const float b0 = fmaf(13.f / 12.f * w.d0, w.d0, 0.25f * w.e0 * w.e0);
+    const float b1 = fmaf(13.f / 12.f * w.d1, w.d1, 0.25f * w.e1 * w.e1);
+    const float b2 = fmaf(13.f / 12.f * w.d2, w.d2, 0.25f * w.e2 * w.e2);
+    w.s0 = kEps + b0; w.s1 = kEps + b1; w.s2 = kEps + b2;
+    // alpha_k = gamma_k / (eps + beta_k)^2, gamma = (0.1, 0.6, 0.3)  (:22, :39)
+    w.a0 = __fdividef(0.1f, w.s0 * w.s0);
+    w.a1 = __fdividef(0.6f, w.s1 * w.s1);
+    w.a2 = __fdividef(0.3f, w.s2 * w.s2);
+    w.inv_sum = __fdividef(1.f, w.a0 + w.a1 + w.a2);
+    w.h = (w.a0 * w.q0 + w.a1 * w.q1 + w.a2 * w.q2) * w.inv_sum;
+}
+
+template <bool RIGHT>
+INC_DEV float weno5(float g0, float g1, float g2, float g3, float g4) {
+    Weno w;
+    weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
+    return w.h;
+}
+
+// Adds hb * d h / d g_m to acc[0..4] (the vector-Jacobian product of weno5).
+// With w_k = a_k / S:  dh/dq_k = w_k,  dh/dbeta_k = -2 w_k (q_k - h) / s_k.
+template <bool RIGHT>
+INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float hb,
+                       float& c0, float& c1, float& c2, float& c3, float& c4) {
+    Weno w;
+    weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
+    const float w0 = w.a0 * w.inv_sum, w1 = w.a1 * w.inv_sum, w2 = w.a2 * w.inv_sum;
+    const float qb0 = hb * w0, qb1 = hb * w1, qb2 = hb * w2;
+    const float bb0 = -2.f * qb0 * (w.q0 - w.h) * __fdividef(1.f, w.s0);
+    const float bb1 = -2.f * qb1 * (w.q1 - w.h) * __fdividef(1.f, w.s1);
+    const float bb2 = -2.f * qb2 * (w.q2 - w.h) * __fdividef(1.f, w.s2);
+    // beta_k = 13/12 d^2 + 1/4 e^2  ->  dbeta = 13/6 d dd + 1/2 e de
+    const float A0 = 13.f / 6.f * w.d0 * bb0, E0 = 0.5f * w.e0 * bb0;
+    const float A1 = 13.f / 6.f * w.d1 * bb1, E1 = 0.5f * w.e1 * bb1;
+    const float A2 = 13.f / 6.f * w.d2 * bb2, E2 = 0.5f * w.e2 * bb2;
+    // q0 on (g0,g1,g2): (1/3, -7/6, 11/6); beta0: d (1,-2,1), e (1,-4,3)
+    c0 += (1.f / 3.f) * qb0 + A0 + E0;
+    c1 += (-7.f / 6.f) * qb0 - 2.f * A0 - 4.f * E0;
+    c2 += (11.f / 6.f) * qb0 + A0 + 3.f * E0;
+    // q1 on (g1,g2,g3): (-1/6, 5/6, 1/3); beta1: d (1,-2,1), e (1,0,-1)
+    c1 += (-1.f / 6.f) * qb1 + A1 + E1;
+    c2 += (5.f / 6.f) * qb1 - 2.f * A1;
+    c3 += (1.f / 3.f) * qb1 + A1 - E1;
+    // q2 on (g2,g3,g4): (1/3, 5/6, -1/6); beta2: d (1,-2,1), e left (3,-4,1) / right (1,-4,3)
+    c2 += (1.f / 3.f) * qb2 + A2 + (RIGHT ? 1.f : 3.f) * E2;
+    c3 += (5.f / 6.f) * qb2 - 2.f * A2 - 4.f * E2;
+    c4 += (-1.f / 6.f) * qb2 + A2 + (RIGHT ? 3.f : 1.f) * E2;
+}
+
+// ---------------------------------------------------------------------------
+// Per-row context.
+// ---------------------------------------------------------------------------
+struct Args {
+    const float* u;
+    const float* s;
+    const float* t_rows;
+    float* out;
+    const float* g_out;  // backward
+    float* g_u;
+    float* g_s;
+    float* frames;
+    float* ckpts;
+    const float* g_frames;
+    const float* g_final;
+    const float* nu_rows;
+    const float* dt_rows;
+    const float* beta_rows;
+    const float* forcing;
+    const float* x;
+    int rows, n, scheme, conv, src, J, steps, ckpt_every;
+    float dx, inv_dx, inv_dx2, inv_2dx, dt, nu, beta, t0;
+};
+
+template <int CPT>
+struct Ctx {
+    float nu, dt, beta, t;
+    float s[CPT];
+    bool has_s;
+    int cell0;  // first cell of this lane
+    int row;
+    bool valid;
+};
+
+template <int CPT, int TPR>
+INC_DEV void make_ctx(const Args& a, int row, int g, bool valid, Ctx<CPT>& cx) {
+    const int r = valid ? row : 0;
+    cx.row = r;
+    cx.valid = valid;
+    cx.cell0 = g * CPT;
+    cx.nu = a.nu_rows ? __ldg(a.nu_rows + r) : a.nu;
+    cx.dt = a.dt_rows ? __ldg(a.dt_rows + r) : a.dt;
+    cx.beta = a.beta_rows ? __ldg(a.beta_rows + r) : a.beta;
+    cx.t = a.t_rows ? __ldg(a.t_rows + r) : a.t0;
+    cx.has_s = a.s != nullptr;
+    if (cx.has_s) load_row_chunk<CPT>(cx.s, a.s + (int64_t)r * a.n + cx.cell0, valid);
+    else {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) cx.s[c] = 0.f;
+    }
+}
+
+template <int CPT, int TPR>
+INC_DEV void halo_window(const float (&u)[CPT], float (&w)[CPT + 6], int left, int right) {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) w[c + 3] = u[c];
+    w[0] = shfl<TPR>(u[CPT - 3], left);
+    w[1] = shfl<TPR>(u[CPT - 2], left);
+    w[2] = shfl<TPR>(u[CPT - 1], left);
+    w[CPT + 3] = shfl<TPR>(u[0], right);
+    w[CPT + 4] = shfl<TPR>(u[1], right);
+    w[CPT + 5] = shfl<TPR>(u[2], right);
+}
+
+// r = nonlinear + linear (no source): calc_nonlinear_weno / _FDM + calc_linear.
+template <int CPT, int TPR>
+INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu,
+                      float inv_dx, float inv_dx2, float inv_2dx, int left, int right) {
+    float w[CPT + 6];
+    halo_window<CPT, TPR>(u, w, left, right);
+    if (conv == INC_CONV_WENO) {
+        float m = 0.f;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
+        const float alpha = group_max<TPR>(m);  // per-row max |u|, solver_1d.py:133
+        float fp[CPT + 6], fm[CPT + 6];
+#pragma unroll
+        for (int k = 0; k < CPT + 6; ++k) {
+            const float fl = 0.5f * w[k] * w[k];  // flux = 0.5 u^2
+            fp[k] = 0.5f * (fl + alpha * w[k]);
+            fm[k] = 0.5f * (fl - alpha * w[k]);
+        }
+        float hp_prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]);
+        float hm_prev = weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float hp = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]);
+            const float hm = weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+            const float nl = -((hp - hp_prev) * inv_dx + (hm - hm_prev) * inv_dx);
+            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
+            hp_prev = hp;
+            hm_prev = hm;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float nl = -w[c + 3] * ((w[c + 4] - w[c + 2]) * inv_2dx);
+            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
+        }
+    }
+}
+
+// r += source(u, t) + correction s (solver_1d.py:104-123).
+template <int CPT>
+INC_DEV void add_source(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], float (&r)[CPT], float t) {
+    if (a.src == INC_SRC_LINEAR) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) r[c] = fmaf(cx.beta, u[c], r[c]);
+    } else if (a.src == INC_SRC_FORCING) {
+        const float* fp = a.forcing + (int64_t)cx.row * 4 * a.J;
+        for (int j = 0; j < a.J; ++j) {
+            const float A = __ldg(fp + j), om = __ldg(fp + a.J + j), ph = __ldg(fp + 2 * a.J + j),
+                        kx = __ldg(fp + 3 * a.J + j);
+            const float wt = om * t;
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+                const float x = __ldg(a.x + cx.cell0 + c);
+                r[c] = fmaf(A, sinf((wt + kx * x) + ph), r[c]);
+            }
+        }
+    }
+    if (cx.has_s) {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) r[c] += cx.s[c];
+    }
+}
+
+template <int CPT, int TPR>
+INC_DEV void full_rhs(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], float (&r)[CPT], float t,
+                      int left, int right) {
+    rhs_core<CPT, TPR>(u, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, left, right);
+    add_source<CPT>(a, cx, u, r, t);
+}
+
+// One step (Euler or SSP-RK3) of size cx.dt starting at time t.
+template <int CPT, int TPR>
+INC_DEV void advance(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], float t, int left, int right) {
+    float r[CPT];
+    const float dt = cx.dt;
+    if (a.scheme == INC_TS_EULER) {
+        full_rhs<CPT, TPR>(a, cx, u, r, t, left, right);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) u[c] = u[c] + dt * r[c];
+    } else {
+        float u0[CPT];
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) u0[c] = u[c];
+        full_rhs<CPT, TPR>(a, cx, u, r, t, left, right);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) u[c] = u0[c] + dt * r[c];
+        full_rhs<CPT, TPR>(a, cx, u, r, t + dt, left, right);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) u[c] = 0.75f * u0[c] + 0.25f * (u[c] + dt * r[c]);
+        full_rhs<CPT, TPR>(a, cx, u, r, t + 0.5f * dt, left, right);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) u[c] = (1.f / 3.f) * u0[c] + (2.f / 3.f) * (u[c] + dt * r[c]);
+    }
+}
+
+// out = J(u)^T v for the spatial operator (nonlinear + linear + beta*u source).
+template <int CPT, int TPR>
+INC_DEV void rhs_vjp(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], const float (&v)[CPT],
+                     float (&out)[CPT], int g, int left, int right) {
+    float w[CPT + 6];
+    halo_window<CPT, TPR>(u, w, left, right);
+    const float v_r = shfl<TPR>(v[0], right);
+    const float v_l = shfl<TPR>(v[CPT - 1], left);
+    const float nu = cx.nu;
+    if (a.conv == INC_CONV_WENO) {
+        float m = -1.f;
+        int mi = 0;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float av = fabsf(u[c]);
+            if (av > m) { m = av; mi = g * CPT + c; }
+        }
+        group_argmax<TPR>(m, mi);
+        const float alpha = m;
+        float fp[CPT + 6], fm[CPT + 6];
+#pragma unroll
+        for (int k = 0; k < CPT + 6; ++k) {
+            const float fl = 0.5f * w[k] * w[k];
+            fp[k] = 0.5f * (fl + alpha * w[k]);
+            fm[k] = 0.5f * (fl - alpha * w[k]);
+        }
+        float accp[CPT + 5], accm[CPT + 5];  // index e <-> cell cell0 - 2 + e
+#pragma unroll
+        for (int e = 0; e < CPT + 5; ++e) { accp[e] = 0.f; accm[e] = 0.f; }
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float vn = (c + 1 < CPT) ? v[c + 1] : v_r;
+            // hp[i] enters R[i] with -1/dx and R[i+1] with +1/dx (same for hm).
+            const float hb = (vn - v[c]) * a.inv_dx;
+            weno5_vjp<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5], hb,
+                             accp[c], accp[c + 1], accp[c + 2], accp[c + 3], accp[c + 4]);
+            weno5_vjp<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6], hb,
+                            accm[c + 1], accm[c + 2], accm[c + 3], accm[c + 4], accm[c + 5]);
+        }
+        float ub[CPT + 5];
+        float abar = 0.f;
+#pragma unroll
+        for (int e = 0; e < CPT + 5; ++e) {
+            const float uj = w[e + 1];
+            ub[e] = accp[e] * (0.5f * (uj + alpha)) + accm[e] * (0.5f * (uj - alpha));
+            abar += 0.5f * uj * (accp[e] - accm[e]);
+        }
+        const float fl0 = shfl<TPR>(ub[CPT + 2], left), fl1 = shfl<TPR>(ub[CPT + 3], left),
+                    fl2 = shfl<TPR>(ub[CPT + 4], left);
+        const float fr0 = shfl<TPR>(ub[0], right), fr1 = shfl<TPR>(ub[1], right);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) out[c] = ub[c + 2];
+        out[0] += fl0;
+        out[1] += fl1;
+        out[2] += fl2;
+        out[CPT - 2] += fr0;
+        out[CPT - 1] += fr1;
+        abar = group_sum<TPR>(abar);
+        // alpha = |u[argmax]|: d|u|/du = sign(u) (torch.abs backward, 0 at 0)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            if (g * CPT + c == mi) {
+                const float sg = u[c] > 0.f ? 1.f : (u[c] < 0.f ? -1.f : 0.f);
+                out[c] = fmaf(abar, sg, out[c]);
+            }
+        }
+    } else {
+        // R_i = -u_i (u_{i+1} - u_{i-1}) / (2 dx)
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float vm = c > 0 ? v[c - 1] : v_l;
+            const float vp = c + 1 < CPT ? v[c + 1] : v_r;
+            out[c] = -v[c] * ((w[c + 4] - w[c + 2]) * a.inv_2dx) - vm * w[c + 2] * a.inv_2dx +
+                     vp * w[c + 4] * a.inv_2dx;
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        const float vm = c > 0 ? v[c - 1] : v_l;
+        const float vp = c + 1 < CPT ? v[c + 1] : v_r;
+        out[c] += nu * ((vm - 2.f * v[c] + vp) * a.inv_dx2);
+        if (a.src == INC_SRC_LINEAR) out[c] = fmaf(cx.beta, v[c], out[c]);
+    }
+}
+
+// Backward of `advance`: given gu = dL/du_new (in), returns dL/du in gu and
+// accumulates dL/ds into gs.
+template <int CPT, int TPR>
+INC_DEV void advance_bwd(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], float (&gu)[CPT],
+                         float (&gs)[CPT], float t, int g, int left, int right) {
+    const float dt = cx.dt;
+    float j[CPT];
+    if (a.scheme == INC_TS_EULER) {
+        rhs_vjp<CPT, TPR>(a, cx, u, gu, j, g, left, right);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            gs[c] += dt * gu[c];
+            gu[c] = gu[c] + dt * j[c];
+        }
+        return;
+    }
+    // recompute the stages
+    float u1[CPT], u2[CPT], r[CPT];
+    full_rhs<CPT, TPR>(a, cx, u, r, t, left, right);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) u1[c] = u[c] + dt * r[c];
+    full_rhs<CPT, TPR>(a, cx, u1, r, t + dt, left, right);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) u2[c] = 0.75f * u[c] + 0.25f * (u1[c] + dt * r[c]);
+    // u3 = 1/3 u + 2/3 (u2 + dt R(u2))
+    float acc[CPT], b[CPT];
+    rhs_vjp<CPT, TPR>(a, cx, u2, gu, j, g, left, right);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        acc[c] = (1.f / 3.f) * gu[c];
+        gs[c] += (2.f / 3.f) * dt * gu[c];
+        b[c] = (2.f / 3.f) * (gu[c] + dt * j[c]);  // dL/du2
+    }
+    // u2 = 3/4 u + 1/4 (u1 + dt R(u1))
+    rhs_vjp<CPT, TPR>(a, cx, u1, b, j, g, left, right);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        acc[c] += 0.75f * b[c];
+        gs[c] += 0.25f * dt * b[c];
+        b[c] = 0.25f * (b[c] + dt * j[c]);  // dL/du1
+    }
+    // u1 = u + dt R(u)
+    rhs_vjp<CPT, TPR>(a, cx, u, b, j, g, left, right);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        gs[c] += dt * b[c];
+        gu[c] = acc[c] + b[c] + dt * j[c];
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Kernels
+// ---------------------------------------------------------------------------
+template <int CPT, int TPR>
+INC_DEV void lane_setup(int& row, int& g, int& left, int& right, bool& valid, int rows) {
+    const int rpb = blockDim.x / TPR;
+    row = blockIdx.x * rpb + threadIdx.x / TPR;
+    g = threadIdx.x % TPR;
+    left = (g + TPR - 1) & (TPR - 1);
+    right = (g + 1) & (TPR - 1);
+    valid = row < rows;
+}
+
+template <int CPT, int TPR>
+__global__ void __launch_bounds__(256) k_step(Args a) {
+    int row, g, left, right;
+    bool valid;
+    lane_setup<CPT, TPR>(row, g, left, right, valid, a.rows);
+    Ctx<CPT> cx;
+    make_ctx<CPT, TPR>(a, row, g, valid, cx);
+    float u[CPT];
+    const int64_t base = (int64_t)row * a.n + g * CPT;
+    load_row_chunk<CPT>(u, a.u + base, valid);
+    advance<CPT, TPR>(a, cx, u, cx.t, left, right);
+    store_row_chunk<CPT>(a.out + base, u, valid);
+}
+
+template <int CPT, int TPR>
+__global__ void __launch_bounds__(256) k_step_bwd(Args a) {
+    int row, g, left, right;
+    bool valid;
+    lane_setup<CPT, TPR>(row, g, left, right, valid, a.rows);
+    Ctx<CPT> cx;
+    make_ctx<CPT, TPR>(a, row, g, valid, cx);
+    float u[CPT], gu[CPT], gs[CPT];
+    const int64_t base = (int64_t)row * a.n + g * CPT;
+    load_row_chunk<CPT>(u, a.u + base, valid);
+    load_row_chunk<CPT>(gu, a.g_out + base, valid);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) gs[c] = 0.f;
+    advance_bwd<CPT, TPR>(a, cx, u, gu, gs, cx.t, g, left, right);
+    store_row_chunk<CPT>(a.g_u + base, gu, valid);
+    if (a.g_s) store_row_chunk<CPT>(a.g_s + base, gs, valid);
+}
+
+// Fused rollout: `steps` steps with the state in registers.
+template <int CPT, int TPR>
+__global__ void __launch_bounds__(256) k_rollout(Args a) {
+    int row, g, left, right;
+    bool valid;
+    lane_setup<CPT, TPR>(row, g, left, right, valid, a.rows);
+    Ctx<CPT> cx;
+    make_ctx<CPT, TPR>(a, row, g, valid, cx);
+    float u[CPT];
+    const int64_t base = (int64_t)row * a.n + g * CPT;
+    load_row_chunk<CPT>(u, a.u + base, valid);
+    const int nseg = a.ckpt_every > 0 ? (a.steps + a.ckpt_every - 1) / a.ckpt_every : 0;
+    for (int k = 0; k < a.steps; ++k) {
+        if (a.ckpts && k % a.ckpt_every == 0)
+            store_row_chunk<CPT>(a.ckpts + ((int64_t)row * nseg + k / a.ckpt_every) * a.n + g * CPT, u, valid);
+        advance<CPT, TPR>(a, cx, u, cx.t + k * cx.dt, left, right);
+        if (a.frames) store_row_chunk_cs<CPT>(a.frames + ((int64_t)row * a.steps + k) * a.n + g * CPT, u, valid);
+    }
+    if (a.out) store_row_chunk<CPT>(a.out + base, u, valid);
+}
+
+// Backward of the fused rollout.  Segments of ckpt_every steps are replayed
+// from their checkpoint; the replayed states of one segment live in shared
+// memory laid out [state][c][lane] so that lanes access consecutive words.
+template <int CPT, int TPR>
+__global__ void __launch_bounds__(256) k_rollout_bwd(Args a) {
+    extern __shared__ float sm[];
+    int row, g, left, right;
+    bool valid;
+    lane_setup<CPT, TPR>(row, g, left, right, valid, a.rows);
+    Ctx<CPT> cx;
+    make_ctx<CPT, TPR>(a, row, g, valid, cx);
+    const int K = a.ckpt_every;
+    const int n = a.n;
+    float* seg = sm + (threadIdx.x / TPR) * (K * n);
+    const int nseg = (a.steps + K - 1) / K;
+    float gu[CPT], gs[CPT];
+    const int64_t base = (int64_t)row * n + g * CPT;
+    if (a.g_final) load_row_chunk<CPT>(gu, a.g_final + base, valid);
+    else {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) gu[c] = 0.f;
+    }
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) gs[c] = 0.f;
+    for (int sidx = nseg - 1; sidx >= 0; --sidx) {
+        const int k0 = sidx * K;
+        const int len = min(K, a.steps - k0);
+        float u[CPT];
+        load_row_chunk<CPT>(u, a.ckpts + ((int64_t)row * nseg + sidx) * n + g * CPT, valid);
+        for (int j = 0; j < len; ++j) {
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) seg[j * n + c * TPR + g] = u[c];
+            if (j + 1 < len) advance<CPT, TPR>(a, cx, u, cx.t + (k0 + j) * cx.dt, left, right);
+        }
+        for (int j = len - 1; j >= 0; --j) {
+            const int k = k0 + j;
+            if (a.g_frames) {
+                float gf[CPT];
+                load_row_chunk<CPT>(gf, a.g_frames + ((int64_t)row * a.steps + k) * n + g * CPT, valid);
+#pragma unroll
+                for (int c = 0; c < CPT; ++c) gu[c] += gf[c];
+            }
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) u[c] = seg[j * n + c * TPR + g];
+            advance_bwd<CPT, TPR>(a, cx, u, gu, gs, cx.t + k * cx.dt, g, left, right);
+        }
+    }
+    store_row_chunk<CPT>(a.g_u + base, gu, valid);
+    if (a.g_s) store_row_chunk<CPT>(a.g_s + base, gs, valid);
+}
+
+// weno_reconstruction(f, direction) as a standalone op (solver_1d.py:4-42).
+template <int CPT, int TPR>
+__global__ void __launch_bounds__(256) k_weno(const float* __restrict__ f, float* __restrict__ out, int rows,
+                                              int n, int right_dir) {
+    int row, g, left, right;
+    bool valid;
+    lane_setup<CPT, TPR>(row, g, left, right, valid, rows);
+    float u[CPT], w[CPT + 6], h[CPT];
+    const int64_t base = (int64_t)row * n + g * CPT;
+    load_row_chunk<CPT>(u, f + base, valid);
+    halo_window<CPT, TPR>(u, w, left, right);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c)
+        h[c] = right_dir ? weno5<true>(w[c + 2], w[c + 3], w[c + 4], w[c + 5], w[c + 6])
+                         : weno5<false>(w[c + 1], w[c + 2], w[c + 3], w[c + 4], w[c + 5]);
+    store_row_chunk<CPT>(out + base, h, valid);
+}
+
+// ---------------------------------------------------------------------------
+// Launchers (instantiated per shape in burgers_inst_*.cu)
+// ---------------------------------------------------------------------------
+enum class Kind { Step, StepBwd, Rollout, RolloutBwd };
+
+// Forward (Step, Rollout) and backward (StepBwd, RolloutBwd) launchers.  They
+// are declared here and explicitly instantiated per shape in
+// burgers_{fwd,bwd}_c*.cu so that the shapes compile in parallel.
+template <int CPT, int TPR>
+int launch_fwd(Kind kind, const Args& a, cudaStream_t st, int block);
+template <int CPT, int TPR>
+int launch_bwd(Kind kind, const Args& a, cudaStream_t st, int block);
+
+template <int CPT, int TPR>
+int launch_fwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
+    const int rpb = block / TPR;
+    const int grid = (a.rows + rpb - 1) / rpb;
+    if (kind == Kind::Step) k_step<CPT, TPR><<<grid, block, 0, st>>>(a);
+    else k_rollout<CPT, TPR><<<grid, block, 0, st>>>(a);
+    return check_launch("burgers");
+}
+
+template <int CPT, int TPR>
+int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
+    const int rpb = block / TPR;
+    const int grid = (a.rows + rpb - 1) / rpb;
+    if (kind == Kind::StepBwd) {
+        k_step_bwd<CPT, TPR><<<grid, block, 0, st>>>(a);
+    } else {
+        const size_t smem = (size_t)rpb * a.ckpt_every * a.n * sizeof(float);
+        if (smem > 227 * 1024) {
+            set_error("rollout_bwd: ckpt_every*n too large for shared memory (%zu bytes)", smem);
+            return INC_E_INVALID;
+        }
+        if (smem > 48 * 1024)
+            cudaFuncSetAttribute(k_rollout_bwd<CPT, TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        k_rollout_bwd<CPT, TPR><<<grid, block, smem, st>>>(a);
+    }
+    return check_launch("burgers_bwd");
+}
+
+template <int CPT, int TPR>
+int launch_weno(const float* f, float* out, int rows, int n, int dir, cudaStream_t st, int block);
+
+template <int CPT, int TPR>
+int launch_weno_impl(const float* f, float* out, int rows, int n, int dir, cudaStream_t st, int block) {
+    const int grid = (rows + block / TPR - 1) / (block / TPR);
+    k_weno<CPT, TPR><<<grid, block, 0, st>>>(f, out, rows, n, dir);
+    return check_launch("weno");
+}
+
+#define INC_BURGERS_SHAPES_C4(X) X(4, 2) X(4, 4) X(4, 8) X(4, 16) X(4, 32)
+#define INC_BURGERS_SHAPES_C8(X) X(8, 4) X(8, 8) X(8, 16) X(8, 32)
+#define INC_BURGERS_SHAPES_C16(X) X(16, 8) X(16, 16) X(16, 32)
+#define INC_BURGERS_SHAPES(X) INC_BURGERS_SHAPES_C4(X) INC_BURGERS_SHAPES_C8(X) INC_BURGERS_SHAPES_C16(X)
+
+}  // namespace burgers
+}  // namespace inc

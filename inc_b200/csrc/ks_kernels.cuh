@@ -1,0 +1,736 @@
+// Kuramoto-Sivashinsky pseudo-spectral ETRK2 / ETD1 stepper for sm_100a.
+//
+// Two rows a, b share one complex FFT of length N: z = u_a + i u_b.  A row pair
+// is owned by a group of T lanes (T <= 32, inside one warp); lane t holds the
+// P = N/T values z[t + T*m] in register m, for physical and spectral data
+// alike.  An FFT is two Stockham passes: a P-point DFT in registers, one
+// exchange through a swizzled shared-memory tile, then T-point DFTs in
+// registers with FP64-derived twiddles.  Every operator of the step is a
+// Fourier multiplier or a pointwise product, so the whole step (both
+// substeps) runs in registers with four FFTs per substep.
+//
+// Spectral storage: "packed" (the FFT of z) when both rows of a pair have the
+// same domain size; otherwise "split": slot k < N/2 holds row a's spectrum
+// A[k], slot k > N/2 holds row b's B[k], slots 0 and N/2 hold (A, B) as
+// (re, im).  Converting costs one mirror exchange (k <-> N-k) by shuffles.
+// Spectra are stored scaled by 1/N so the inverse FFT needs no scaling.
+//
+// Reference (tum-pbs/INC solvers/solver_1d.py): calc_nonlinear :225-233,
+// calc_linear :235-240, etd1_step :242-255, etrk2_step :257-278,
+// etd1/etrk2 (double step, correction_u) :280-288.  The derivative multiplier
+// is zero at the Nyquist bin: the reference's value there is purely imaginary
+// and is discarded by ifft(.).real, so the two are the same map.
+#pragma once
+#include "common.cuh"
+
+namespace inc {
+namespace ks {
+
+// ---- complex helpers ---------------------------------------------------------
+INC_DEV float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+INC_DEV float2 csub(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+INC_DEV float2 cmul(float2 a, float2 b) { return make_float2(fmaf(a.x, b.x, -a.y * b.y), fmaf(a.x, b.y, a.y * b.x)); }
+INC_DEV float2 cmulc(float2 a, float2 b) {  // a * conj(b)
+    return make_float2(fmaf(a.x, b.x, a.y * b.y), fmaf(a.y, b.x, -a.x * b.y));
+}
+INC_DEV float2 cscale(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+
+// cos(2*pi*m/32), sin(2*pi*m/32) for m in [0, 16), rounded from FP64.
+INC_DEV float cos32(int m) {
+    switch (m) {
+        case 0: return 1.0f;
+        case 1: return 0.9807852506637573f;
+        case 2: return 0.9238795042037964f;
+        case 3: return 0.8314695954322815f;
+        case 4: return 0.7071067690849304f;
+        case 5: return 0.5555702447891235f;
+        case 6: return 0.3826834261417389f;
+        case 7: return 0.19509032368659973f;
+        case 8: return 0.0f;
+        case 9: return -0.19509032368659973f;
+        case 10: return -0.3826834261417389f;
+        case 11: return -0.5555702447891235f;
+        case 12: return -0.7071067690849304f;
+        case 13: return -0.8314695954322815f;
+        case 14: return -0.9238795042037964f;
+        default: return -0.9807852506637573f;
+    }
+}
+INC_DEV float sin32(int m) {
+    switch (m) {
+        case 0: return 0.0f;
+        case 1: return 0.19509032368659973f;
+        case 2: return 0.3826834261417389f;
+        case 3: return 0.5555702447891235f;
+        case 4: return 0.7071067690849304f;
+        case 5: return 0.8314695954322815f;
+        case 6: return 0.9238795042037964f;
+        case 7: return 0.9807852506637573f;
+        case 8: return 1.0f;
+        case 9: return 0.9807852506637573f;
+        case 10: return 0.9238795042037964f;
+        case 11: return 0.8314695954322815f;
+        case 12: return 0.7071067690849304f;
+        case 13: return 0.5555702447891235f;
+        case 14: return 0.3826834261417389f;
+        default: return 0.19509032368659973f;
+    }
+}
+
+// b * exp(-+ 2 pi i m / 32) (forward: minus, inverse: plus).
+template <bool INV>
+INC_DEV float2 rot32(float2 b, int m) {
+    if (m == 0) return b;
+    if (m == 8) return INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+    const float c = cos32(m), s = INV ? sin32(m) : -sin32(m);
+    return make_float2(fmaf(b.x, c, -b.y * s), fmaf(b.x, s, b.y * c));
+}
+
+// In-register DFT of P <= 32 points, natural order in and out: radix-2
+// Stockham autosort (every index is arithmetic on unrolled loop counters, so
+// the whole transform stays in registers).
+template <int P, bool INV>
+INC_DEV void dft_reg(float2 (&v)[P]) {
+#pragma unroll
+    for (int ns = 1; ns < P; ns *= 2) {
+        float2 w[P];
+#pragma unroll
+        for (int j = 0; j < P / 2; ++j) {
+            const int k = j % ns;
+            const float2 a = v[j];
+            const float2 b = rot32<INV>(v[j + P / 2], k * (16 / ns));
+            const int idx = (j / ns) * ns * 2 + k;
+            w[idx] = cadd(a, b);
+            w[idx + ns] = csub(a, b);
+        }
+#pragma unroll
+        for (int i = 0; i < P; ++i) v[i] = w[i];
+    }
+}
+
+// Length-N (= P*T) forward FFT of a row pair held as z[t + T*m] in v[m]; same
+// layout out.  buf: N float2 of shared memory private to the group.
+// tw[(q + Q*r)*T + t] = exp(-2 pi i r (t + T q) / N) (Q = P/T).
+template <int P, int T>
+INC_DEV void fft_fwd(float2 (&v)[P], float2* buf, const float2* tw, int t) {
+    constexpr int Q = P / T;
+    dft_reg<P, false>(v);
+    __syncwarp();
+#pragma unroll
+    for (int r = 0; r < P; ++r) buf[t * P + (r ^ t)] = v[r];
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < Q; ++q) {
+        float2 w[T];
+        const int j = t + T * q;
+#pragma unroll
+        for (int r = 0; r < T; ++r) {
+            float2 y = buf[r * P + (j ^ r)];
+            if (r > 0) y = cmul(y, tw[(q + Q * r) * T + t]);
+            w[r] = y;
+        }
+        dft_reg<T, false>(w);
+#pragma unroll
+        for (int r = 0; r < T; ++r) v[q + Q * r] = w[r];
+    }
+}
+
+// Unnormalised inverse FFT: conj(FFT(conj(v))).
+template <int P, int T>
+INC_DEV void fft_inv(float2 (&v)[P], float2* buf, const float2* tw, int t) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+    fft_fwd<P, T>(v, buf, tw, t);
+#pragma unroll
+    for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+}
+
+// ---- mirror exchange: slot k <-> slot N-k --------------------------------------
+// Slot k = t + T*m.  Its mirror lives in lane (T-t)%T, register P-1-m (t != 0)
+// or in lane 0, register (P-m)%P (t == 0).
+template <int P, int T>
+INC_DEV void mirror(const float2 (&v)[P], float2 (&mv)[P], int t) {
+    float2 recv[P];
+    const int partner = (T - t) & (T - 1);
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        recv[m].x = shfl<T>(v[m].x, partner);
+        recv[m].y = shfl<T>(v[m].y, partner);
+    }
+#pragma unroll
+    for (int m = 0; m < P; ++m) mv[m] = (t != 0) ? recv[P - 1 - m] : v[(P - m) % P];
+}
+
+// packed Z = FFT(a + i b)  ->  split (A in the lower half, B in the upper half)
+template <int P, int T>
+INC_DEV void to_split(float2 (&v)[P], int t) {
+    constexpr int N = P * T;
+    float2 mv[P];
+    mirror<P, T>(v, mv, t);
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int k = t + T * m;
+        const float2 z = v[m], zm = mv[m];
+        if (k == 0 || k == N / 2) continue;
+        if (k < N / 2) v[m] = make_float2(0.5f * (z.x + zm.x), 0.5f * (z.y - zm.y));
+        else v[m] = make_float2(0.5f * (z.y + zm.y), -0.5f * (z.x - zm.x));
+    }
+}
+
+template <int P, int T>
+INC_DEV void to_packed(float2 (&v)[P], int t) {
+    constexpr int N = P * T;
+    float2 mv[P];
+    mirror<P, T>(v, mv, t);
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int k = t + T * m;
+        const float2 s = v[m], sm = mv[m];
+        if (k == 0 || k == N / 2) continue;
+        if (k < N / 2) v[m] = make_float2(s.x + sm.y, s.y + sm.x);
+        else v[m] = make_float2(sm.x - s.y, s.x - sm.y);
+    }
+}
+
+// ---- arguments ---------------------------------------------------------------
+struct Args {
+    const float* u;
+    const float* s;
+    const float* cu;
+    float* out;
+    const float* g_out;
+    float* g_u;
+    float* g_s;
+    float* frames;
+    float* ckpts;
+    const float* g_frames;
+    const float* g_final;
+    const int* pairs;     // [npairs][2], second = -1 for a lone row
+    const float* dR;      // [rows] pi / L
+    const float* coef;    // [rows][3][nhp]: exp(L dt), phi1, phi2
+    const float2* tw;     // [N] FFT twiddles (layout of fft())
+    int rows, n, npairs, scheme, split, dealias, steps, ckpt_every, nhp;
+    float invN;
+};
+
+// Per-lane context of one row pair.
+struct Ctx {
+    int ra, rb;      // rows (rb = -1: lone row)
+    int rbc;         // row whose coefficients the upper half uses
+    int t;
+    bool valid;
+    float dRa, dRb;  // pi / L of each row
+};
+
+INC_DEV void make_ctx(const Args& a, int pair, int t, bool valid, Ctx& c) {
+    c.t = t;
+    c.valid = valid;
+    const int p = valid ? pair : 0;
+    c.ra = __ldg(a.pairs + 2 * p);
+    c.rb = valid ? __ldg(a.pairs + 2 * p + 1) : -1;
+    c.rbc = c.rb >= 0 ? c.rb : c.ra;
+    c.dRa = __ldg(a.dR + c.ra);
+    c.dRb = __ldg(a.dR + c.rbc);
+}
+
+// Multipliers of slot k = t + T*m.  `sp` marks slots 0 and N/2 in split
+// storage, whose .x belongs to row a and .y to row b (real multipliers there).
+struct Slot {
+    float E, p1, p2, d;  // d: derivative multiplier is -i*d (unscaled)
+    float Eb, p1b, p2b;
+    bool sp;
+};
+
+template <int P, int T>
+INC_DEV Slot slot(const Args& a, const Ctx& c, int m, bool need_p2) {
+    constexpr int N = P * T;
+    const int k = c.t + T * m;
+    const bool up = k > N / 2;
+    const int kk = up ? N - k : k;
+    const int row = (a.split && up) ? c.rbc : c.ra;
+    const float* cr = a.coef + (int64_t)row * 3 * a.nhp;
+    Slot s;
+    s.E = __ldg(cr + kk);
+    s.p1 = __ldg(cr + a.nhp + kk);
+    s.p2 = need_p2 ? __ldg(cr + 2 * a.nhp + kk) : 0.f;
+    int f = (k < N / 2) ? k : (k == N / 2 ? 0 : k - N);
+    if (a.dealias && 3 * abs(f) > N) f = 0;
+    s.d = (float)f * ((a.split && up) ? c.dRb : c.dRa);
+    s.sp = a.split && (k == 0 || k == N / 2);
+    if (s.sp) {
+        const float* cb = a.coef + (int64_t)c.rbc * 3 * a.nhp;
+        s.Eb = __ldg(cb + kk);
+        s.p1b = __ldg(cb + a.nhp + kk);
+        s.p2b = need_p2 ? __ldg(cb + 2 * a.nhp + kk) : 0.f;
+    } else {
+        s.Eb = s.E; s.p1b = s.p1; s.p2b = s.p2;
+    }
+    return s;
+}
+
+// real multiplier (row a on .x, row b on .y at the special slots)
+INC_DEV float2 rmul(float2 z, float ma, float mb) { return make_float2(ma * z.x, mb * z.y); }
+// -i * d * z
+INC_DEV float2 dmul(float2 z, float d) { return make_float2(d * z.y, -d * z.x); }
+
+// ---- loads / stores of a row pair in the lane layout ----------------------------
+template <int P, int T>
+INC_DEV void load_pair(float2 (&x)[P], const float* __restrict__ src, const Ctx& c, int n) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int i = c.t + T * m;
+        x[m].x = c.valid ? __ldg(src + (int64_t)c.ra * n + i) : 0.f;
+        x[m].y = (c.valid && c.rb >= 0) ? __ldg(src + (int64_t)c.rb * n + i) : 0.f;
+    }
+}
+
+template <int P, int T>
+INC_DEV void add_pair(float2 (&x)[P], const float* __restrict__ src, const Ctx& c, int n) {
+    float2 y[P];
+    load_pair<P, T>(y, src, c, n);
+#pragma unroll
+    for (int m = 0; m < P; ++m) x[m] = cadd(x[m], y[m]);
+}
+
+template <int P, int T>
+INC_DEV void store_pair(float* __restrict__ dst, const float2 (&x)[P], const Ctx& c, int n) {
+    if (!c.valid) return;
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int i = c.t + T * m;
+        dst[(int64_t)c.ra * n + i] = x[m].x;
+        if (c.rb >= 0) dst[(int64_t)c.rb * n + i] = x[m].y;
+    }
+}
+
+// Row-strided variant for [rows][steps][n] frames / [rows][nseg][n] checkpoints.
+template <int P, int T>
+INC_DEV void store_pair_strided(float* __restrict__ dst, const float2 (&x)[P], const Ctx& c, int n,
+                                int64_t row_stride, int64_t off) {
+    if (!c.valid) return;
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int i = c.t + T * m;
+        __stcs(dst + (int64_t)c.ra * row_stride + off + i, x[m].x);
+        if (c.rb >= 0) __stcs(dst + (int64_t)c.rb * row_stride + off + i, x[m].y);
+    }
+}
+
+template <int P, int T>
+INC_DEV void load_pair_strided(float2 (&x)[P], const float* __restrict__ src, const Ctx& c, int n,
+                               int64_t row_stride, int64_t off) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const int i = c.t + T * m;
+        x[m].x = c.valid ? __ldg(src + (int64_t)c.ra * row_stride + off + i) : 0.f;
+        x[m].y = (c.valid && c.rb >= 0) ? __ldg(src + (int64_t)c.rb * row_stride + off + i) : 0.f;
+    }
+}
+
+// ---- the step -----------------------------------------------------------------
+// Forward FFT of physical v into scaled spectral storage (packed or split).
+template <int P, int T>
+INC_DEV void to_spec(const Args& a, float2 (&v)[P], float2* buf, const float2* tw, int t, bool scale) {
+    fft_fwd<P, T>(v, buf, tw, t);
+    if (scale) {
+#pragma unroll
+        for (int m = 0; m < P; ++m) v[m] = cscale(v[m], a.invN);
+    }
+    if (a.split) to_split<P, T>(v, t);
+}
+
+// Inverse FFT of scaled spectral storage into physical values.
+template <int P, int T>
+INC_DEV void to_phys(const Args& a, float2 (&v)[P], float2* buf, const float2* tw, int t) {
+    if (a.split) to_packed<P, T>(v, t);
+    fft_inv<P, T>(v, buf, tw, t);
+}
+
+INC_DEV float2 sq2(float2 x) { return make_float2(x.x * x.x, x.y * x.y); }
+
+// SS = phi1 * FFT(s) / N, held for the whole step (s enters stage 1 of each substep).
+template <int P, int T>
+INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], float2* buf, const float2* tw) {
+    if (!a.s) {
+#pragma unroll
+        for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
+        return;
+    }
+    load_pair<P, T>(SS, a.s, c, a.n);
+    to_spec<P, T>(a, SS, buf, tw, c.t, true);
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const Slot s = slot<P, T>(a, c, m, false);
+        SS[m] = rmul(SS[m], s.p1, s.p1b);
+    }
+}
+
+// One substep.  x: physical in/out; X: scaled spectrum of x in/out.
+// If xi != nullptr (ETRK2) the intermediate physical state is also returned.
+template <int P, int T>
+INC_DEV void substep(const Args& a, const Ctx& c, float2 (&x)[P], float2 (&X)[P], const float2 (&SS)[P],
+                     float2* buf, const float2* tw, float2 (*xi)[P]) {
+    const int t = c.t;
+    float2 v[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
+    to_spec<P, T>(a, v, buf, tw, t, false);
+    if (a.scheme == INC_KS_ETD1) {
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const Slot s = slot<P, T>(a, c, m, false);
+            const float2 DV = dmul(v[m], s.d * a.invN);
+            X[m] = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
+            v[m] = X[m];
+        }
+        to_phys<P, T>(a, v, buf, tw, t);
+#pragma unroll
+        for (int m = 0; m < P; ++m) x[m] = v[m];
+        return;
+    }
+    // ETRK2 stage 1: Zi = E X + phi1 (D V + S);  carry Y = Zi - phi2 D V
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const Slot s = slot<P, T>(a, c, m, true);
+        const float2 DV = dmul(v[m], s.d * a.invN);
+        const float2 Zi = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
+        X[m] = csub(Zi, cscale(DV, s.p2));
+        v[m] = Zi;
+    }
+    to_phys<P, T>(a, v, buf, tw, t);
+    if (xi) {
+#pragma unroll
+        for (int m = 0; m < P; ++m) (*xi)[m] = v[m];
+    }
+    // stage 2: X' = Y + phi2 D V2
+#pragma unroll
+    for (int m = 0; m < P; ++m) v[m] = sq2(v[m]);
+    to_spec<P, T>(a, v, buf, tw, t, false);
+#pragma unroll
+    for (int m = 0; m < P; ++m) {
+        const Slot s = slot<P, T>(a, c, m, true);
+        X[m] = cadd(X[m], cscale(dmul(v[m], s.d * a.invN), s.p2));
+        v[m] = X[m];
+    }
+    to_phys<P, T>(a, v, buf, tw, t);
+#pragma unroll
+    for (int m = 0; m < P; ++m) x[m] = v[m];
+}
+
+// Shared-memory carve-up: twiddles (N) then, per group, `per_group` float2.
+template <int P, int T>
+INC_DEV float2* group_smem(float2* sm, int per_group) {
+    constexpr int N = P * T;
+    return sm + N + (threadIdx.x / T) * per_group;
+}
+
+template <int P, int T>
+INC_DEV void load_twiddles(const Args& a, float2* sm) {
+    constexpr int N = P * T;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) sm[i] = a.tw[i];
+    __syncthreads();
+}
+
+template <int P, int T>
+__global__ void __launch_bounds__(128) k_step(Args a) {
+    extern __shared__ float2 sm[];
+    constexpr int N = P * T;
+    load_twiddles<P, T>(a, sm);
+    float2* buf = group_smem<P, T>(sm, N + 8);
+    const int t = threadIdx.x % T;
+    const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
+    Ctx c;
+    make_ctx(a, pair, t, pair < a.npairs, c);
+    float2 x[P], X[P], SS[P];
+    source_spec<P, T>(a, c, SS, buf, sm);
+    load_pair<P, T>(x, a.u, c, N);
+    if (a.cu) add_pair<P, T>(x, a.cu, c, N);  // u + correction_u, solver_1d.py:281/286
+#pragma unroll
+    for (int m = 0; m < P; ++m) X[m] = x[m];
+    to_spec<P, T>(a, X, buf, sm, t, true);
+#pragma unroll 1
+    for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, sm, nullptr);
+    store_pair<P, T>(a.out, x, c, N);
+}
+
+// Fused rollout of `steps` step() calls with s held constant.
+template <int P, int T>
+__global__ void __launch_bounds__(128) k_rollout(Args a) {
+    extern __shared__ float2 sm[];
+    constexpr int N = P * T;
+    load_twiddles<P, T>(a, sm);
+    float2* buf = group_smem<P, T>(sm, N + 8);
+    const int t = threadIdx.x % T;
+    const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
+    Ctx c;
+    make_ctx(a, pair, t, pair < a.npairs, c);
+    float2 x[P], X[P], SS[P];
+    source_spec<P, T>(a, c, SS, buf, sm);
+    load_pair<P, T>(x, a.u, c, N);
+    const int nseg = a.ckpt_every > 0 ? (a.steps + a.ckpt_every - 1) / a.ckpt_every : 0;
+#pragma unroll
+    for (int m = 0; m < P; ++m) X[m] = x[m];
+    to_spec<P, T>(a, X, buf, sm, t, true);
+    for (int k = 0; k < a.steps; ++k) {
+        if (a.ckpts && k % a.ckpt_every == 0)
+            store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)(k / a.ckpt_every) * N);
+#pragma unroll 1
+        for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, sm, nullptr);
+        if (a.frames) store_pair_strided<P, T>(a.frames, x, c, N, (int64_t)a.steps * N, (int64_t)k * N);
+    }
+    if (a.out) store_pair<P, T>(a.out, x, c, N);
+}
+
+// ---- adjoint ------------------------------------------------------------------
+// Per-group shared memory of the backward kernels, in lane layout [m][t]:
+//   st[0..3]: x0, xi1, x1, xi2 of the step being differentiated
+//   w2: scratch for the second-stage adjoint field
+INC_DEV int lidx(int T, int m, int t) { return m * T + t; }
+
+template <int P, int T>
+INC_DEV void st_put(float2* st, const float2 (&v)[P], int t) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) st[m * T + t] = v[m];
+}
+template <int P, int T>
+INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) v[m] = st[m * T + t];
+}
+
+// Backward of one step() from its input state x0 (physical, correction_u
+// already added).  G: scaled adjoint spectrum w.r.t. the step output (in),
+// w.r.t. the step input (out).  Sacc accumulates phi1-weighted adjoints whose
+// inverse FFT is dL/ds.
+template <int P, int T>
+INC_DEV void step_bwd(const Args& a, const Ctx& c, const float2 (&x0)[P], float2 (&G)[P], float2 (&Sacc)[P],
+                      const float2 (&SS)[P], float2* buf, const float2* tw, float2* st) {
+    constexpr int N = P * T;
+    const int t = c.t;
+    const bool rk2 = a.scheme == INC_KS_ETRK2;
+    // forward recompute: states at the start of each substep and the ETRK2 intermediates
+    {
+        float2 x[P], X[P], xi[P];
+#pragma unroll
+        for (int m = 0; m < P; ++m) { x[m] = x0[m]; X[m] = x0[m]; }
+        st_put<P, T>(st, x, t);
+        to_spec<P, T>(a, X, buf, tw, t, true);
+        substep<P, T>(a, c, x, X, SS, buf, tw, rk2 ? &xi : nullptr);
+        if (rk2) st_put<P, T>(st + N, xi, t);
+        st_put<P, T>(st + 2 * N, x, t);
+        if (rk2) {
+            // substep 2, stage 1 only (its intermediate state)
+            float2 v[P];
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
+            to_spec<P, T>(a, v, buf, tw, t, false);
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+                const Slot s = slot<P, T>(a, c, m, false);
+                const float2 DV = dmul(v[m], s.d * a.invN);
+                v[m] = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
+            }
+            to_phys<P, T>(a, v, buf, tw, t);
+            st_put<P, T>(st + 3 * N, v, t);
+        }
+    }
+    float2* w2s = st + 4 * N;
+#pragma unroll 1
+    for (int sub = 1; sub >= 0; --sub) {
+        const float2* xs = st + (sub == 0 ? 0 : 2 * N);
+        const float2* xis = st + (sub == 0 ? N : 3 * N);
+        float2 v[P], u[P];
+        if (rk2) {
+            // w2 = IFFT(d phi2 G)
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+                const Slot s = slot<P, T>(a, c, m, true);
+                v[m] = cscale(dmul(G[m], s.d), s.p2);
+            }
+            to_phys<P, T>(a, v, buf, tw, t);
+            st_put<P, T>(w2s, v, t);
+            // Gi = G - FFT(2 xi w2)/N
+            st_get<P, T>(u, xis, t);
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = make_float2(2.f * u[m].x * v[m].x, 2.f * u[m].y * v[m].y);
+            to_spec<P, T>(a, v, buf, tw, t, true);
+#pragma unroll
+            for (int m = 0; m < P; ++m) G[m] = csub(G[m], v[m]);
+        }
+        // w1 = IFFT(d phi1 Gi); Sacc += phi1 Gi
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const Slot s = slot<P, T>(a, c, m, false);
+            v[m] = cscale(dmul(G[m], s.d), s.p1);
+            Sacc[m] = cadd(Sacc[m], rmul(G[m], s.p1, s.p1b));
+        }
+        to_phys<P, T>(a, v, buf, tw, t);
+        // ETRK2: P1 = 2 x (w2 - w1);  ETD1: P1 = -2 x w1
+        st_get<P, T>(u, xs, t);
+        if (rk2) {
+            float2 w2[P];
+            st_get<P, T>(w2, w2s, t);
+#pragma unroll
+            for (int m = 0; m < P; ++m)
+                v[m] = make_float2(2.f * u[m].x * (w2[m].x - v[m].x), 2.f * u[m].y * (w2[m].y - v[m].y));
+        } else {
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = make_float2(-2.f * u[m].x * v[m].x, -2.f * u[m].y * v[m].y);
+        }
+        to_spec<P, T>(a, v, buf, tw, t, true);
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const Slot s = slot<P, T>(a, c, m, false);
+            G[m] = cadd(rmul(G[m], s.E, s.Eb), v[m]);
+        }
+    }
+}
+
+// Shared memory per group of the backward kernels: FFT buffer + 5 state slots.
+template <int P, int T>
+constexpr int bwd_group_smem() { return (P * T + 8) + 5 * P * T; }
+
+template <int P, int T>
+__global__ void __launch_bounds__(128) k_step_bwd(Args a) {
+    extern __shared__ float2 sm[];
+    constexpr int N = P * T;
+    load_twiddles<P, T>(a, sm);
+    float2* buf = group_smem<P, T>(sm, bwd_group_smem<P, T>());
+    float2* st = buf + N + 8;
+    const int t = threadIdx.x % T;
+    const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
+    Ctx c;
+    make_ctx(a, pair, t, pair < a.npairs, c);
+    float2 x0[P], G[P], Sacc[P], SS[P];
+    source_spec<P, T>(a, c, SS, buf, sm);
+    load_pair<P, T>(x0, a.u, c, N);
+    if (a.cu) add_pair<P, T>(x0, a.cu, c, N);
+    load_pair<P, T>(G, a.g_out, c, N);
+    to_spec<P, T>(a, G, buf, sm, t, true);
+#pragma unroll
+    for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
+    step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, sm, st);
+    to_phys<P, T>(a, G, buf, sm, t);
+    store_pair<P, T>(a.g_u, G, c, N);
+    if (a.g_s) {
+        to_phys<P, T>(a, Sacc, buf, sm, t);
+        store_pair<P, T>(a.g_s, Sacc, c, N);
+    }
+}
+
+// Backward of the fused rollout: segments of ckpt_every steps are replayed from
+// their checkpoint into shared memory, then differentiated step by step.
+template <int P, int T>
+__global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
+    extern __shared__ float2 sm[];
+    constexpr int N = P * T;
+    load_twiddles<P, T>(a, sm);
+    const int K = a.ckpt_every;
+    float2* buf = group_smem<P, T>(sm, bwd_group_smem<P, T>() + K * N);
+    float2* st = buf + N + 8;
+    float2* seg = st + 5 * N;
+    const int t = threadIdx.x % T;
+    const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
+    Ctx c;
+    make_ctx(a, pair, t, pair < a.npairs, c);
+    float2 G[P], Sacc[P], SS[P];
+    source_spec<P, T>(a, c, SS, buf, sm);
+    if (a.g_final) load_pair<P, T>(G, a.g_final, c, N);
+    else {
+#pragma unroll
+        for (int m = 0; m < P; ++m) G[m] = make_float2(0.f, 0.f);
+    }
+    to_spec<P, T>(a, G, buf, sm, t, true);
+#pragma unroll
+    for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
+    const int nseg = (a.steps + K - 1) / K;
+    for (int sidx = nseg - 1; sidx >= 0; --sidx) {
+        const int k0 = sidx * K;
+        const int len = min(K, a.steps - k0);
+        {
+            float2 x[P], X[P];
+            load_pair_strided<P, T>(x, a.ckpts, c, N, (int64_t)nseg * N, (int64_t)sidx * N);
+#pragma unroll
+            for (int m = 0; m < P; ++m) X[m] = x[m];
+            to_spec<P, T>(a, X, buf, sm, t, true);
+            for (int j = 0; j < len; ++j) {
+                st_put<P, T>(seg + j * N, x, t);
+                if (j + 1 < len) {
+#pragma unroll 1
+                    for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, sm, nullptr);
+                }
+            }
+        }
+        for (int j = len - 1; j >= 0; --j) {
+            const int k = k0 + j;
+            if (a.g_frames) {
+                float2 gf[P];
+                load_pair_strided<P, T>(gf, a.g_frames, c, N, (int64_t)a.steps * N, (int64_t)k * N);
+                to_spec<P, T>(a, gf, buf, sm, t, true);
+#pragma unroll
+                for (int m = 0; m < P; ++m) G[m] = cadd(G[m], gf[m]);
+            }
+            float2 x0[P];
+            st_get<P, T>(x0, seg + j * N, t);
+            step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, sm, st);
+        }
+    }
+    to_phys<P, T>(a, G, buf, sm, t);
+    store_pair<P, T>(a.g_u, G, c, N);
+    if (a.g_s) {
+        to_phys<P, T>(a, Sacc, buf, sm, t);
+        store_pair<P, T>(a.g_s, Sacc, c, N);
+    }
+}
+
+// ---- launchers (instantiated per shape in ks_{fwd,bwd}_*.cu) ---------------------
+enum class Kind { Step, Rollout, StepBwd, RolloutBwd };
+
+template <int P, int T>
+int launch_fwd(Kind kind, const Args& a, cudaStream_t st, int block);
+template <int P, int T>
+int launch_bwd(Kind kind, const Args& a, cudaStream_t st, int block);
+
+template <int P, int T>
+size_t smem_bytes(Kind kind, int block, int K) {
+    constexpr int N = P * T;
+    const int groups = block / T;
+    size_t per = (kind == Kind::Step || kind == Kind::Rollout) ? (N + 8)
+               : (kind == Kind::StepBwd ? bwd_group_smem<P, T>() : bwd_group_smem<P, T>() + (size_t)K * N);
+    return (N + groups * per) * sizeof(float2);
+}
+
+template <typename F>
+int launch_with_smem(F kernel, int grid, int block, size_t smem, cudaStream_t st, const Args& a) {
+    if (smem > 227 * 1024) {
+        set_error("ks: %zu bytes of shared memory needed (max 227 KB); lower ckpt_every", smem);
+        return INC_E_INVALID;
+    }
+    if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kernel<<<grid, block, smem, st>>>(a);
+    return check_launch("ks");
+}
+
+template <int P, int T>
+int launch_fwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
+    const int gpb = block / T;
+    const int grid = (a.npairs + gpb - 1) / gpb;
+    const size_t smem = smem_bytes<P, T>(kind, block, a.ckpt_every);
+    if (kind == Kind::Step) return launch_with_smem(k_step<P, T>, grid, block, smem, st, a);
+    return launch_with_smem(k_rollout<P, T>, grid, block, smem, st, a);
+}
+
+template <int P, int T>
+int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
+    const int gpb = block / T;
+    const int grid = (a.npairs + gpb - 1) / gpb;
+    const size_t smem = smem_bytes<P, T>(kind, block, a.ckpt_every);
+    if (kind == Kind::StepBwd) return launch_with_smem(k_step_bwd<P, T>, grid, block, smem, st, a);
+    return launch_with_smem(k_rollout_bwd<P, T>, grid, block, smem, st, a);
+}
+
+// (P, T) shapes: N = P*T with T | P.
+#define INC_KS_SHAPES(X) X(4, 4) X(8, 4) X(8, 8) X(16, 8) X(16, 16) X(32, 8) X(32, 16)
+
+}  // namespace ks
+}  // namespace inc

@@ -1,0 +1,192 @@
+/*
+ * inc_b200.h -- C ABI of the B200 (sm_100a) INC 1D hybrid time-stepper.
+ *
+ * One shared library, libinc_b200.so, exports these entry points.  They take
+ * plain device pointers, sizes and a cudaStream_t passed as `void*`; no torch
+ * or C++ types cross the boundary.  All arrays are FP32, row-major [rows][n],
+ * contiguous, on the device that is current for the calling thread.  Every
+ * call is asynchronous on `stream`, allocates nothing and synchronises
+ * nothing, and returns 0 on success or one of the INC_E* codes below; the
+ * message for the last failure on the calling thread is inc_last_error_string().
+ *
+ * Reference interfaces replaced (tum-pbs/INC, solvers/solver_1d.py):
+ *   weno_reconstruction(f, direction)             :4-42    -> inc_weno_reconstruct
+ *   BurgersSolverTorch.step(u)                    :181-195 -> inc_burgers_step
+ *     (calc_nonlinear_weno :129, calc_nonlinear_FDM :125, calc_linear :144,
+ *      _compute_source :104, _apply_corrections :116, forward Euler :192;
+ *      SSP-RK3 composed on the same right-hand side)
+ *   autograd backward through BurgersSolverTorch.step -> inc_burgers_step_bwd
+ *   BurgersSolverTorch.step_adaptive(u)           :148-179 -> inc_burgers_step_adaptive
+ *   simulate_rollout(model=None, BurgersSolverTorch) trainer/trainer_1d.py:154-183
+ *                                                  -> inc_burgers_rollout (+ _bwd)
+ *   KSSolverTorch.__init__ / calc_linear / etd coefficients :199-212, :235-267
+ *                                                  -> inc_ks_plan_size, inc_ks_plan_init
+ *   KSSolverTorch.step(u, L) = etrk2 / etd1        :280-288 -> inc_ks_step
+ *   autograd backward through KSSolverTorch.step   -> inc_ks_step_bwd
+ *   simulate_rollout(model=None, KSSolverTorch)    -> inc_ks_rollout (+ _bwd)
+ */
+#ifndef INC_B200_H
+#define INC_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes ------------------------------------------------------ */
+#define INC_OK              0
+#define INC_E_INVALID       1   /* bad argument: size, enum, null pointer    */
+#define INC_E_UNSUPPORTED   2   /* valid request the library has no kernel for */
+#define INC_E_LAUNCH        3   /* CUDA launch/config error                   */
+#define INC_E_NONFINITE     4   /* a kernel saw a non-finite state            */
+
+/* ---- enums ------------------------------------------------------------- */
+#define INC_TS_EULER        0   /* forward Euler (reference parity)          */
+#define INC_TS_SSPRK3       1   /* Shu-Osher SSP-RK3                          */
+#define INC_CONV_WENO       0   /* WENO5 + Lax-Friedrichs splitting          */
+#define INC_CONV_FDM        1   /* central 2nd-order  -u * du/dx             */
+#define INC_SRC_NONE        0   /* equation_type homogeneous / viscosity     */
+#define INC_SRC_LINEAR      1   /* equation_type linear: beta * u            */
+#define INC_SRC_FORCING     2   /* equation_type learning: sum_j A sin(...)   */
+#define INC_KS_ETRK2        0
+#define INC_KS_ETD1         1
+
+/* Burgers problem description (solver_1d.py:45-66 sim_params fields). */
+typedef struct inc_burgers_desc {
+    int32_t rows;            /* B                                           */
+    int32_t n;               /* cells per row, power of two in [8, 512]     */
+    int32_t scheme;          /* INC_TS_*                                    */
+    int32_t convection;      /* INC_CONV_*                                  */
+    int32_t source;          /* INC_SRC_*                                   */
+    int32_t forcing_terms;   /* J for INC_SRC_FORCING                       */
+    int32_t cells_per_thread;/* 0 = library default, else 4, 8 or 16        */
+    int32_t reserved;
+    float dx;                /* L / n                                       */
+    float dt;                /* used when dt_rows == NULL                   */
+    float nu;                /* used when nu_rows == NULL                   */
+    float beta;              /* used when beta_rows == NULL                 */
+    const float* nu_rows;    /* [rows] or NULL                               */
+    const float* dt_rows;    /* [rows] or NULL                               */
+    const float* beta_rows;  /* [rows] or NULL                               */
+    const float* forcing;    /* [rows][4][J]: A, omega, phi, 2*pi*l/L        */
+    const float* x;          /* [n] grid coordinates (forcing), or NULL      */
+} inc_burgers_desc;
+
+/* Ragged batch: rows of different n, nu, dt and dx, packed back to back. */
+typedef struct inc_burgers_ragged_desc {
+    int32_t rows;
+    int32_t scheme;          /* INC_TS_*                                    */
+    int32_t convection;      /* INC_CONV_*                                  */
+    int32_t warps_per_block; /* 0 = library default                          */
+    const int64_t* offsets;  /* [rows] first cell of each row in the packing */
+    const int32_t* n_rows;   /* [rows] powers of two in [8, 512]            */
+    const float* nu_rows;    /* [rows]                                       */
+    const float* dt_rows;    /* [rows]                                       */
+    const float* dx_rows;    /* [rows]                                       */
+    const int32_t* order;    /* [rows] processing order (longest first)      */
+} inc_burgers_ragged_desc;
+
+/* KS plan (solver_1d.py:199-212).  The caller fills the inputs, owns `dev`
+ * (inc_ks_plan_size() bytes of device memory) and calls inc_ks_plan_init once;
+ * the plan is then immutable and may be shared by any number of calls.      */
+typedef struct inc_ks_plan {
+    int32_t rows;            /* in: B                                        */
+    int32_t n;               /* in: power of two in [16, 512]                */
+    int32_t scheme;          /* in: INC_KS_*                                 */
+    int32_t dealias;         /* in: 0 = reference (no dealiasing), 1 = 2/3   */
+    int32_t threads_per_pair;/* in: 0 = library default                       */
+    int32_t npairs;          /* out: row pairs sharing one complex FFT        */
+    int32_t split;           /* out: 1 if a pair holds two domain sizes       */
+    int32_t reserved;
+    double dt;               /* in                                           */
+    void* dev;               /* in: device buffer                            */
+} inc_ks_plan;
+
+/* ---- library ------------------------------------------------------------ */
+int32_t     inc_version(void);               /* 10000*major + 100*minor + patch */
+const char* inc_last_error_string(void);
+
+/* ---- WENO5 reconstruction (solver_1d.py:4-42); direction 0=left 1=right - */
+int inc_weno_reconstruct(const float* f, float* out, int32_t rows, int32_t n,
+                         int32_t direction, void* stream);
+
+/* ---- Burgers ------------------------------------------------------------ */
+/* One step of size dt per row: u_out = S(u, s).  s (correction_s) may be NULL.
+ * t_rows [rows] (or NULL: t0 for every row) is the time at the step start,
+ * read only by INC_SRC_FORCING.                                              */
+int inc_burgers_step(const inc_burgers_desc* d, const float* u, const float* s,
+                     const float* t_rows, double t0, float* u_out, void* stream);
+
+/* Vector-Jacobian product of inc_burgers_step: given g_out = dL/du_out,
+ * writes g_u = dL/du and (if g_s != NULL) g_s = dL/ds.  u, s, t as passed to
+ * the forward step (SSP-RK3 replays its stages from them).                  */
+int inc_burgers_step_bwd(const inc_burgers_desc* d, const float* u, const float* s,
+                         const float* t_rows, double t0, const float* g_out,
+                         float* g_u, float* g_s, void* stream);
+
+/* `steps` fixed steps in one launch with the state held on chip.  s is held
+ * constant.  frames [rows][steps][n] (or NULL) receives every state after a
+ * step; u_final [rows][n] the last.  If ckpts != NULL the state at the start of
+ * every `ckpt_every`-step segment is stored in ckpts [rows][nseg][n],
+ * nseg = ceil(steps / ckpt_every), for inc_burgers_rollout_bwd.             */
+int inc_burgers_rollout(const inc_burgers_desc* d, const float* u0, const float* s,
+                        const float* t_rows, double t0, int32_t steps,
+                        float* frames, float* u_final, int32_t ckpt_every,
+                        float* ckpts, void* stream);
+
+/* Backward of inc_burgers_rollout from its checkpoints.  g_frames
+ * [rows][steps][n] and g_final [rows][n] may each be NULL (zero).           */
+int inc_burgers_rollout_bwd(const inc_burgers_desc* d, const float* ckpts,
+                            const float* s, const float* t_rows, double t0,
+                            int32_t steps, int32_t ckpt_every,
+                            const float* g_frames, const float* g_final,
+                            float* g_u0, float* g_s, void* stream);
+
+/* Adaptive-CFL Euler sub-stepping over one dt with the global max |u|
+ * (solver_1d.py:148-179), all on the device: no host synchronisation.  One
+ * CTA runs the whole batch (block barriers between substeps).  t_out [rows]
+ * (or NULL) receives t + sum(dt_local); substeps_out (device int32, or NULL)
+ * the substep count.  work is reserved and may be NULL.                     */
+int inc_burgers_step_adaptive(const inc_burgers_desc* d, float cfl,
+                              int32_t max_substeps, const float* u,
+                              const float* s, const float* t_rows, double t0,
+                              float* u_out, float* t_out, float* work,
+                              int32_t* substeps_out, void* stream);
+
+/* Ragged batch: every row advances `steps` steps in one persistent launch.
+ * queue: one device int32 of caller memory, zeroed by this call.            */
+int inc_burgers_ragged_rollout(const inc_burgers_ragged_desc* d,
+                               const float* u0, int32_t steps, float* u_final,
+                               int32_t* queue, int32_t grid_blocks, void* stream);
+
+/* ---- Kuramoto-Sivashinsky --------------------------------------------- */
+/* Bytes of device memory a plan needs.                                       */
+int64_t inc_ks_plan_size(int32_t rows, int32_t n);
+/* Pairs rows (equal domain sizes first), uploads the pairing, and computes
+ * exp(L dt), phi1, phi2 per row in FP64 on the GPU (stored FP32) and the FFT
+ * twiddles.  domain_size_host: [rows] on the host.  Synchronises `stream`
+ * before returning (set-up call; not for use inside stream capture).       */
+int inc_ks_plan_init(inc_ks_plan* plan, const float* domain_size_host, void* stream);
+
+/* One reference step() = two ETRK2 / ETD1 substeps.  s (correction_s) and cu
+ * (correction_u) may be NULL.                                                */
+int inc_ks_step(const inc_ks_plan* plan, const float* u, const float* s,
+                const float* cu, float* u_out, void* stream);
+/* Vector-Jacobian product of inc_ks_step (g_s may be NULL).                 */
+int inc_ks_step_bwd(const inc_ks_plan* plan, const float* u, const float* s,
+                    const float* cu, const float* g_out, float* g_u, float* g_s,
+                    void* stream);
+/* `steps` step() calls in one launch with s held constant; frames, u_final,
+ * ckpts as for inc_burgers_rollout.                                          */
+int inc_ks_rollout(const inc_ks_plan* plan, const float* u0, const float* s,
+                   int32_t steps, float* frames, float* u_final,
+                   int32_t ckpt_every, float* ckpts, void* stream);
+int inc_ks_rollout_bwd(const inc_ks_plan* plan, const float* ckpts, const float* s,
+                       int32_t steps, int32_t ckpt_every, const float* g_frames,
+                       const float* g_final, float* g_u0, float* g_s, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* INC_B200_H */

@@ -1,0 +1,69 @@
+"""The C-ABI library builds, loads without a GPU and exports every symbol of
+include/inc_b200.h; the ctypes structures match the C layout (CPU)."""
+import ctypes as C
+import os
+import re
+import subprocess
+
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+HEADER = os.path.join(ROOT, "include", "inc_b200.h")
+
+
+def header_functions():
+    text = open(HEADER).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(inc_[a-z0-9_]+)\s*\(", text)))
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from inc_b200 import build, _native
+    build.build()
+    return _native.lib()
+
+
+def test_header_lists_entry_points():
+    names = header_functions()
+    assert "inc_burgers_step" in names and "inc_ks_rollout_bwd" in names and len(names) >= 15
+
+
+def test_library_exports_every_declared_symbol(lib):
+    from inc_b200 import _native
+    out = subprocess.run(["nm", "-D", "--defined-only", _native.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r"\bT (inc_[a-z0-9_]+)\b", out))
+    missing = [n for n in header_functions() if n not in exported]
+    assert not missing, missing
+    assert set(_native.SIGNATURES) == set(header_functions())
+
+
+def test_version_and_error_string(lib):
+    assert lib.inc_version() == 100
+    assert isinstance(lib.inc_last_error_string(), bytes)
+
+
+def test_argument_checks_need_no_gpu(lib):
+    """Invalid descriptors are rejected on the host before any CUDA call."""
+    from inc_b200 import _native as nat
+    d = nat.BurgersDesc()
+    d.rows, d.n, d.dx = 0, 64, 0.1
+    assert lib.inc_burgers_step(C.byref(d), None, None, None, 0.0, None, None) == nat.INC_E_INVALID
+    d.rows, d.scheme = 2, 7
+    assert lib.inc_burgers_step(C.byref(d), None, None, None, 0.0, None, None) == nat.INC_E_INVALID
+    assert b"scheme" in lib.inc_last_error_string()
+    d.scheme, d.convection = 0, 5
+    assert lib.inc_burgers_step(C.byref(d), None, None, None, 0.0, None, None) == nat.INC_E_INVALID
+    assert b"Convection" in lib.inc_last_error_string()
+    assert lib.inc_weno_reconstruct(None, None, 1, 64, 0, None) == nat.INC_E_INVALID
+    assert lib.inc_ks_plan_size(4, 96) == -1
+    assert lib.inc_ks_plan_size(4, 64) > 0
+    p = nat.KSPlan()
+    assert lib.inc_ks_step(C.byref(p), None, None, None, None, None) == nat.INC_E_INVALID
+
+
+def test_struct_layouts():
+    from inc_b200 import _native as nat
+    assert C.sizeof(nat.BurgersDesc) == 8 * 4 + 4 * 4 + 5 * 8
+    assert C.sizeof(nat.KSPlan) == 8 * 4 + 8 + 8
+    assert C.sizeof(nat.BurgersRaggedDesc) == 4 * 4 + 6 * 8
