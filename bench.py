@@ -1,0 +1,633 @@
+#!/usr/bin/env python
+"""Benchmark of the INC 1D hybrid time-stepper on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload ks_plain|burgers_plain|burgers_batched]
+
+Metric: cell-steps/s (one grid point advanced by one reference step()).
+Default workload: the plain KS configuration - 1024 trajectories, N=256,
+L=64, dt=0.25, ETRK2, a constant seeded correction field s, 400 step() calls
+per rollout, all frames stored.  A bench "step" is one such rollout.
+
+Printed (rank 0, one JSON line):
+  value      - fused rollout (one launch for the whole rollout), inputs resident
+               in HBM, device-timed with CUDA events, max over ranks;
+  e2e        - the same through the public API (inc_b200.rollout.ks_rollout)
+               with the inputs copied from pinned host memory and the final
+               state copied back inside the timed region;
+  plain      - the same kernels one launch per step() (eager, and captured in
+               a CUDA graph), plus forward+backward numbers of both forms;
+  roofline   - the fused kernel's FP32 throughput against an FMA-loop peak
+               measured in this run;
+  cpu_baseline - the FP32 numpy port of the reference (oracle/) on the host
+               cores, on a bounded sample.
+Multi-GPU (torchrun): every rank runs the full workload on its own GPU (weak
+scaling, trajectories are independent, no data-path collective).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["ks_plain", "burgers_plain", "burgers_batched"], default="ks_plain")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
+    ap.add_argument("--profile", action="store_true", help="one small fused launch for ncu (no JSON)")
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------
+# CPU baseline: the oracle's FP32 numpy port of the reference, on a process
+# pool of all host cores (started with spawn before any CUDA call).
+# ----------------------------------------------------------------------------
+def _cpu_ks_worker(args):
+    import numpy as np
+    from oracle import ks as oks
+    u0, s, L, dt, steps, scheme = args
+    u = u0.astype(np.float32)
+    s = s.astype(np.float32)
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u = oks.step(u, [L] * u.shape[0], dt, scheme, s)
+    return time.perf_counter() - t0, u.shape[0] * u.shape[1] * steps
+
+
+def _cpu_burgers_worker(args):
+    import numpy as np
+    from oracle import burgers as ob
+    u0, N, L, nu, dt, steps, scheme = args
+    p = ob.BurgersParams(resolution=N, L=L, dt=dt, nu=np.float32(nu))
+    u, t = u0.astype(np.float32), 0.0
+    fn = ob.step_ssprk3 if scheme == "ssprk3" else ob.step_euler
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        u, t = fn(u, p, t)
+    return time.perf_counter() - t0, u.shape[0] * u.shape[1] * steps
+
+
+class CpuBaseline:
+    def __init__(self):
+        import multiprocessing as mp
+        self.cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+        self.pool = mp.get_context("spawn").Pool(self.cores)
+
+    def run(self, workload, cfg, steps):
+        """Wall time and cell-steps of `steps` steps of the whole batch, rows split over the pool."""
+        import numpy as np
+        chunks = np.array_split(np.arange(cfg["B"]), self.cores)
+        if workload == "ks_plain":
+            jobs = [(cfg["u0"][c], cfg["s"][c], cfg["L"], cfg["dt"], steps, cfg["scheme"]) for c in chunks if len(c)]
+            fn = _cpu_ks_worker
+        else:
+            jobs = [(cfg["u0"][c], cfg["N"], cfg["L"], cfg["nu"], cfg["dt"], steps, cfg["scheme"])
+                    for c in chunks if len(c)]
+            fn = _cpu_burgers_worker
+        t0 = time.perf_counter()
+        res = self.pool.map(fn, jobs)
+        wall = time.perf_counter() - t0
+        return wall, sum(r[1] for r in res)
+
+    def sample(self, workload, cfg, budget_s):
+        """(cell-steps/s, description) of a bounded sample of about budget_s seconds."""
+        self.run(workload, cfg, 1)  # worker start-up and imports
+        wall1, _ = self.run(workload, cfg, 1)  # calibration
+        steps = int(max(1, min(cfg["steps"], budget_s / max(wall1, 1e-3))))
+        wall, cells = self.run(workload, cfg, steps)
+        desc = (f"{cfg['B']} rows x {steps} of {cfg['steps']} steps, numpy FP32 port of the reference "
+                f"(oracle/), rows split over {self.cores} spawned processes")
+        return cells / wall, desc, steps
+
+    def close(self):
+        self.pool.terminate()
+
+
+# ----------------------------------------------------------------------------
+# GPU helpers
+# ----------------------------------------------------------------------------
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index):
+        self.path = tempfile.mktemp(suffix=".csv")
+        self.proc = None
+        self.dev = device_index
+
+    def __enter__(self):
+        try:
+            import torch
+            uuid = str(torch.cuda.get_device_properties(self.dev).uuid)
+            target = f"GPU-{uuid}" if not uuid.startswith("GPU-") else uuid
+        except Exception:
+            target = str(self.dev)
+        try:
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", target, f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.f, stderr=subprocess.DEVNULL)
+            time.sleep(0.3)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            self.proc.wait(timeout=10)
+            self.f.close()
+
+    def summary(self):
+        if self.proc is None or not os.path.exists(self.path):
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        rows = []
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                rows.append((float(parts[0]), float(parts[1]), parts[3:7]))
+            except ValueError:
+                continue
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for _, _, r in rows for i, v in enumerate(r) if v.lower().startswith("active")})
+        loaded = [r[0] for r in rows if r[0] > 0.5 * r[1]] or [r[0] for r in rows]
+        return {"sm_mhz": statistics.median(loaded), "sm_max_mhz": max(r[1] for r in rows),
+                "reasons": reasons, "samples": len(rows)}
+
+
+def event_time(fn, iters, flush=None):
+    """Per-iteration device times (ms) with CUDA events on the current stream."""
+    import torch
+    times = []
+    for _ in range(iters):
+        if flush is not None:
+            flush()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record()
+        fn()
+        b.record()
+        b.synchronize()
+        times.append(a.elapsed_time(b))
+    return times
+
+
+def fp32_peak_tflops(device):
+    """FP32 FMA throughput of this GPU, measured with inc_bench_fma."""
+    import torch
+    from inc_b200 import _native as nat
+    sms = torch.cuda.get_device_properties(device).multi_processor_count
+    blocks, iters = sms * 8, 4096
+    out = torch.empty(blocks * 256, device=device)
+
+    def run():
+        nat.check(nat.lib().inc_bench_fma(out.data_ptr(), blocks, iters, nat.stream_of(device)), "bench_fma")
+
+    run()
+    torch.cuda.synchronize()
+    best = min(event_time(run, 5))
+    flops = blocks * 256 * iters * 16 * 8 * 2
+    return flops / (best * 1e-3) / 1e12
+
+
+# ----------------------------------------------------------------------------
+# KS plain configuration
+# ----------------------------------------------------------------------------
+def bench_ks(args, dev, world):
+    import torch
+    from types import SimpleNamespace
+    from inc_b200.roofline import ks_flops_per_cell_step, plain_bytes_per_cell_step
+    from inc_b200.rollout import ks_rollout
+    from inc_b200.solvers import KSSolverTorch
+    from inc_b200.workloads import ks_plain_config
+
+    cfg = ks_plain_config()
+    B, N, steps, L, dt = cfg["B"], cfg["N"], cfg["steps"], cfg["L"], cfg["dt"]
+    cells = B * N * steps
+    ds = torch.full((B,), L, device=dev)
+    solver = KSSolverTorch(SimpleNamespace(resolution=N, dt=dt, device=dev, domain_size=ds,
+                                           alpha=torch.zeros(B, device=dev), time_scheme=cfg["scheme"]))
+    u0_h = torch.tensor(cfg["u0"], dtype=torch.float32).pin_memory()
+    s_h = torch.tensor(cfg["s"], dtype=torch.float32).pin_memory()
+    u0 = u0_h.to(dev)
+    s = s_h.to(dev)
+    plan = solver.plan_for(u0, ds)
+    frames = torch.empty(B, steps, N, device=dev)
+    flush_buf = torch.empty(256 * 2 ** 20 // 4, device=dev)  # 256 MB > 126 MB L2
+
+    def flush():
+        flush_buf.fill_(1.0)
+
+    # --- fused rollout (value) -------------------------------------------------
+    def fused():
+        plan.rollout(u0, s, steps, frames, None, 0, None)
+
+    for _ in range(args.warmup):
+        fused()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        t_fused = event_time(fused, args.steps, flush)
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    ms_fused = sum(t_fused) / len(t_fused)
+
+    # --- plain: one launch per step() (eager, and captured in a CUDA graph) -------
+    bufs = [torch.empty(B, N, device=dev) for _ in range(2)]
+    results = torch.empty(B, steps, N, device=dev)
+
+    def plain():
+        u = u0
+        for k in range(steps):
+            out = bufs[k & 1]
+            plan.step(u, s, None, out)
+            results[:, k] = out  # simulate_rollout's results[:, step] = u_next
+            u = out
+
+    for _ in range(args.warmup):
+        plain()
+    torch.cuda.synchronize()
+    t_plain = event_time(plain, max(2, args.steps // 2), flush)
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        plain()
+    torch.cuda.current_stream(dev).wait_stream(side)
+    with torch.cuda.graph(graph):
+        plain()
+    graph.replay()
+    torch.cuda.synchronize()
+    t_graph = event_time(graph.replay, max(2, args.steps // 2), flush)
+
+    # --- forward + backward (loss = sum(w * frames)) ---------------------------
+    K = 8
+    nseg = (steps + K - 1) // K
+    ckpts = torch.empty(B, nseg, N, device=dev)
+    g_frames = torch.randn(B, steps, N, device=dev, generator=torch.Generator(dev).manual_seed(5))
+    g_u0 = torch.empty(B, N, device=dev)
+    g_s = torch.empty(B, N, device=dev)
+
+    def fused_fb():
+        plan.rollout(u0, s, steps, frames, None, K, ckpts)
+        plan.rollout_bwd(ckpts, s, steps, K, g_frames, None, g_u0, g_s)
+
+    states = torch.empty(steps + 1, B, N, device=dev)
+    ga, gb, gsk = torch.empty(B, N, device=dev), torch.empty(B, N, device=dev), torch.empty(B, N, device=dev)
+
+    def plain_fb():
+        states[0].copy_(u0)
+        for k in range(steps):
+            plan.step(states[k], s, None, states[k + 1])
+        g_s.zero_()
+        ga.zero_()
+        for k in range(steps - 1, -1, -1):
+            ga.add_(g_frames[:, k])
+            plan.step_bwd(states[k], s, None, ga, gb, gsk)
+            g_s.add_(gsk)
+            ga.copy_(gb)
+
+    for _ in range(max(1, args.warmup)):
+        fused_fb()
+        plain_fb()
+    torch.cuda.synchronize()
+    t_ffb = event_time(fused_fb, max(2, args.steps // 2), flush)
+    t_pfb = event_time(plain_fb, 2, flush)
+
+    # --- e2e through the public API with host buffers -----------------------------
+    u_final_h = torch.empty(B, N).pin_memory()
+
+    def e2e():
+        u0_d = u0_h.to(dev, non_blocking=True)
+        s_d = s_h.to(dev, non_blocking=True)
+        fr = ks_rollout(solver, u0_d, steps, ds, s=s_d)
+        u_final_h.copy_(fr[:, -1], non_blocking=True)
+
+    with torch.no_grad():
+        for _ in range(args.warmup):
+            e2e()
+        torch.cuda.synchronize()
+        t_e2e = event_time(e2e, args.steps, flush)
+
+    # --- roofline of the fused kernel ------------------------------------------------
+    peak = fp32_peak_tflops(dev)
+    flops_cell = ks_flops_per_cell_step(N, cfg["scheme"])
+    achieved = flops_cell * cells / (ms_fused * 1e-3) / 1e12
+    plain_ms_step = sum(t_plain) / len(t_plain) / steps
+    times = dict(fused=ms_fused, plain=sum(t_plain) / len(t_plain), graph=sum(t_graph) / len(t_graph),
+                 fused_fb=sum(t_ffb) / len(t_ffb), plain_fb=sum(t_pfb) / len(t_pfb),
+                 e2e=sum(t_e2e) / len(t_e2e))
+    extra = dict(
+        flops_per_cell_step=flops_cell, peak=peak, achieved=achieved,
+        plain_hbm_gbs=plain_bytes_per_cell_step(True) * B * N / (plain_ms_step * 1e-3) / 1e9,
+        clocks=clk.summary(), h2d=2 * B * N * 4, d2h=B * N * 4, launches=args.steps,
+    )
+    return cfg, cells, times, extra
+
+
+# ----------------------------------------------------------------------------
+# Burgers plain configuration (N=128, B=32, SSP-RK3, 200 steps)
+# ----------------------------------------------------------------------------
+def bench_burgers_plain(args, dev, world):
+    import torch
+    from types import SimpleNamespace
+    from inc_b200.roofline import BURGERS_FLOPS, plain_bytes_per_cell_step
+    from inc_b200.rollout import burgers_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    from inc_b200.workloads import burgers_plain_config
+
+    cfg = burgers_plain_config()
+    B, N, steps = cfg["B"], cfg["N"], cfg["steps"]
+    cells = B * N * steps
+    sp = SimpleNamespace(resolution=N, dt=cfg["dt"], x=None, adaptive_CFL=None, L=cfg["L"], nu=cfg["nu"], device=dev,
+                         convection_term="WENO", equation_type="viscosity", batch_size=B, time_scheme=cfg["scheme"])
+    solver = BurgersSolverTorch(sp)
+    u0_h = torch.tensor(cfg["u0"], dtype=torch.float32).pin_memory()
+    u0 = u0_h.to(dev)
+    launch = solver.launch_for(u0)
+    frames = torch.empty(B, steps, N, device=dev)
+    flush_buf = torch.empty(256 * 2 ** 20 // 4, device=dev)
+
+    def flush():
+        flush_buf.fill_(1.0)
+
+    def fused():
+        launch.rollout(u0, None, steps, frames, None, 0, None)
+
+    for _ in range(args.warmup):
+        fused()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        t_fused = event_time(fused, args.steps, flush)
+    bufs = [torch.empty(B, N, device=dev) for _ in range(2)]
+
+    def plain():
+        u = u0
+        for k in range(steps):
+            out = bufs[k & 1]
+            launch.step(u, None, out)
+            frames[:, k] = out
+            u = out
+
+    for _ in range(args.warmup):
+        plain()
+    t_plain = event_time(plain, max(2, args.steps // 2), flush)
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        plain()
+    torch.cuda.current_stream(dev).wait_stream(side)
+    with torch.cuda.graph(graph):
+        plain()
+    graph.replay()
+    torch.cuda.synchronize()
+    t_graph = event_time(graph.replay, max(2, args.steps // 2), flush)
+    K = 8
+    ckpts = torch.empty(B, (steps + K - 1) // K, N, device=dev)
+    g_frames = torch.randn(B, steps, N, device=dev)
+    g_u0 = torch.empty(B, N, device=dev)
+
+    def fused_fb():
+        launch.rollout(u0, None, steps, frames, None, K, ckpts)
+        launch.rollout_bwd(ckpts, None, steps, K, g_frames, None, g_u0, None)
+
+    states = torch.empty(steps + 1, B, N, device=dev)
+    ga, gb = torch.empty(B, N, device=dev), torch.empty(B, N, device=dev)
+
+    def plain_fb():
+        states[0].copy_(u0)
+        for k in range(steps):
+            launch.step(states[k], None, states[k + 1])
+        ga.zero_()
+        for k in range(steps - 1, -1, -1):
+            ga.add_(g_frames[:, k])
+            launch.step_bwd(states[k], None, ga, gb, None)
+            ga.copy_(gb)
+
+    fused_fb()
+    plain_fb()
+    torch.cuda.synchronize()
+    t_ffb = event_time(fused_fb, max(2, args.steps // 2), flush)
+    t_pfb = event_time(plain_fb, 2, flush)
+    u_final_h = torch.empty(B, N).pin_memory()
+
+    def e2e():
+        u0_d = u0_h.to(dev, non_blocking=True)
+        fr = burgers_rollout(solver, u0_d, steps)
+        u_final_h.copy_(fr[:, -1], non_blocking=True)
+
+    with torch.no_grad():
+        for _ in range(args.warmup):
+            e2e()
+        t_e2e = event_time(e2e, args.steps, flush)
+    peak = fp32_peak_tflops(dev)
+    flops_cell = BURGERS_FLOPS[cfg["scheme"]]
+    ms_fused = sum(t_fused) / len(t_fused)
+    achieved = flops_cell * cells / (ms_fused * 1e-3) / 1e12
+    plain_ms_step = sum(t_plain) / len(t_plain) / steps
+    times = dict(fused=ms_fused, plain=sum(t_plain) / len(t_plain), graph=sum(t_graph) / len(t_graph),
+                 fused_fb=sum(t_ffb) / len(t_ffb), plain_fb=sum(t_pfb) / len(t_pfb), e2e=sum(t_e2e) / len(t_e2e))
+    extra = dict(flops_per_cell_step=flops_cell, peak=peak, achieved=achieved,
+                 plain_hbm_gbs=plain_bytes_per_cell_step(False) * B * N / (plain_ms_step * 1e-3) / 1e9,
+                 clocks=clk.summary(), h2d=B * N * 4, d2h=B * N * 4, launches=args.steps)
+    return cfg, cells, times, extra
+
+
+def bench_burgers_batched(args, dev, world):
+    import numpy as np
+    import torch
+    from inc_b200.batched import RaggedBurgers
+    from inc_b200.roofline import BURGERS_FLOPS
+    from inc_b200.workloads import burgers_batched_config
+
+    cfg = burgers_batched_config()
+    rb = RaggedBurgers(cfg["u0"], cfg["nu"], cfg["dt"], cfg["dx"], scheme=cfg["scheme"], device=dev)
+    steps = cfg["steps"]
+    cells = rb.total * steps
+    out = torch.empty_like(rb.u0)
+
+    def run():
+        rb.rollout(steps, out=out)
+
+    for _ in range(args.warmup):
+        run()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        t = event_time(run, args.steps)
+    u0_h = rb.u0.cpu().pin_memory()
+    out_h = torch.empty_like(u0_h).pin_memory()
+
+    def e2e():
+        u = u0_h.to(dev, non_blocking=True)
+        o = rb.rollout(steps, u0=u)
+        out_h.copy_(o, non_blocking=True)
+
+    for _ in range(args.warmup):
+        e2e()
+    t_e2e = event_time(e2e, args.steps)
+    peak = fp32_peak_tflops(dev)
+    ms = sum(t) / len(t)
+    flops_cell = BURGERS_FLOPS[cfg["scheme"]]
+    times = dict(fused=ms, e2e=sum(t_e2e) / len(t_e2e))
+    extra = dict(flops_per_cell_step=flops_cell, peak=peak, achieved=flops_cell * cells / (ms * 1e-3) / 1e12,
+                 clocks=clk.summary(), h2d=rb.total * 4, d2h=rb.total * 4, launches=args.steps)
+    cfg = dict(name="burgers_batched", B=cfg["rows"], N="64..512", steps=steps, scheme=cfg["scheme"])
+    return cfg, cells, times, extra
+
+
+# ----------------------------------------------------------------------------
+def reference_arm(args, rank, world):
+    """The reference's algorithm on the host cores (the oracle's numpy port)."""
+    if rank != 0:
+        return
+    from inc_b200.workloads import burgers_plain_config, ks_plain_config
+    cfg = ks_plain_config() if args.workload == "ks_plain" else burgers_plain_config()
+    cpu = CpuBaseline()
+    try:
+        cpu.run(args.workload, cfg, 1)  # worker start-up and imports
+        wall1, _ = cpu.run(args.workload, cfg, 1)
+        per_step = max(1, min(cfg["steps"], int(1.0 / max(wall1, 1e-3))))  # ~1 s of CPU work per bench step
+        for _ in range(args.warmup):
+            cpu.run(args.workload, cfg, per_step)
+        walls, cells = [], 0
+        for _ in range(args.steps):
+            w, c = cpu.run(args.workload, cfg, per_step)
+            walls.append(w)
+            cells = c
+    finally:
+        cpu.close()
+    v = cells / (sum(walls) / len(walls))
+    sample = (f"{cfg['B']} rows x {per_step} steps per bench step (of {cfg['steps']} in the workload), numpy FP32 "
+              f"port of the reference (oracle/), rows split over {cpu.cores} spawned processes")
+    line = {"metric": "cell-steps/s", "value": v, "unit": "cell-steps/s", "impl": "reference",
+            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1e3 * sum(walls) / len(walls), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": cfg["name"]},
+            "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cpu.cores, "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    args = parse_args()
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        reference_arm(args, rank, world)
+        return
+    cpu = None
+    if rank == 0 and not args.no_cpu_baseline and not args.profile:
+        cpu = CpuBaseline()  # spawned before any CUDA call
+    import torch
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
+                                             device_id=dev)
+    if args.profile:
+        from inc_b200.workloads import ks_plain_config  # noqa: F401
+        profile_small(dev)
+        return
+    fn = {"ks_plain": bench_ks, "burgers_plain": bench_burgers_plain, "burgers_batched": bench_burgers_batched}
+    cfg, cells, times, extra = fn[args.workload](args, dev, world)
+    # max over ranks of every device time
+    if world > 1:
+        keys = sorted(times)
+        t = torch.tensor([times[k] for k in keys], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        times = dict(zip(keys, t.tolist()))
+    total_cells = cells * world
+    rate = lambda ms: total_cells / (ms * 1e-3)  # noqa: E731
+    line = None
+    if rank == 0:
+        cpu_b = None
+        if cpu is not None and args.workload in ("ks_plain", "burgers_plain"):
+            v, desc, _ = cpu.sample(args.workload, cfg, args.cpu_seconds)
+            cpu_b = {"value": v, "unit": "cell-steps/s", "cores": cpu.cores, "kind": "port", "sample": desc}
+        if cpu is not None:
+            cpu.close()
+        clk = extra["clocks"]
+        line = {
+            "metric": "cell-steps/s", "value": rate(times["fused"]), "unit": "cell-steps/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": times["fused"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "steps_per_rollout": cfg["steps"],
+                       "scheme": cfg["scheme"], "l2": "flushed (256 MB write) before every timed iteration",
+                       "per_gpu": "full workload on every rank (trajectories are independent)"},
+            "e2e": {"value": rate(times["e2e"]), "unit": "cell-steps/s", "h2d_bytes_per_step": extra["h2d"],
+                    "d2h_bytes_per_step": extra["d2h"], "api": "inc_b200.rollout (fused launch)"},
+            "roofline": {"bound": "fp32", "achieved": extra["achieved"], "peak": extra["peak"], "unit": "TFLOP/s",
+                         "frac": extra["achieved"] / extra["peak"], "traffic": None,
+                         "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run",
+                         "flops_per_cell_step": extra["flops_per_cell_step"]},
+            "cpu_baseline": cpu_b,
+            "clocks": clk,
+            "gpu_launches": extra["launches"],
+        }
+        if "plain" in times:
+            line["plain"] = {
+                "eager_per_step": rate(times["plain"]), "graph_per_step": rate(times["graph"]),
+                "fwd_bwd_fused": rate(times["fused_fb"]), "fwd_bwd_per_step": rate(times["plain_fb"]),
+                "fused_over_eager": times["plain"] / times["fused"],
+                "fused_over_graph": times["graph"] / times["fused"],
+                "fwd_bwd_fused_over_per_step": times["plain_fb"] / times["fused_fb"],
+                "plain_step_hbm_gbs": extra.get("plain_hbm_gbs"),
+            }
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+
+
+def profile_small(dev):
+    """A small KS fused launch (B=512, 64 steps) for an ncu capture."""
+    import torch
+    from types import SimpleNamespace
+    from inc_b200.solvers import KSSolverTorch
+    from inc_b200.workloads import ks_plain_config
+    cfg = ks_plain_config(B=512, steps=64)
+    B, N = cfg["B"], cfg["N"]
+    ds = torch.full((B,), cfg["L"], device=dev)
+    solver = KSSolverTorch(SimpleNamespace(resolution=N, dt=cfg["dt"], device=dev, domain_size=ds,
+                                           alpha=torch.zeros(B, device=dev), time_scheme="ETRK2"))
+    u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=dev)
+    s = torch.tensor(cfg["s"], dtype=torch.float32, device=dev)
+    plan = solver.plan_for(u0, ds)
+    frames = torch.empty(B, cfg["steps"], N, device=dev)
+    for _ in range(2):
+        plan.rollout(u0, s, cfg["steps"], frames, None, 0, None)
+    u = torch.empty_like(u0)
+    plan.step(u0, s, None, u)
+    torch.cuda.synchronize()
+
+
+if __name__ == "__main__":
+    main()

@@ -70,6 +70,7 @@ SIGNATURES = {
     "inc_ks_rollout": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, C.c_int32, _vp, _vp, C.c_int32, _vp, _vp]),
     "inc_ks_rollout_bwd": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp,
                                      _vp]),
+    "inc_bench_fma": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp]),
 }
 
 _lib = None

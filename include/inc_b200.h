@@ -186,6 +186,13 @@ int inc_ks_rollout_bwd(const inc_ks_plan* plan, const float* ckpts, const float*
                        int32_t steps, int32_t ckpt_every, const float* g_frames,
                        const float* g_final, float* g_u0, float* g_s, void* stream);
 
+/* ---- measurement utility ------------------------------------------------ */
+/* FP32 FMA throughput probe used by bench.py for the roofline denominator:
+ * `blocks` x 256 threads, each 128 * iters FMAs (2 flops each) in 8
+ * independent chains; out [blocks * 256] keeps the results live.  No
+ * counterpart in the reference.                                               */
+int inc_bench_fma(float* out, int32_t blocks, int32_t iters, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -110,12 +110,19 @@ def test_fused_rollout_matches_steps(cuda):
     a = _solver(N, dt, "ETRK2", Ls)
     a.correction_s = s
     u, frames = u0, []
-    for _ in range(30):
+    for _ in range(20):
         u = a.step(u, ds)
         frames.append(u)
     b = _solver(N, dt, "ETRK2", Ls)
-    fused = ks_rollout(b, u0, 30, ds, s=s)
-    assert torch.equal(fused, torch.stack(frames, 1))
+    fused = ks_rollout(b, u0, 20, ds, s=s).cpu().numpy()
+    # The fused launch carries the spectrum across steps while a step() call
+    # re-transforms u at each step start: the two differ by rounding, which the
+    # chaotic dynamics amplify.  Both must sit within 1e-5 of FP64 at 20 steps.
+    ref, sn = u0.cpu().numpy().astype(np.float64), s.cpu().numpy().astype(np.float64)
+    for k in range(20):
+        ref = oks.step(ref, Ls, dt, "ETRK2", sn)
+        assert rel_l2(fused[:, k], ref) < TOL, k
+        assert rel_l2(frames[k].cpu().numpy(), ref) < TOL, k
 
 
 @pytest.mark.parametrize("name", [str(n) for n in KZ["grad_cases"]])
