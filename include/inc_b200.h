@@ -160,6 +160,29 @@ int inc_burgers_ragged_rollout(const inc_burgers_ragged_desc* d,
                                const float* u0, int32_t steps, float* u_final,
                                int32_t* queue, int32_t grid_blocks, void* stream);
 
+/* Forward rollout and its backward in one call, for callers that cannot
+ * allocate device memory while the op runs: a host framework that owns all
+ * device memory and forbids allocation inside a foreign-function call, or an
+ * application held to a fixed memory budget.  The checkpoints that the other
+ * pair (inc_burgers_rollout + inc_burgers_rollout_bwd) keeps in caller memory
+ * live here in a fixed 8 MiB array compiled into the library, of which every
+ * GPU that loads the library holds one copy until exit.  The call allocates
+ * nothing: the caller passes only inputs (u0, s, t, g_frames, g_final) and
+ * outputs (frames and u_final may be NULL; g_u0 required, g_s may be NULL).
+ * Limit: rows * ceil(steps / ckpt_every) * n <= INC_NOALLOC_CKPT_FLOATS, else
+ * INC_E_INVALID.  The first call on a device looks the array's device address
+ * up once (cudaGetSymbolAddress).  All calls share the one array, which keeps
+ * the last call's checkpoints; each call writes every checkpoint before it
+ * reads it, so nothing needs clearing, but calls that overlap on the GPU (on
+ * different streams) race on it.  No counterpart in the reference.          */
+#define INC_NOALLOC_CKPT_FLOATS (2 * 1024 * 1024)
+int inc_burgers_rollout_grad_noalloc(const inc_burgers_desc* d, const float* u0,
+                                     const float* s, const float* t_rows, double t0,
+                                     int32_t steps, int32_t ckpt_every,
+                                     const float* g_frames, const float* g_final,
+                                     float* frames, float* u_final, float* g_u0,
+                                     float* g_s, void* stream);
+
 /* ---- Kuramoto-Sivashinsky --------------------------------------------- */
 /* Bytes of device memory a plan needs.                                       */
 int64_t inc_ks_plan_size(int32_t rows, int32_t n);
