@@ -39,16 +39,22 @@ __global__ void k_coef(const float* __restrict__ dsz, float* __restrict__ coef, 
     }
 }
 
-// FFT twiddles in the layout of fft(): tw[(q + Q r) T + t] = exp(-2 pi i r (t + T q) / N).
+// FFT twiddles of the later Stockham passes in the layout of fft_later():
+// entry pi*N + (q*R + r)*T + t = exp(-2 pi i r k / (NS R)), k = (t + T q) % NS,
+// for the pass with index pi, span NS and radix R.  FP64, stored FP32.
 __global__ void k_twiddle(float2* tw, int n, int T) {
-    const int P = n / T, Q = P / T;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int t = i % T, m = i / T;
-        const int q = m % Q, r = m / Q;
-        const long long e = ((long long)r * (t + T * q)) % n;
-        double s, c;
-        sincospi(-2.0 * (double)e / (double)n, &s, &c);
-        tw[i] = make_float2((float)c, (float)s);
+    const int P = n / T;
+    int pi = 0;
+    for (int ns = P; ns < n; ns *= (P < n / ns ? P : n / ns), ++pi) {
+        const int R = P < n / ns ? P : n / ns;
+        const int Q = P / R;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < Q * R * T; i += gridDim.x * blockDim.x) {
+            const int t = i % T, r = (i / T) % R, q = i / (T * R);
+            const int k = (t + T * q) % ns;
+            double s, c;
+            sincospi(-2.0 * (double)r * (double)k / ((double)ns * (double)R), &s, &c);
+            tw[pi * n + i] = make_float2((float)c, (float)s);
+        }
     }
 }
 
@@ -64,29 +70,31 @@ inline Layout layout(int rows, int n) {
     int64_t off = 0;
     l.dR = off; off = align256(off + (int64_t)rows * 4);
     l.pairs = off; off = align256(off + (int64_t)((rows + 1) / 2) * 2 * 4);
-    l.tw = off; off = align256(off + (int64_t)n * 8);
+    l.tw = off; off = align256(off + (int64_t)4 * n * 8);  // <= 4 later FFT passes
     l.coef = off; off = align256(off + (int64_t)rows * 3 * nhp_of(n) * 4);
     l.L = off; off = align256(off + (int64_t)rows * 4);
     l.total = off;
     return l;
 }
 
+// Lanes per row pair: as many as the n allows (<= 32), for latency.
 inline int default_tpp(int n) {
     switch (n) {
         case 16: return 4;
-        case 32: return 4;
-        case 64: return 8;
-        case 128: return 8;
-        case 256: return 16;
-        default: return 16;
+        case 32: return 8;
+        case 64: return 16;
+        default: return 32;
     }
 }
 
+// The (P, T) shapes that have kernels (INC_KS_SHAPES).
 inline bool valid_shape(int n, int T) {
-    if (!is_pow2(n) || n < 16 || n > 512) return false;
-    if (!is_pow2(T) || T < 4 || T > 16) return false;
+    if (!is_pow2(n) || n < 16 || n > 512 || T <= 0 || n % T) return false;
     const int P = n / T;
-    return P <= 32 && P % T == 0;
+#define INC_HAS(PP, TT) if (P == PP && T == TT) return true;
+    INC_KS_SHAPES(INC_HAS)
+#undef INC_HAS
+    return false;
 }
 
 int fill_args(const inc_ks_plan* p, Args& a) {
@@ -107,13 +115,13 @@ int fill_args(const inc_ks_plan* p, Args& a) {
 int pick_block(Kind kind, int npairs, int T, int n, int K) {
     int block = 128;
     // keep >= 2 blocks per SM when the batch allows it
-    while (block > T && block > 32 && (int64_t)npairs * T / block < 2 * 148) block >>= 1;
-    if (block < 32) block = 32;
+    while (block > 32 && (int64_t)npairs * T / block < 2 * 148) block >>= 1;
     auto smem = [&](int b) {
         const int groups = b / T;
-        int64_t per = (kind == Kind::Step || kind == Kind::Rollout) ? (n + 8) : (n + 8) + 5 * n;
+        int64_t per = 2 * (n + 8);
+        if (kind == Kind::StepBwd || kind == Kind::RolloutBwd) per += 5 * n;
         if (kind == Kind::RolloutBwd) per += (int64_t)K * n;
-        return (int64_t)(n + groups * per) * 8;
+        return (int64_t)(4 * n + groups * per) * 8;
     };
     while (block > 32 && smem(block) > 100 * 1024) block >>= 1;
     return block;

@@ -1,4 +1,4 @@
-// Explicit instantiation of the KS bwd kernels for P=16 values per lane, T=8 lanes per row pair.
+// Explicit instantiation of the KS bwd kernels for P=4 values per lane, T=8 lanes per row pair.
 #include "ks_kernels.cuh"
 
 namespace inc {
@@ -8,7 +8,7 @@ template <int P, int T>
 int launch_bwd(Kind kind, const Args& a, cudaStream_t st, int block) {
     return launch_bwd_impl<P, T>(kind, a, st, block);
 }
-template int launch_bwd<16, 8>(Kind, const Args&, cudaStream_t, int);
+template int launch_bwd<4, 8>(Kind, const Args&, cudaStream_t, int);
 
 }  // namespace ks
 }  // namespace inc

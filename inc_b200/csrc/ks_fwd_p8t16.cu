@@ -1,4 +1,4 @@
-// Explicit instantiation of the KS fwd kernels for P=16 values per lane, T=8 lanes per row pair.
+// Explicit instantiation of the KS fwd kernels for P=8 values per lane, T=16 lanes per row pair.
 #include "ks_kernels.cuh"
 
 namespace inc {
@@ -8,7 +8,7 @@ template <int P, int T>
 int launch_fwd(Kind kind, const Args& a, cudaStream_t st, int block) {
     return launch_fwd_impl<P, T>(kind, a, st, block);
 }
-template int launch_fwd<16, 8>(Kind, const Args&, cudaStream_t, int);
+template int launch_fwd<8, 16>(Kind, const Args&, cudaStream_t, int);
 
 }  // namespace ks
 }  // namespace inc

@@ -108,36 +108,82 @@ INC_DEV void dft_reg(float2 (&v)[P]) {
     }
 }
 
-// Length-N (= P*T) forward FFT of a row pair held as z[t + T*m] in v[m]; same
-// layout out.  buf: N float2 of shared memory private to the group.
-// tw[(q + Q*r)*T + t] = exp(-2 pi i r (t + T q) / N) (Q = P/T).
-template <int P, int T>
-INC_DEV void fft_fwd(float2 (&v)[P], float2* buf, const float2* tw, int t) {
-    constexpr int Q = P / T;
-    dft_reg<P, false>(v);
+// ---- FFT -------------------------------------------------------------------------
+// Length-N (= P*T) FFT of a row pair held as z[t + T*m] in v[m] (same layout
+// out), as Stockham passes: pass 1 is a P-point DFT in registers; every later
+// pass (span NS, radix R = min(P, N/NS), P/R butterflies per lane) reads the
+// previous pass's output from shared memory, applies its twiddles, runs R-point
+// DFTs in registers and writes the next buffer -- or, in the last pass, the
+// registers.  Two buffers per group alternate, so one barrier per pass
+// suffices; indices are XOR-swizzled to spread shared-memory banks.
+INC_DEV constexpr int pass_radix(int P, int T, int ns) { return P < (P * T) / ns ? P : (P * T) / ns; }
+INC_DEV constexpr int num_later_passes(int P, int T) {
+    int n = 0;
+    for (int ns = P; ns < P * T; ns *= pass_radix(P, T, ns)) ++n;
+    return n;
+}
+// twiddle-table offset (in float2) of the pass with span ns
+INC_DEV constexpr int pass_index(int P, int T, int ns) {
+    int i = 0;
+    for (int x = P; x < ns; x *= pass_radix(P, T, x)) ++i;
+    return i;
+}
+INC_DEV int swz(int i) { return i ^ ((i >> 4) & 15); }
+
+template <int T>
+INC_DEV void group_sync() {
+    static_assert(T <= 32, "a row pair lives inside one warp");
     __syncwarp();
+}
+
+struct Buf {
+    float2* a;
+    float2* b;
+};
+
+template <int P, int T, int NS>
+INC_DEV void fft_later(float2 (&v)[P], float2* src, float2* dst, const float2* tw, int t) {
+    constexpr int N = P * T;
+    if constexpr (NS < N) {
+        constexpr int R = pass_radix(P, T, NS);
+        constexpr int Q = P / R;
+        constexpr bool LAST = NS * R == N;
+        const float2* twp = tw + pass_index(P, T, NS) * N;
+        group_sync<T>();
 #pragma unroll
-    for (int r = 0; r < P; ++r) buf[t * P + (r ^ t)] = v[r];
-    __syncwarp();
+        for (int q = 0; q < Q; ++q) {
+            const int j = t + T * q;
+            const int k = j % NS;
+            float2 w[R];
 #pragma unroll
-    for (int q = 0; q < Q; ++q) {
-        float2 w[T];
-        const int j = t + T * q;
+            for (int r = 0; r < R; ++r) {
+                float2 y = src[swz(j + r * (N / R))];
+                if (r > 0) y = cmul(y, twp[(q * R + r) * T + t]);
+                w[r] = y;
+            }
+            dft_reg<R, false>(w);
 #pragma unroll
-        for (int r = 0; r < T; ++r) {
-            float2 y = buf[r * P + (j ^ r)];
-            if (r > 0) y = cmul(y, tw[(q + Q * r) * T + t]);
-            w[r] = y;
+            for (int r = 0; r < R; ++r) {
+                if constexpr (LAST) v[q + Q * r] = w[r];
+                else dst[swz((j / NS) * NS * R + k + r * NS)] = w[r];
+            }
         }
-        dft_reg<T, false>(w);
-#pragma unroll
-        for (int r = 0; r < T; ++r) v[q + Q * r] = w[r];
+        if constexpr (!LAST) fft_later<P, T, NS * R>(v, dst, src, tw, t);
     }
+}
+
+template <int P, int T>
+INC_DEV void fft_fwd(float2 (&v)[P], Buf buf, const float2* tw, int t) {
+    dft_reg<P, false>(v);
+    group_sync<T>();  // the previous transform's last reads are done
+#pragma unroll
+    for (int r = 0; r < P; ++r) buf.a[swz(t * P + r)] = v[r];
+    fft_later<P, T, P>(v, buf.a, buf.b, tw, t);
 }
 
 // Unnormalised inverse FFT: conj(FFT(conj(v))).
 template <int P, int T>
-INC_DEV void fft_inv(float2 (&v)[P], float2* buf, const float2* tw, int t) {
+INC_DEV void fft_inv(float2 (&v)[P], Buf buf, const float2* tw, int t) {
 #pragma unroll
     for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
     fft_fwd<P, T>(v, buf, tw, t);
@@ -330,7 +376,7 @@ INC_DEV void load_pair_strided(float2 (&x)[P], const float* __restrict__ src, co
 // ---- the step -----------------------------------------------------------------
 // Forward FFT of physical v into scaled spectral storage (packed or split).
 template <int P, int T>
-INC_DEV void to_spec(const Args& a, float2 (&v)[P], float2* buf, const float2* tw, int t, bool scale) {
+INC_DEV void to_spec(const Args& a, float2 (&v)[P], Buf buf, const float2* tw, int t, bool scale) {
     fft_fwd<P, T>(v, buf, tw, t);
     if (scale) {
 #pragma unroll
@@ -341,7 +387,7 @@ INC_DEV void to_spec(const Args& a, float2 (&v)[P], float2* buf, const float2* t
 
 // Inverse FFT of scaled spectral storage into physical values.
 template <int P, int T>
-INC_DEV void to_phys(const Args& a, float2 (&v)[P], float2* buf, const float2* tw, int t) {
+INC_DEV void to_phys(const Args& a, float2 (&v)[P], Buf buf, const float2* tw, int t) {
     if (a.split) to_packed<P, T>(v, t);
     fft_inv<P, T>(v, buf, tw, t);
 }
@@ -350,7 +396,7 @@ INC_DEV float2 sq2(float2 x) { return make_float2(x.x * x.x, x.y * x.y); }
 
 // SS = phi1 * FFT(s) / N, held for the whole step (s enters stage 1 of each substep).
 template <int P, int T>
-INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], float2* buf, const float2* tw) {
+INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], Buf buf, const float2* tw) {
     if (!a.s) {
 #pragma unroll
         for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
@@ -369,7 +415,7 @@ INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], float2* b
 // If xi != nullptr (ETRK2) the intermediate physical state is also returned.
 template <int P, int T>
 INC_DEV void substep(const Args& a, const Ctx& c, float2 (&x)[P], float2 (&X)[P], const float2 (&SS)[P],
-                     float2* buf, const float2* tw, float2 (*xi)[P]) {
+                     Buf buf, const float2* tw, float2 (*xi)[P]) {
     const int t = c.t;
     float2 v[P];
 #pragma unroll
@@ -417,18 +463,117 @@ INC_DEV void substep(const Args& a, const Ctx& c, float2 (&x)[P], float2 (&X)[P]
     for (int m = 0; m < P; ++m) x[m] = v[m];
 }
 
-// Shared-memory carve-up: twiddles (N) then, per group, `per_group` float2.
+// ---- shared memory ----------------------------------------------------------------
+// Per CTA: the twiddle table of the later passes ((passes-1) * N float2), then
+// per group its two FFT buffers (N + 8 each; the 8-entry pad staggers the
+// groups of one warp across banks) and, for the backward kernels, state slots.
+template <int P, int T>
+INC_DEV constexpr int tw_size() { return num_later_passes(P, T) * P * T; }
+template <int P, int T>
+INC_DEV constexpr int fft_buf_size() { return 2 * (P * T + 8); }
+
 template <int P, int T>
 INC_DEV float2* group_smem(float2* sm, int per_group) {
-    constexpr int N = P * T;
-    return sm + N + (threadIdx.x / T) * per_group;
+    return sm + tw_size<P, T>() + (threadIdx.x / T) * per_group;
+}
+
+template <int P, int T>
+INC_DEV Buf group_buf(float2* g) {
+    return Buf{g, g + P * T + 8};
 }
 
 template <int P, int T>
 INC_DEV void load_twiddles(const Args& a, float2* sm) {
-    constexpr int N = P * T;
-    for (int i = threadIdx.x; i < N; i += blockDim.x) sm[i] = a.tw[i];
+    for (int i = threadIdx.x; i < tw_size<P, T>(); i += blockDim.x) sm[i] = a.tw[i];
     __syncthreads();
+}
+
+// ---- the forward program ------------------------------------------------------------
+// A rollout is a sequence of FFT phases: [FFT(s)] FFT(u), then per step() and
+// substep FFT(u^2) -> stage 1 -> IFFT -> [FFT(ui^2) -> stage 2 -> IFFT] (the
+// bracketed half for ETRK2).  Running them as one loop around a single FFT
+// keeps one copy of the transform in the kernel's code.
+enum Phase { PH_S, PH_U, PH_NL1, PH_NL2, PH_INV };
+
+template <int P, int T>
+INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, Buf buf, const float2* tw,
+                             bool frames_on, int nseg) {
+    constexpr int N = P * T;
+    const int t = c.t;
+    const bool rk2 = a.scheme == INC_KS_ETRK2;
+    const int per_sub = rk2 ? 4 : 2;
+    const int per_step = 2 * per_sub;
+    const int pro = a.s ? 2 : 1;
+    const int total = pro + steps * per_step;
+    float2 X[P], SS[P], v[P];
+#pragma unroll
+    for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
+#pragma unroll 1
+    for (int ph = 0; ph < total; ++ph) {
+        int kind, step = 0, q = 0;
+        if (ph < pro) {
+            kind = (ph == 0 && a.s) ? PH_S : PH_U;
+        } else {
+            q = ph - pro;
+            step = q / per_step;
+            const int f = (q % per_step) % per_sub;
+            kind = (f & 1) ? PH_INV : (f == 0 ? PH_NL1 : PH_NL2);
+            if (q % per_step == 0 && a.ckpts && step % a.ckpt_every == 0)
+                store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)(step / a.ckpt_every) * N);
+        }
+        // operand of this transform
+        if (kind == PH_S) {
+            load_pair<P, T>(v, a.s, c, N);
+        } else if (kind == PH_U) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = x[m];
+        } else if (kind != PH_INV) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
+        }
+        fft_fwd<P, T>(v, buf, tw, t);
+        if (kind == PH_INV) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) x[m] = make_float2(v[m].x, -v[m].y);
+            if (frames_on && (q % per_step) == per_step - 1)
+                store_pair_strided<P, T>(a.frames, x, c, N, (int64_t)a.steps * N, (int64_t)step * N);
+            continue;
+        }
+        if (a.split) to_split<P, T>(v, t);
+        if (kind == PH_S) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+                const Slot s = slot<P, T>(a, c, m, false);
+                SS[m] = rmul(cscale(v[m], a.invN), s.p1, s.p1b);
+            }
+            continue;
+        }
+        if (kind == PH_U) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) X[m] = cscale(v[m], a.invN);
+            continue;
+        }
+        if (kind == PH_NL1) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+                const Slot s = slot<P, T>(a, c, m, rk2);
+                const float2 DV = dmul(v[m], s.d * a.invN);
+                const float2 Zi = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
+                X[m] = rk2 ? csub(Zi, cscale(DV, s.p2)) : Zi;  // ETRK2 carries Y = Zi - phi2 D V
+                v[m] = Zi;
+            }
+        } else {  // PH_NL2: X' = Y + phi2 D V2
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+                const Slot s = slot<P, T>(a, c, m, true);
+                X[m] = cadd(X[m], cscale(dmul(v[m], s.d * a.invN), s.p2));
+                v[m] = X[m];
+            }
+        }
+        if (a.split) to_packed<P, T>(v, t);
+#pragma unroll
+        for (int m = 0; m < P; ++m) v[m].y = -v[m].y;  // the next transform is an inverse
+    }
 }
 
 template <int P, int T>
@@ -436,20 +581,15 @@ __global__ void __launch_bounds__(128) k_step(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
     load_twiddles<P, T>(a, sm);
-    float2* buf = group_smem<P, T>(sm, N + 8);
+    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
     const int t = threadIdx.x % T;
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
-    float2 x[P], X[P], SS[P];
-    source_spec<P, T>(a, c, SS, buf, sm);
+    float2 x[P];
     load_pair<P, T>(x, a.u, c, N);
     if (a.cu) add_pair<P, T>(x, a.cu, c, N);  // u + correction_u, solver_1d.py:281/286
-#pragma unroll
-    for (int m = 0; m < P; ++m) X[m] = x[m];
-    to_spec<P, T>(a, X, buf, sm, t, true);
-#pragma unroll 1
-    for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, sm, nullptr);
+    forward_program<P, T>(a, c, x, 1, buf, sm, false, 0);
     store_pair<P, T>(a.out, x, c, N);
 }
 
@@ -459,25 +599,15 @@ __global__ void __launch_bounds__(128) k_rollout(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
     load_twiddles<P, T>(a, sm);
-    float2* buf = group_smem<P, T>(sm, N + 8);
+    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
     const int t = threadIdx.x % T;
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
-    float2 x[P], X[P], SS[P];
-    source_spec<P, T>(a, c, SS, buf, sm);
+    float2 x[P];
     load_pair<P, T>(x, a.u, c, N);
     const int nseg = a.ckpt_every > 0 ? (a.steps + a.ckpt_every - 1) / a.ckpt_every : 0;
-#pragma unroll
-    for (int m = 0; m < P; ++m) X[m] = x[m];
-    to_spec<P, T>(a, X, buf, sm, t, true);
-    for (int k = 0; k < a.steps; ++k) {
-        if (a.ckpts && k % a.ckpt_every == 0)
-            store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)(k / a.ckpt_every) * N);
-#pragma unroll 1
-        for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, sm, nullptr);
-        if (a.frames) store_pair_strided<P, T>(a.frames, x, c, N, (int64_t)a.steps * N, (int64_t)k * N);
-    }
+    forward_program<P, T>(a, c, x, a.steps, buf, sm, a.frames != nullptr, nseg);
     if (a.out) store_pair<P, T>(a.out, x, c, N);
 }
 
@@ -504,7 +634,7 @@ INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
 // inverse FFT is dL/ds.
 template <int P, int T>
 INC_DEV void step_bwd(const Args& a, const Ctx& c, const float2 (&x0)[P], float2 (&G)[P], float2 (&Sacc)[P],
-                      const float2 (&SS)[P], float2* buf, const float2* tw, float2* st) {
+                      const float2 (&SS)[P], Buf buf, const float2* tw, float2* st) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
@@ -586,17 +716,18 @@ INC_DEV void step_bwd(const Args& a, const Ctx& c, const float2 (&x0)[P], float2
     }
 }
 
-// Shared memory per group of the backward kernels: FFT buffer + 5 state slots.
+// Shared memory per group of the backward kernels: FFT buffers + 5 state slots.
 template <int P, int T>
-constexpr int bwd_group_smem() { return (P * T + 8) + 5 * P * T; }
+INC_DEV constexpr int bwd_group_smem() { return fft_buf_size<P, T>() + 5 * P * T; }
 
 template <int P, int T>
 __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
     load_twiddles<P, T>(a, sm);
-    float2* buf = group_smem<P, T>(sm, bwd_group_smem<P, T>());
-    float2* st = buf + N + 8;
+    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>());
+    const Buf buf = group_buf<P, T>(g);
+    float2* st = g + fft_buf_size<P, T>();
     const int t = threadIdx.x % T;
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
@@ -626,8 +757,9 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     constexpr int N = P * T;
     load_twiddles<P, T>(a, sm);
     const int K = a.ckpt_every;
-    float2* buf = group_smem<P, T>(sm, bwd_group_smem<P, T>() + K * N);
-    float2* st = buf + N + 8;
+    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>() + K * N);
+    const Buf buf = group_buf<P, T>(g);
+    float2* st = g + fft_buf_size<P, T>();
     float2* seg = st + 5 * N;
     const int t = threadIdx.x % T;
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
@@ -695,9 +827,9 @@ template <int P, int T>
 size_t smem_bytes(Kind kind, int block, int K) {
     constexpr int N = P * T;
     const int groups = block / T;
-    size_t per = (kind == Kind::Step || kind == Kind::Rollout) ? (N + 8)
+    size_t per = (kind == Kind::Step || kind == Kind::Rollout) ? fft_buf_size<P, T>()
                : (kind == Kind::StepBwd ? bwd_group_smem<P, T>() : bwd_group_smem<P, T>() + (size_t)K * N);
-    return (N + groups * per) * sizeof(float2);
+    return (tw_size<P, T>() + groups * per) * sizeof(float2);
 }
 
 template <typename F>
@@ -729,8 +861,10 @@ int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     return launch_with_smem(k_rollout_bwd<P, T>, grid, block, smem, st, a);
 }
 
-// (P, T) shapes: N = P*T with T | P.
-#define INC_KS_SHAPES(X) X(4, 4) X(8, 4) X(8, 8) X(16, 8) X(16, 16) X(32, 8) X(32, 16)
+
+// (P, T) shapes: N = P*T, T <= 32 lanes per row pair, P <= 32 values per lane.
+#define INC_KS_SHAPES(X) \
+    X(4, 4) X(4, 8) X(4, 16) X(8, 8) X(4, 32) X(8, 16) X(8, 32) X(16, 16) X(16, 32) X(32, 16)
 
 }  // namespace ks
 }  // namespace inc
