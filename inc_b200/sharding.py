@@ -1,0 +1,63 @@
+"""Sharding of independent trajectories over ranks (one process per GPU).
+
+Trajectories never exchange data, so a batch splits by rows with no collective
+on the data path.  ``partition_rows`` balances rows by their work (n * steps for
+a ragged batch) with a deterministic longest-first greedy assignment, so every
+rank computes the same partition without communication.  ``gather_rows`` and
+``max_over_ranks`` are the only collectives: assembling results (optional) and
+the max-over-ranks of device times for benchmarking.
+"""
+from __future__ import annotations
+
+import heapq
+
+import torch
+
+
+def partition_rows(work, world: int):
+    """Row indices per rank, balanced by `work` (longest first onto the lightest rank).
+
+    Deterministic for a given `work`; returns `world` sorted index lists."""
+    if world <= 0:
+        raise ValueError("world must be positive")
+    work = [float(w) for w in work]
+    order = sorted(range(len(work)), key=lambda i: (-work[i], i))
+    heap = [(0.0, r) for r in range(world)]
+    parts = [[] for _ in range(world)]
+    for i in order:
+        load, r = heapq.heappop(heap)
+        parts[r].append(i)
+        heapq.heappush(heap, (load + work[i], r))
+    return [sorted(p) for p in parts]
+
+
+def contiguous_rows(rows: int, rank: int, world: int) -> range:
+    """The contiguous block of a uniform batch owned by `rank`."""
+    per, extra = divmod(rows, world)
+    start = rank * per + min(rank, extra)
+    return range(start, start + per + (1 if rank < extra else 0))
+
+
+def gather_rows(local: torch.Tensor, parts, rank: int, world: int, group=None) -> torch.Tensor:
+    """Reassemble a [rows, ...] tensor from every rank's rows (indices `parts`)."""
+    import torch.distributed as dist
+    width = max(len(p) for p in parts)
+    pad = torch.zeros((width,) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+    pad[: local.shape[0]] = local
+    bufs = [torch.empty_like(pad) for _ in range(world)]
+    dist.all_gather(bufs, pad, group=group)
+    rows = sum(len(p) for p in parts)
+    out = torch.empty((rows,) + tuple(local.shape[1:]), dtype=local.dtype, device=local.device)
+    for r, p in enumerate(parts):
+        if p:
+            out[torch.as_tensor(p, device=local.device)] = bufs[r][: len(p)]
+    return out
+
+
+def max_over_ranks(value: float, device=None, group=None) -> float:
+    import torch.distributed as dist
+    if not dist.is_available() or not dist.is_initialized():
+        return float(value)
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
+    return float(t.item())

@@ -62,7 +62,10 @@ class _BurgersLaunch:
         d.rows, d.n = rows, n
         d.scheme = _SCHEMES[solver.time_scheme]
         d.convection = nat.INC_CONV_WENO if p.convection_term == "WENO" else nat.INC_CONV_FDM
-        d.cells_per_thread = int(getattr(solver, "cells_per_thread", 0) or 0)
+        cpt = int(getattr(solver, "cells_per_thread", 0) or 0)
+        if cpt == 0:
+            cpt = solver._tuned_cpt(n, rows, dev)
+        d.cells_per_thread = cpt
         d.dx = float(solver.dx)
         d.dt = float(solver.dt)
         self.keep = []
@@ -185,6 +188,15 @@ class BurgersSolverTorch:
         self.cells_per_thread = int(getattr(sim_params, "cells_per_thread", 0) or 0)
         self._forcing_cache = None
         self._x_cache = None
+        self._cpt_cache = None
+
+    def _tuned_cpt(self, n, rows, dev):
+        """Cells per lane from the autotuner cache (0 = library default)."""
+        key = (n, rows, self.time_scheme, str(dev))
+        if self._cpt_cache is None or self._cpt_cache[0] != key:
+            from . import autotune
+            self._cpt_cache = (key, autotune.best_burgers(n, rows, self.time_scheme, dev))
+        return self._cpt_cache[1]
 
     # -- parameters packed for the kernels ------------------------------------
     def _forcing_pack(self, rows, dev):
@@ -419,8 +431,11 @@ class KSSolverTorch:
                tuple(vals))
         plan = self._plan_cache.get(key)
         if plan is None:
-            plan = KSPlan(rows, self.resolution, self.dt, scheme, vals, u.device, self.dealias,
-                          self.threads_per_pair)
+            tpp = self.threads_per_pair
+            if tpp == 0:
+                from . import autotune
+                tpp = autotune.best_ks(self.resolution, rows, scheme, u.device)
+            plan = KSPlan(rows, self.resolution, self.dt, scheme, vals, u.device, self.dealias, tpp)
             if len(self._plan_cache) > 16:
                 self._plan_cache.clear()
             self._plan_cache[key] = plan

@@ -1,0 +1,119 @@
+"""Host-side logic that needs no GPU: sharding over ranks (gloo, world size 2),
+autotuner cache, workload generators, roofline counts, solver argument errors."""
+import os
+import socket
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out_dir):
+    import torch.distributed as dist
+    from inc_b200.sharding import gather_rows, max_over_ranks, partition_rows
+    from inc_b200.workloads import burgers_batched_config
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    cfg = burgers_batched_config(rows=37, steps=5)
+    work = [int(n) * cfg["steps"] for n in cfg["n"]]
+    parts = partition_rows(work, world)
+    mine = parts[rank]
+    # each rank "computes" its rows: a row-dependent value standing in for the solver output
+    local = torch.tensor([[float(i), float(cfg["n"][i])] for i in mine], dtype=torch.float64)
+    full = gather_rows(local, parts, rank, world)
+    t = max_over_ranks(1.0 + rank)
+    torch.save({"full": full, "t": t, "parts": parts}, os.path.join(out_dir, f"rank{rank}.pt"))
+    dist.barrier()
+    dist.destroy_process_group()
+
+
+def test_sharding_gloo_world2(tmp_path):
+    world = 2
+    mp.spawn(_rank_main, args=(world, _free_port(), str(tmp_path)), nprocs=world, join=True)
+    from inc_b200.workloads import burgers_batched_config
+    cfg = burgers_batched_config(rows=37, steps=5)
+    res = [torch.load(tmp_path / f"rank{r}.pt") for r in range(world)]
+    for r in res:
+        assert r["t"] == 2.0                                    # max over ranks
+        assert torch.equal(r["full"][:, 0], torch.arange(37, dtype=torch.float64))
+        assert np.array_equal(r["full"][:, 1].numpy(), cfg["n"].astype(np.float64))
+    p = res[0]["parts"]
+    assert sorted(p[0] + p[1]) == list(range(37)) and res[1]["parts"] == p
+    loads = [sum(int(cfg["n"][i]) for i in q) for q in p]
+    assert max(loads) - min(loads) <= 512                      # within one largest row
+
+
+def test_partition_properties():
+    from inc_b200.sharding import contiguous_rows, partition_rows
+    w = [5, 1, 1, 1, 9, 3, 3, 2]
+    parts = partition_rows(w, 3)
+    assert sorted(sum(parts, [])) == list(range(8))
+    assert partition_rows(w, 3) == parts
+    assert [len(contiguous_rows(10, r, 3)) for r in range(3)] == [4, 3, 3]
+    assert list(contiguous_rows(10, 2, 3)) == [7, 8, 9]
+    with pytest.raises(ValueError):
+        partition_rows(w, 0)
+
+
+def test_autotune_cache_roundtrip(tmp_path, monkeypatch):
+    from inc_b200 import autotune
+    monkeypatch.setenv("INC_B200_AUTOTUNE_CACHE", str(tmp_path / "at.json"))
+    monkeypatch.setattr(autotune, "_cache", None)
+    assert autotune.bucket(1000) == 1024 and autotune.bucket(1024) == 1024 and autotune.bucket(1) == 1
+    assert autotune.ks_candidates(256) == [16, 32]
+    assert autotune.ks_candidates(16) == [4]
+    assert autotune.burgers_candidates(512) == [16]
+    assert autotune.burgers_candidates(128) == [4, 8, 16]
+    k = autotune.key("ks", 256, 1000, "ETRK2", None)
+    assert k.endswith("|ks|n256|b1024|ETRK2")
+    autotune._load()[k] = {"threads_per_pair": 16}
+    autotune._save()
+    monkeypatch.setattr(autotune, "_cache", None)
+    assert autotune.best_ks(256, 700, "ETRK2", None) == 16       # same bucket
+    assert autotune.best_ks(256, 5000, "ETRK2", None) == 0       # untuned: library default
+
+
+def test_workloads_are_seeded_and_shaped():
+    from inc_b200.workloads import (burgers_batched_config, burgers_plain_config, ks_diff_config,
+                                    ks_plain_config)
+    a, b = ks_plain_config(B=8), ks_plain_config(B=8)
+    assert np.array_equal(a["u0"], b["u0"]) and np.array_equal(a["s"], b["s"])
+    assert a["u0"].shape == (8, 256) and abs(a["s"].std() - 0.01) < 0.003
+    c = burgers_plain_config()
+    assert c["u0"].shape == (32, 128) and np.abs(c["u0"]).max() <= 2.5
+    r = burgers_batched_config(rows=64, steps=3)
+    assert set(np.unique(r["n"])) <= {64, 128, 256, 512} and r["nu"].min() >= 1e-3 and r["nu"].max() <= 5e-2
+    for u, n, dt, dx, nu in zip(r["u0"], r["n"], r["dt"], r["dx"], r["nu"]):
+        assert u.shape == (n,) and dt <= 0.4 * dx / np.abs(u).max() + 1e-15 and dt <= 0.4 * dx * dx / nu + 1e-15
+    assert ks_diff_config(B=4)["u0"].shape == (4, 512)
+
+
+def test_roofline_counts():
+    from inc_b200.roofline import BURGERS_FLOPS, ks_flops_per_cell_step
+    assert BURGERS_FLOPS["euler"] == 167 and BURGERS_FLOPS["ssprk3"] == 503
+    assert ks_flops_per_cell_step(256) == 184
+    assert ks_flops_per_cell_step(256, "ETD1") == 2 * (5 * 8 + 8)
+
+
+def test_solver_errors_without_gpu():
+    from inc_b200.solvers import BurgersSolverTorch, KSSolverTorch
+    base = dict(resolution=64, dt=0.01, x=None, adaptive_CFL=None, L=6.28, nu=0.01, device="cpu",
+                equation_type="viscosity", batch_size=2)
+    with pytest.raises(ValueError, match="Convection scheme not recognized"):
+        BurgersSolverTorch(SimpleNamespace(convection_term="upwind", **base))
+    with pytest.raises(ValueError):
+        BurgersSolverTorch(SimpleNamespace(convection_term="WENO", time_scheme="rk4", **base))
+    with pytest.raises(KeyError):
+        KSSolverTorch(SimpleNamespace(resolution=64, dt=0.1, device="cpu", domain_size=torch.ones(2),
+                                      alpha=torch.zeros(2), time_scheme="RK4"))
+    s = BurgersSolverTorch(SimpleNamespace(convection_term="WENO", **base))
+    with pytest.raises(ValueError, match="CUDA"):
+        s.step(torch.zeros(2, 64))                                  # no CPU path
