@@ -46,7 +46,8 @@ def parse_args():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["ks_plain", "burgers_plain", "burgers_batched"], default="ks_plain")
+    ap.add_argument("--workload", choices=["ks_plain", "burgers_plain", "burgers_batched", "burgers_diff", "ks_diff"],
+                    default="ks_plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--profile", action="store_true", help="one small fused launch for ncu (no JSON)")
@@ -221,12 +222,16 @@ def bench_ks(args, dev, world):
     from inc_b200.solvers import KSSolverTorch
     from inc_b200.workloads import ks_plain_config
 
+    from inc_b200 import autotune
     cfg = ks_plain_config()
     B, N, steps, L, dt = cfg["B"], cfg["N"], cfg["steps"], cfg["L"], cfg["dt"]
     cells = B * N * steps
+    tpp, tune_ms = autotune.tune_ks(N, B, cfg["scheme"], device=dev, L=L, dt=dt)  # outside the timed regions
+    cfg["layout"] = {"threads_per_pair": tpp, "autotune_ms_per_50_steps": tune_ms}
     ds = torch.full((B,), L, device=dev)
     solver = KSSolverTorch(SimpleNamespace(resolution=N, dt=dt, device=dev, domain_size=ds,
-                                           alpha=torch.zeros(B, device=dev), time_scheme=cfg["scheme"]))
+                                           alpha=torch.zeros(B, device=dev), time_scheme=cfg["scheme"],
+                                           threads_per_pair=tpp))
     u0_h = torch.tensor(cfg["u0"], dtype=torch.float32).pin_memory()
     s_h = torch.tensor(cfg["s"], dtype=torch.float32).pin_memory()
     u0 = u0_h.to(dev)
@@ -359,11 +364,15 @@ def bench_burgers_plain(args, dev, world):
     from inc_b200.solvers import BurgersSolverTorch
     from inc_b200.workloads import burgers_plain_config
 
+    from inc_b200 import autotune
     cfg = burgers_plain_config()
     B, N, steps = cfg["B"], cfg["N"], cfg["steps"]
     cells = B * N * steps
+    cpt, tune_ms = autotune.tune_burgers(N, B, cfg["scheme"], device=dev)  # outside the timed regions
+    cfg["layout"] = {"cells_per_thread": cpt, "autotune_ms_per_50_steps": tune_ms}
     sp = SimpleNamespace(resolution=N, dt=cfg["dt"], x=None, adaptive_CFL=None, L=cfg["L"], nu=cfg["nu"], device=dev,
-                         convection_term="WENO", equation_type="viscosity", batch_size=B, time_scheme=cfg["scheme"])
+                         convection_term="WENO", equation_type="viscosity", batch_size=B, time_scheme=cfg["scheme"],
+                         cells_per_thread=cpt)
     solver = BurgersSolverTorch(sp)
     u0_h = torch.tensor(cfg["u0"], dtype=torch.float32).pin_memory()
     u0 = u0_h.to(dev)
@@ -500,6 +509,89 @@ def bench_burgers_batched(args, dev, world):
 
 
 # ----------------------------------------------------------------------------
+# Differentiable rollouts with a corrector network in the loop
+# (Burgers + periodic CNN, KS + FNO): one training step = rollout, MSE loss,
+# backward through solver and network, Adam update.
+# ----------------------------------------------------------------------------
+def bench_diff(args, dev, world, which):
+    import torch
+    from types import SimpleNamespace
+    from inc_b200.correctors import FNO1D, PeriodicCNN1D
+    from inc_b200.rollout import simulate_rollout
+    from inc_b200.solvers import BurgersSolverTorch, KSSolverTorch
+    from inc_b200.workloads import burgers_diff_config, ks_diff_config
+
+    torch.manual_seed(0)
+    if which == "burgers_diff":
+        cfg = burgers_diff_config()
+        B, N, steps = cfg["B"], cfg["N"], cfg["steps"]
+        mk = lambda: BurgersSolverTorch(SimpleNamespace(  # noqa: E731
+            resolution=N, dt=cfg["dt"], x=None, adaptive_CFL=None, L=cfg["L"], nu=cfg["nu"], device=dev,
+            convection_term="WENO", equation_type="viscosity", batch_size=B, time_scheme=cfg["scheme"]))
+        net = PeriodicCNN1D(channels=32, kernel=5, layers=4).to(dev)
+        L = None
+    else:
+        cfg = ks_diff_config()
+        B, N, steps = cfg["B"], cfg["N"], cfg["steps"]
+        L = torch.full((B,), cfg["L"], device=dev)
+        mk = lambda: KSSolverTorch(SimpleNamespace(  # noqa: E731
+            resolution=N, dt=cfg["dt"], device=dev, domain_size=L, alpha=torch.zeros(B, device=dev),
+            time_scheme=cfg["scheme"]))
+        net = FNO1D(modes=16, width=64, layers=4).to(dev)
+    cells = B * N * steps
+    u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=dev)
+    with torch.no_grad():  # target: the uncorrected solver's trajectory
+        target, _ = simulate_rollout(None, mk(), u0, steps, None, L)
+        target = target + 0.01 * torch.randn_like(target)
+    opt = torch.optim.Adam(net.parameters(), lr=1e-4, capturable=True)
+
+    solver = mk()  # built once: a KS plan uploads its pairing (a host sync) when first used
+
+    def train_step(ckpt):
+        if which == "burgers_diff":
+            solver.t = 0.0
+        res, _ = simulate_rollout(net, solver, u0, steps, "INC", L, checkpoint_every=ckpt)
+        loss = torch.mean((res - target) ** 2)
+        loss.backward()
+        opt.step()
+        opt.zero_grad(set_to_none=False)
+        return loss
+
+    def forward_only():
+        with torch.no_grad():
+            simulate_rollout(net, solver, u0, steps, "INC", L)
+
+    for _ in range(args.warmup):
+        train_step(8)
+        train_step(None)
+        forward_only()
+    torch.cuda.synchronize()
+    with ClockSampler(dev.index) as clk:
+        t_ck = event_time(lambda: train_step(8), args.steps)
+    t_plain = event_time(lambda: train_step(None), args.steps)
+    t_fwd = event_time(forward_only, args.steps)
+    # the whole training step captured in one CUDA graph
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            train_step(8)
+    torch.cuda.current_stream(dev).wait_stream(side)
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        train_step(8)
+    graph.replay()
+    torch.cuda.synchronize()
+    t_graph = event_time(graph.replay, args.steps)
+    ms = lambda t: sum(t) / len(t)  # noqa: E731
+    times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck))
+    extra = dict(clocks=clk.summary(), h2d=0, d2h=4, launches=None)
+    cfg = dict(name=which, B=B, N=N, steps=steps, scheme=cfg["scheme"],
+               corrector=("PeriodicCNN1D(4x32ch,k5,GELU)" if which == "burgers_diff" else "FNO1D(4 layers,w64,16 modes)"))
+    return cfg, cells, times, extra
+
+
+# ----------------------------------------------------------------------------
 def reference_arm(args, rank, world):
     """The reference's algorithm on the host cores (the oracle's numpy port)."""
     if rank != 0:
@@ -556,6 +648,33 @@ def main():
         from inc_b200.workloads import ks_plain_config  # noqa: F401
         profile_small(dev)
         return
+    if args.workload in ("burgers_diff", "ks_diff"):
+        cfg, cells, times, extra = bench_diff(args, dev, world, args.workload)
+        if world > 1:
+            keys = sorted(times)
+            t = torch.tensor([times[k] for k in keys], device=dev, dtype=torch.float64)
+            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+            times = dict(zip(keys, t.tolist()))
+        if rank == 0:
+            if cpu is not None:
+                cpu.close()
+            tot = cells * world
+            print(json.dumps({
+                "metric": "cell-steps/s (fwd+bwd training step)", "value": tot / (times["fused"] * 1e-3),
+                "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+                "ms_per_step": times["fused"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+                "dtype": "f32", "data": "synthetic (seeded)",
+                "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "unroll": cfg["steps"],
+                           "scheme": cfg["scheme"], "corrector": cfg["corrector"], "checkpoint_every": 8,
+                           "value_is": "whole training step (rollout, loss, backward, Adam) in one CUDA graph"},
+                "eager": {"train_step_ckpt8": tot / (times["ckpt"] * 1e-3),
+                          "train_step_no_ckpt": tot / (times["plain"] * 1e-3),
+                          "forward_only": tot / (times["fwd"] * 1e-3)},
+                "clocks": extra["clocks"]}), flush=True)
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.destroy_process_group()
+        return
     fn = {"ks_plain": bench_ks, "burgers_plain": bench_burgers_plain, "burgers_batched": bench_burgers_batched}
     cfg, cells, times, extra = fn[args.workload](args, dev, world)
     # max over ranks of every device time
@@ -581,7 +700,8 @@ def main():
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "steps_per_rollout": cfg["steps"],
                        "scheme": cfg["scheme"], "l2": "flushed (256 MB write) before every timed iteration",
-                       "per_gpu": "full workload on every rank (trajectories are independent)"},
+                       "per_gpu": "full workload on every rank (trajectories are independent)",
+                       "layout": cfg.get("layout")},
             "e2e": {"value": rate(times["e2e"]), "unit": "cell-steps/s", "h2d_bytes_per_step": extra["h2d"],
                     "d2h_bytes_per_step": extra["d2h"], "api": "inc_b200.rollout (fused launch)"},
             "roofline": {"bound": "fp32", "achieved": extra["achieved"], "peak": extra["peak"], "unit": "TFLOP/s",

@@ -286,9 +286,75 @@ def make_ks():
     np.savez_compressed(os.path.join(OUT, "ks_golden.npz"), **out)
 
 
+def make_hybrid():
+    """A corrector network in the loop: s = net(u) before every reference step()
+    (trainer_1d.py:168-175), loss = MSE(frames, target), FP64 autograd."""
+    sys.path.insert(0, os.path.dirname(os.path.dirname(OUT)))
+    from inc_b200.correctors import FNO1D, PeriodicCNN1D
+    rng = np.random.default_rng(77)
+    out = {}
+    # Burgers, SSP-RK3 and Euler, with a periodic CNN corrector
+    for name, scheme in (("h_burgers_rk3", "rk3"), ("h_burgers_euler", "euler")):
+        torch.manual_seed(5)
+        B, N, steps = 3, 32, 3
+        net = PeriodicCNN1D(channels=4, kernel=5, layers=4)
+        p = burgers_params(rng, B, N, eq="viscosity", nu_rows=False)
+        solver = _FixedBurgers(p)
+        u0 = torch.from_numpy(sines_u0(rng, B, N)).requires_grad_(True)
+        target = torch.from_numpy(rng.standard_normal((B, steps, N)) * 0.3)
+        u, frames = u0, []
+        for _ in range(steps):
+            solver.correction_s = net(u)
+            u = solver.step_rk3(u) if scheme == "rk3" else solver.step(u)
+            frames.append(u)
+        loss = torch.mean((torch.stack(frames, 1) - target) ** 2)
+        params = list(net.parameters())
+        grads = torch.autograd.grad(loss, [u0] + params)
+        out.update(p_to_dict(f"{name}.", p))
+        out[f"{name}.scheme"] = scheme
+        out[f"{name}.u0"] = u0.detach().numpy()
+        out[f"{name}.target"] = target.numpy()
+        out[f"{name}.loss"] = np.float64(loss.item())
+        out[f"{name}.grad_u"] = grads[0].numpy()
+        for (pn, prm), g in zip(net.named_parameters(), grads[1:]):
+            out[f"{name}.param.{pn}"] = prm.detach().numpy()
+            out[f"{name}.pgrad.{pn}"] = g.numpy()
+    # KS ETRK2 with an FNO corrector taking the domain size
+    torch.manual_seed(6)
+    name = "h_ks"
+    B, N, steps, dt = 2, 32, 2, 0.2
+    Ls = [32.0, 40.0]
+    net = FNO1D(modes=4, width=8, layers=2)
+    ds = torch.tensor(Ls)
+    sp = SimpleNamespace(resolution=N, dt=dt, device="cpu", domain_size=ds, alpha=torch.zeros(B),
+                         time_scheme="ETRK2")
+    solver = KSSolverTorch(sp)
+    u0 = torch.from_numpy(np.stack([ks_u0(rng, 1, N, L)[0] for L in Ls])).requires_grad_(True)
+    target = torch.from_numpy(rng.standard_normal((B, steps, N)) * 0.3)
+    u, frames = u0, []
+    for _ in range(steps):
+        solver.correction_s = net(u, ds)
+        u = solver.step(u, ds)
+        frames.append(u)
+    loss = torch.mean((torch.stack(frames, 1) - target) ** 2)
+    grads = torch.autograd.grad(loss, [u0] + list(net.parameters()))
+    out[f"{name}.N"] = np.int64(N)
+    out[f"{name}.L"] = np.array(Ls)
+    out[f"{name}.dt"] = np.float64(dt)
+    out[f"{name}.u0"] = u0.detach().numpy()
+    out[f"{name}.target"] = target.numpy()
+    out[f"{name}.loss"] = np.float64(loss.item())
+    out[f"{name}.grad_u"] = grads[0].numpy()
+    for (pn, prm), g in zip(net.named_parameters(), grads[1:]):
+        out[f"{name}.param.{pn}"] = prm.detach().numpy()
+        out[f"{name}.pgrad.{pn}"] = g.numpy()
+    np.savez_compressed(os.path.join(OUT, "hybrid_golden.npz"), **out)
+
+
 if __name__ == "__main__":
     torch.set_default_dtype(torch.float64)
     make_burgers()
     make_ks()
-    for f in ("burgers_golden.npz", "ks_golden.npz"):
+    make_hybrid()
+    for f in ("burgers_golden.npz", "ks_golden.npz", "hybrid_golden.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
