@@ -522,6 +522,9 @@ def bench_diff(args, dev, world, which):
     from inc_b200.workloads import burgers_diff_config, ks_diff_config
 
     torch.manual_seed(0)
+    # FP32 throughout, the corrector included (cuDNN would otherwise run its convolutions in TF32)
+    torch.backends.cudnn.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = False
     if which == "burgers_diff":
         cfg = burgers_diff_config()
         B, N, steps = cfg["B"], cfg["N"], cfg["steps"]

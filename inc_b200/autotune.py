@@ -2,7 +2,7 @@
 
 The free kernel parameters are the row layout across lanes: cells per lane
 (Burgers, 4 / 8 / 16; rows are n / cells lanes wide) and lanes per row pair (KS,
-4..32).  Narrow layouts give more instruction-level parallelism per lane and win
+4..64).  Narrow layouts give more instruction-level parallelism per lane and win
 on large batches; wide layouts give more warps per row and win on small
 batches.  ``tune_burgers`` / ``tune_ks`` time every valid layout on the current
 GPU for one (kind, n, batch bucket, scheme) and store the winner; the solvers
@@ -23,8 +23,9 @@ import threading
 import torch
 
 BURGERS_CPT = (4, 8, 16)
-KS_TPP = (4, 8, 16, 32)
-KS_SHAPES = {(4, 4), (4, 8), (4, 16), (8, 8), (4, 32), (8, 16), (8, 32), (16, 16), (16, 32), (32, 16)}
+KS_TPP = (4, 8, 16, 32, 64)
+KS_SHAPES = {(4, 4), (4, 8), (4, 16), (8, 8), (4, 32), (8, 16), (8, 32), (16, 16), (16, 32), (32, 16),
+             (4, 64), (8, 64)}
 
 _lock = threading.Lock()
 _cache = None

@@ -83,7 +83,8 @@ inline int default_tpp(int n) {
         case 16: return 4;
         case 32: return 8;
         case 64: return 16;
-        default: return 32;
+        case 128: return 32;
+        default: return 64;
     }
 }
 
@@ -113,6 +114,7 @@ int fill_args(const inc_ks_plan* p, Args& a) {
 }
 
 int pick_block(Kind kind, int npairs, int T, int n, int K) {
+    if (T > 32) return T;  // a wide pair is the whole CTA
     int block = 128;
     // keep >= 2 blocks per SM when the batch allows it
     while (block > 32 && (int64_t)npairs * T / block < 2 * 148) block >>= 1;

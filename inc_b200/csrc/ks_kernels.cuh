@@ -115,25 +115,46 @@ INC_DEV void dft_reg(float2 (&v)[P]) {
 // previous pass's output from shared memory, applies its twiddles, runs R-point
 // DFTs in registers and writes the next buffer -- or, in the last pass, the
 // registers.  Two buffers per group alternate, so one barrier per pass
-// suffices; indices are XOR-swizzled to spread shared-memory banks.
+// suffices.  Shared indices are padded by one slot per 16 (padx), which
+// spreads the strided accesses over the banks and keeps every address a
+// per-lane base plus a compile-time constant.
 INC_DEV constexpr int pass_radix(int P, int T, int ns) { return P < (P * T) / ns ? P : (P * T) / ns; }
 INC_DEV constexpr int num_later_passes(int P, int T) {
     int n = 0;
     for (int ns = P; ns < P * T; ns *= pass_radix(P, T, ns)) ++n;
     return n;
 }
-// twiddle-table offset (in float2) of the pass with span ns
+// index of the later pass with span ns (0 for the first later pass)
 INC_DEV constexpr int pass_index(int P, int T, int ns) {
     int i = 0;
     for (int x = P; x < ns; x *= pass_radix(P, T, x)) ++i;
     return i;
 }
-INC_DEV int swz(int i) { return i ^ ((i >> 4) & 15); }
+// twiddles one lane applies in all later passes, and before the pass with span ns
+INC_DEV constexpr int lane_twiddles(int P, int T) {
+    int c = 0;
+    for (int ns = P; ns < P * T; ns *= pass_radix(P, T, ns)) c += (P / pass_radix(P, T, ns)) * (pass_radix(P, T, ns) - 1);
+    return c;
+}
+INC_DEV constexpr int lane_twiddle_offset(int P, int T, int ns) {
+    int c = 0;
+    for (int x = P; x < ns; x *= pass_radix(P, T, x)) c += (P / pass_radix(P, T, x)) * (pass_radix(P, T, x) - 1);
+    return c;
+}
+// a lane keeps its twiddles in registers when it needs at most 16
+template <int P, int T>
+INC_DEV constexpr bool twiddles_in_registers() { return lane_twiddles(P, T) <= 16; }
+template <int P, int T>
+INC_DEV constexpr int reg_twiddles() { return twiddles_in_registers<P, T>() ? lane_twiddles(P, T) : 1; }
+
+INC_DEV constexpr int padx(int i) { return i + (i >> 4); }
+template <int N>
+INC_DEV constexpr int buf_len() { return N + N / 16 + 8; }  // + 8 staggers the groups of a warp
 
 template <int T>
 INC_DEV void group_sync() {
-    static_assert(T <= 32, "a row pair lives inside one warp");
-    __syncwarp();
+    if constexpr (T <= 32) __syncwarp();
+    else __syncthreads();
 }
 
 struct Buf {
@@ -141,31 +162,61 @@ struct Buf {
     float2* b;
 };
 
+// Twiddles of the later passes: in registers (reg) or in the shared table (sm).
+template <int P, int T>
+struct Twiddles {
+    float2 reg[reg_twiddles<P, T>()];
+    const float2* sm;
+};
+
+template <int P, int T>
+INC_DEV void load_lane_twiddles(Twiddles<P, T>& tw, const float2* table, int t) {
+    constexpr int N = P * T;
+    if constexpr (twiddles_in_registers<P, T>()) {
+        int i = 0;
+#pragma unroll
+        for (int ns = P; ns < N; ns *= pass_radix(P, T, ns)) {
+            const int R = pass_radix(P, T, ns), Q = P / R, pi = pass_index(P, T, ns);
+#pragma unroll
+            for (int q = 0; q < Q; ++q)
+#pragma unroll
+                for (int r = 1; r < R; ++r) tw.reg[i++] = __ldg(table + pi * N + (q * R + r) * T + t);
+        }
+    }
+}
+
 template <int P, int T, int NS>
-INC_DEV void fft_later(float2 (&v)[P], float2* src, float2* dst, const float2* tw, int t) {
+INC_DEV void fft_later(float2 (&v)[P], float2* src, float2* dst, const Twiddles<P, T>& tw, int t) {
     constexpr int N = P * T;
     if constexpr (NS < N) {
         constexpr int R = pass_radix(P, T, NS);
         constexpr int Q = P / R;
         constexpr bool LAST = NS * R == N;
-        const float2* twp = tw + pass_index(P, T, NS) * N;
+        constexpr int TOFF = lane_twiddle_offset(P, T, NS);
+        const float2* twp = tw.sm + pass_index(P, T, NS) * N;
         group_sync<T>();
 #pragma unroll
         for (int q = 0; q < Q; ++q) {
             const int j = t + T * q;
-            const int k = j % NS;
+            const float2* rd = src + padx(j);
             float2 w[R];
 #pragma unroll
             for (int r = 0; r < R; ++r) {
-                float2 y = src[swz(j + r * (N / R))];
-                if (r > 0) y = cmul(y, twp[(q * R + r) * T + t]);
+                float2 y = rd[padx(r * (N / R))];
+                if (r > 0) {
+                    if constexpr (twiddles_in_registers<P, T>()) y = cmul(y, tw.reg[TOFF + q * (R - 1) + r - 1]);
+                    else y = cmul(y, twp[(q * R + r) * T + t]);
+                }
                 w[r] = y;
             }
             dft_reg<R, false>(w);
+            if constexpr (LAST) {
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                if constexpr (LAST) v[q + Q * r] = w[r];
-                else dst[swz((j / NS) * NS * R + k + r * NS)] = w[r];
+                for (int r = 0; r < R; ++r) v[q + Q * r] = w[r];
+            } else {
+                float2* wr = dst + padx((j / NS) * NS * R + (j % NS));
+#pragma unroll
+                for (int r = 0; r < R; ++r) wr[padx(r * NS)] = w[r];
             }
         }
         if constexpr (!LAST) fft_later<P, T, NS * R>(v, dst, src, tw, t);
@@ -173,17 +224,18 @@ INC_DEV void fft_later(float2 (&v)[P], float2* src, float2* dst, const float2* t
 }
 
 template <int P, int T>
-INC_DEV void fft_fwd(float2 (&v)[P], Buf buf, const float2* tw, int t) {
+INC_DEV void fft_fwd(float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t) {
     dft_reg<P, false>(v);
     group_sync<T>();  // the previous transform's last reads are done
+    float2* wr = buf.a + padx(t * P);
 #pragma unroll
-    for (int r = 0; r < P; ++r) buf.a[swz(t * P + r)] = v[r];
+    for (int r = 0; r < P; ++r) wr[padx(r)] = v[r];
     fft_later<P, T, P>(v, buf.a, buf.b, tw, t);
 }
 
 // Unnormalised inverse FFT: conj(FFT(conj(v))).
 template <int P, int T>
-INC_DEV void fft_inv(float2 (&v)[P], Buf buf, const float2* tw, int t) {
+INC_DEV void fft_inv(float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t) {
 #pragma unroll
     for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
     fft_fwd<P, T>(v, buf, tw, t);
@@ -194,25 +246,37 @@ INC_DEV void fft_inv(float2 (&v)[P], Buf buf, const float2* tw, int t) {
 // ---- mirror exchange: slot k <-> slot N-k --------------------------------------
 // Slot k = t + T*m.  Its mirror lives in lane (T-t)%T, register P-1-m (t != 0)
 // or in lane 0, register (P-m)%P (t == 0).
+// A group wider than a warp exchanges through `scratch` (N float2 of the
+// group's shared memory, free between transforms).
 template <int P, int T>
-INC_DEV void mirror(const float2 (&v)[P], float2 (&mv)[P], int t) {
-    float2 recv[P];
-    const int partner = (T - t) & (T - 1);
+INC_DEV void mirror(const float2 (&v)[P], float2 (&mv)[P], int t, float2* scratch) {
+    if constexpr (T <= 32) {
+        float2 recv[P];
+        const int partner = (T - t) & (T - 1);
 #pragma unroll
-    for (int m = 0; m < P; ++m) {
-        recv[m].x = shfl<T>(v[m].x, partner);
-        recv[m].y = shfl<T>(v[m].y, partner);
+        for (int m = 0; m < P; ++m) {
+            recv[m].x = shfl<T>(v[m].x, partner);
+            recv[m].y = shfl<T>(v[m].y, partner);
+        }
+#pragma unroll
+        for (int m = 0; m < P; ++m) mv[m] = (t != 0) ? recv[P - 1 - m] : v[(P - m) % P];
+    } else {
+        constexpr int N = P * T;
+        group_sync<T>();
+#pragma unroll
+        for (int m = 0; m < P; ++m) scratch[t + T * m] = v[m];
+        group_sync<T>();
+#pragma unroll
+        for (int m = 0; m < P; ++m) mv[m] = scratch[(N - (t + T * m)) & (N - 1)];
     }
-#pragma unroll
-    for (int m = 0; m < P; ++m) mv[m] = (t != 0) ? recv[P - 1 - m] : v[(P - m) % P];
 }
 
 // packed Z = FFT(a + i b)  ->  split (A in the lower half, B in the upper half)
 template <int P, int T>
-INC_DEV void to_split(float2 (&v)[P], int t) {
+INC_DEV void to_split(float2 (&v)[P], int t, float2* scratch) {
     constexpr int N = P * T;
     float2 mv[P];
-    mirror<P, T>(v, mv, t);
+    mirror<P, T>(v, mv, t, scratch);
 #pragma unroll
     for (int m = 0; m < P; ++m) {
         const int k = t + T * m;
@@ -224,10 +288,10 @@ INC_DEV void to_split(float2 (&v)[P], int t) {
 }
 
 template <int P, int T>
-INC_DEV void to_packed(float2 (&v)[P], int t) {
+INC_DEV void to_packed(float2 (&v)[P], int t, float2* scratch) {
     constexpr int N = P * T;
     float2 mv[P];
-    mirror<P, T>(v, mv, t);
+    mirror<P, T>(v, mv, t, scratch);
 #pragma unroll
     for (int m = 0; m < P; ++m) {
         const int k = t + T * m;
@@ -314,6 +378,47 @@ INC_DEV Slot slot(const Args& a, const Ctx& c, int m, bool need_p2) {
     return s;
 }
 
+// The multipliers of this lane's P slots, read once per launch and kept in
+// registers (P <= 8); larger lanes re-read them (L1-resident) per stage.
+template <int P, int T>
+struct SlotCache {
+    static constexpr bool ON = P <= 8;
+    static constexpr int M = ON ? P : 1;
+    float E[M], p1[M], p2[M], d[M];
+    float Eb[2], p1b[2], p2b[2];  // row b at slots 0 and N/2 (split storage)
+
+    INC_DEV void load(const Args& a, const Ctx& c) {
+        if constexpr (ON) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) {
+                const Slot s = slot<P, T>(a, c, m, true);
+                E[m] = s.E; p1[m] = s.p1; p2[m] = s.p2; d[m] = s.d;
+                if (m == 0 || m == P / 2) {
+                    const int i = m == 0 ? 0 : 1;
+                    Eb[i] = s.Eb; p1b[i] = s.p1b; p2b[i] = s.p2b;
+                }
+            }
+        }
+    }
+
+    INC_DEV Slot get(const Args& a, const Ctx& c, int m, bool need_p2) const {
+        if constexpr (ON) {
+            Slot s;
+            s.E = E[m]; s.p1 = p1[m]; s.p2 = p2[m]; s.d = d[m];
+            if (m == 0 || m == P / 2) {
+                const int i = m == 0 ? 0 : 1;
+                s.Eb = Eb[i]; s.p1b = p1b[i]; s.p2b = p2b[i];
+            } else {
+                s.Eb = s.E; s.p1b = s.p1; s.p2b = s.p2;
+            }
+            s.sp = false;
+            return s;
+        } else {
+            return slot<P, T>(a, c, m, need_p2);
+        }
+    }
+};
+
 // real multiplier (row a on .x, row b on .y at the special slots)
 INC_DEV float2 rmul(float2 z, float ma, float mb) { return make_float2(ma * z.x, mb * z.y); }
 // -i * d * z
@@ -376,19 +481,19 @@ INC_DEV void load_pair_strided(float2 (&x)[P], const float* __restrict__ src, co
 // ---- the step -----------------------------------------------------------------
 // Forward FFT of physical v into scaled spectral storage (packed or split).
 template <int P, int T>
-INC_DEV void to_spec(const Args& a, float2 (&v)[P], Buf buf, const float2* tw, int t, bool scale) {
+INC_DEV void to_spec(const Args& a, float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t, bool scale) {
     fft_fwd<P, T>(v, buf, tw, t);
     if (scale) {
 #pragma unroll
         for (int m = 0; m < P; ++m) v[m] = cscale(v[m], a.invN);
     }
-    if (a.split) to_split<P, T>(v, t);
+    if (a.split) to_split<P, T>(v, t, buf.a);
 }
 
 // Inverse FFT of scaled spectral storage into physical values.
 template <int P, int T>
-INC_DEV void to_phys(const Args& a, float2 (&v)[P], Buf buf, const float2* tw, int t) {
-    if (a.split) to_packed<P, T>(v, t);
+INC_DEV void to_phys(const Args& a, float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t) {
+    if (a.split) to_packed<P, T>(v, t, buf.a);
     fft_inv<P, T>(v, buf, tw, t);
 }
 
@@ -396,7 +501,7 @@ INC_DEV float2 sq2(float2 x) { return make_float2(x.x * x.x, x.y * x.y); }
 
 // SS = phi1 * FFT(s) / N, held for the whole step (s enters stage 1 of each substep).
 template <int P, int T>
-INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], Buf buf, const float2* tw) {
+INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], Buf buf, const Twiddles<P, T>& tw) {
     if (!a.s) {
 #pragma unroll
         for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
@@ -415,7 +520,7 @@ INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], Buf buf, 
 // If xi != nullptr (ETRK2) the intermediate physical state is also returned.
 template <int P, int T>
 INC_DEV void substep(const Args& a, const Ctx& c, float2 (&x)[P], float2 (&X)[P], const float2 (&SS)[P],
-                     Buf buf, const float2* tw, float2 (*xi)[P]) {
+                     Buf buf, const Twiddles<P, T>& tw, float2 (*xi)[P]) {
     const int t = c.t;
     float2 v[P];
 #pragma unroll
@@ -468,9 +573,9 @@ INC_DEV void substep(const Args& a, const Ctx& c, float2 (&x)[P], float2 (&X)[P]
 // per group its two FFT buffers (N + 8 each; the 8-entry pad staggers the
 // groups of one warp across banks) and, for the backward kernels, state slots.
 template <int P, int T>
-INC_DEV constexpr int tw_size() { return num_later_passes(P, T) * P * T; }
+INC_DEV constexpr int tw_size() { return twiddles_in_registers<P, T>() ? 0 : num_later_passes(P, T) * P * T; }
 template <int P, int T>
-INC_DEV constexpr int fft_buf_size() { return 2 * (P * T + 8); }
+INC_DEV constexpr int fft_buf_size() { return 2 * buf_len<P * T>(); }
 
 template <int P, int T>
 INC_DEV float2* group_smem(float2* sm, int per_group) {
@@ -479,13 +584,19 @@ INC_DEV float2* group_smem(float2* sm, int per_group) {
 
 template <int P, int T>
 INC_DEV Buf group_buf(float2* g) {
-    return Buf{g, g + P * T + 8};
+    return Buf{g, g + buf_len<P * T>()};
 }
 
+// The block's shared twiddle table (when lanes do not hold them in registers)
+// and this lane's register twiddles.
 template <int P, int T>
-INC_DEV void load_twiddles(const Args& a, float2* sm) {
+INC_DEV Twiddles<P, T> setup_twiddles(const Args& a, float2* sm, int t) {
     for (int i = threadIdx.x; i < tw_size<P, T>(); i += blockDim.x) sm[i] = a.tw[i];
     __syncthreads();
+    Twiddles<P, T> tw;
+    tw.sm = sm;
+    load_lane_twiddles<P, T>(tw, a.tw, t);
+    return tw;
 }
 
 // ---- the forward program ------------------------------------------------------------
@@ -496,8 +607,8 @@ INC_DEV void load_twiddles(const Args& a, float2* sm) {
 enum Phase { PH_S, PH_U, PH_NL1, PH_NL2, PH_INV };
 
 template <int P, int T>
-INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, Buf buf, const float2* tw,
-                             bool frames_on, int nseg) {
+INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, Buf buf,
+                             const Twiddles<P, T>& tw, bool frames_on, int nseg) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
@@ -506,6 +617,8 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
     const int pro = a.s ? 2 : 1;
     const int total = pro + steps * per_step;
     float2 X[P], SS[P], v[P];
+    SlotCache<P, T> cc;
+    cc.load(a, c);
 #pragma unroll
     for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
 #pragma unroll 1
@@ -539,11 +652,11 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
                 store_pair_strided<P, T>(a.frames, x, c, N, (int64_t)a.steps * N, (int64_t)step * N);
             continue;
         }
-        if (a.split) to_split<P, T>(v, t);
+        if (a.split) to_split<P, T>(v, t, buf.a);
         if (kind == PH_S) {
 #pragma unroll
             for (int m = 0; m < P; ++m) {
-                const Slot s = slot<P, T>(a, c, m, false);
+                const Slot s = cc.get(a, c, m, false);
                 SS[m] = rmul(cscale(v[m], a.invN), s.p1, s.p1b);
             }
             continue;
@@ -556,7 +669,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
         if (kind == PH_NL1) {
 #pragma unroll
             for (int m = 0; m < P; ++m) {
-                const Slot s = slot<P, T>(a, c, m, rk2);
+                const Slot s = cc.get(a, c, m, rk2);
                 const float2 DV = dmul(v[m], s.d * a.invN);
                 const float2 Zi = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
                 X[m] = rk2 ? csub(Zi, cscale(DV, s.p2)) : Zi;  // ETRK2 carries Y = Zi - phi2 D V
@@ -565,12 +678,12 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
         } else {  // PH_NL2: X' = Y + phi2 D V2
 #pragma unroll
             for (int m = 0; m < P; ++m) {
-                const Slot s = slot<P, T>(a, c, m, true);
+                const Slot s = cc.get(a, c, m, true);
                 X[m] = cadd(X[m], cscale(dmul(v[m], s.d * a.invN), s.p2));
                 v[m] = X[m];
             }
         }
-        if (a.split) to_packed<P, T>(v, t);
+        if (a.split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
         for (int m = 0; m < P; ++m) v[m].y = -v[m].y;  // the next transform is an inverse
     }
@@ -580,16 +693,16 @@ template <int P, int T>
 __global__ void __launch_bounds__(128) k_step(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
-    load_twiddles<P, T>(a, sm);
-    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
     const int t = threadIdx.x % T;
+    const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
+    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
     float2 x[P];
     load_pair<P, T>(x, a.u, c, N);
     if (a.cu) add_pair<P, T>(x, a.cu, c, N);  // u + correction_u, solver_1d.py:281/286
-    forward_program<P, T>(a, c, x, 1, buf, sm, false, 0);
+    forward_program<P, T>(a, c, x, 1, buf, tw, false, 0);
     store_pair<P, T>(a.out, x, c, N);
 }
 
@@ -598,16 +711,16 @@ template <int P, int T>
 __global__ void __launch_bounds__(128) k_rollout(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
-    load_twiddles<P, T>(a, sm);
-    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
     const int t = threadIdx.x % T;
+    const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
+    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
     float2 x[P];
     load_pair<P, T>(x, a.u, c, N);
     const int nseg = a.ckpt_every > 0 ? (a.steps + a.ckpt_every - 1) / a.ckpt_every : 0;
-    forward_program<P, T>(a, c, x, a.steps, buf, sm, a.frames != nullptr, nseg);
+    forward_program<P, T>(a, c, x, a.steps, buf, tw, a.frames != nullptr, nseg);
     if (a.out) store_pair<P, T>(a.out, x, c, N);
 }
 
@@ -634,7 +747,7 @@ INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
 // inverse FFT is dL/ds.
 template <int P, int T>
 INC_DEV void step_bwd(const Args& a, const Ctx& c, const float2 (&x0)[P], float2 (&G)[P], float2 (&Sacc)[P],
-                      const float2 (&SS)[P], Buf buf, const float2* tw, float2* st) {
+                      const float2 (&SS)[P], Buf buf, const Twiddles<P, T>& tw, float2* st) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
@@ -724,27 +837,27 @@ template <int P, int T>
 __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
-    load_twiddles<P, T>(a, sm);
+    const int t = threadIdx.x % T;
+    const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
     float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>());
     const Buf buf = group_buf<P, T>(g);
     float2* st = g + fft_buf_size<P, T>();
-    const int t = threadIdx.x % T;
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
     float2 x0[P], G[P], Sacc[P], SS[P];
-    source_spec<P, T>(a, c, SS, buf, sm);
+    source_spec<P, T>(a, c, SS, buf, tw);
     load_pair<P, T>(x0, a.u, c, N);
     if (a.cu) add_pair<P, T>(x0, a.cu, c, N);
     load_pair<P, T>(G, a.g_out, c, N);
-    to_spec<P, T>(a, G, buf, sm, t, true);
+    to_spec<P, T>(a, G, buf, tw, t, true);
 #pragma unroll
     for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
-    step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, sm, st);
-    to_phys<P, T>(a, G, buf, sm, t);
+    step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, tw, st);
+    to_phys<P, T>(a, G, buf, tw, t);
     store_pair<P, T>(a.g_u, G, c, N);
     if (a.g_s) {
-        to_phys<P, T>(a, Sacc, buf, sm, t);
+        to_phys<P, T>(a, Sacc, buf, tw, t);
         store_pair<P, T>(a.g_s, Sacc, c, N);
     }
 }
@@ -755,24 +868,24 @@ template <int P, int T>
 __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
-    load_twiddles<P, T>(a, sm);
+    const int t = threadIdx.x % T;
+    const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
     const int K = a.ckpt_every;
     float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>() + K * N);
     const Buf buf = group_buf<P, T>(g);
     float2* st = g + fft_buf_size<P, T>();
     float2* seg = st + 5 * N;
-    const int t = threadIdx.x % T;
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
     float2 G[P], Sacc[P], SS[P];
-    source_spec<P, T>(a, c, SS, buf, sm);
+    source_spec<P, T>(a, c, SS, buf, tw);
     if (a.g_final) load_pair<P, T>(G, a.g_final, c, N);
     else {
 #pragma unroll
         for (int m = 0; m < P; ++m) G[m] = make_float2(0.f, 0.f);
     }
-    to_spec<P, T>(a, G, buf, sm, t, true);
+    to_spec<P, T>(a, G, buf, tw, t, true);
 #pragma unroll
     for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
     const int nseg = (a.steps + K - 1) / K;
@@ -784,12 +897,12 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
             load_pair_strided<P, T>(x, a.ckpts, c, N, (int64_t)nseg * N, (int64_t)sidx * N);
 #pragma unroll
             for (int m = 0; m < P; ++m) X[m] = x[m];
-            to_spec<P, T>(a, X, buf, sm, t, true);
+            to_spec<P, T>(a, X, buf, tw, t, true);
             for (int j = 0; j < len; ++j) {
                 st_put<P, T>(seg + j * N, x, t);
                 if (j + 1 < len) {
 #pragma unroll 1
-                    for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, sm, nullptr);
+                    for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, tw, nullptr);
                 }
             }
         }
@@ -798,19 +911,19 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
             if (a.g_frames) {
                 float2 gf[P];
                 load_pair_strided<P, T>(gf, a.g_frames, c, N, (int64_t)a.steps * N, (int64_t)k * N);
-                to_spec<P, T>(a, gf, buf, sm, t, true);
+                to_spec<P, T>(a, gf, buf, tw, t, true);
 #pragma unroll
                 for (int m = 0; m < P; ++m) G[m] = cadd(G[m], gf[m]);
             }
             float2 x0[P];
             st_get<P, T>(x0, seg + j * N, t);
-            step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, sm, st);
+            step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, tw, st);
         }
     }
-    to_phys<P, T>(a, G, buf, sm, t);
+    to_phys<P, T>(a, G, buf, tw, t);
     store_pair<P, T>(a.g_u, G, c, N);
     if (a.g_s) {
-        to_phys<P, T>(a, Sacc, buf, sm, t);
+        to_phys<P, T>(a, Sacc, buf, tw, t);
         store_pair<P, T>(a.g_s, Sacc, c, N);
     }
 }
@@ -864,7 +977,7 @@ int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
 
 // (P, T) shapes: N = P*T, T <= 32 lanes per row pair, P <= 32 values per lane.
 #define INC_KS_SHAPES(X) \
-    X(4, 4) X(4, 8) X(4, 16) X(8, 8) X(4, 32) X(8, 16) X(8, 32) X(16, 16) X(16, 32) X(32, 16)
+    X(4, 4) X(4, 8) X(4, 16) X(8, 8) X(4, 32) X(8, 16) X(8, 32) X(16, 16) X(16, 32) X(32, 16) X(4, 64) X(8, 64)
 
 }  // namespace ks
 }  // namespace inc

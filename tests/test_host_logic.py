@@ -68,7 +68,7 @@ def test_autotune_cache_roundtrip(tmp_path, monkeypatch):
     monkeypatch.setenv("INC_B200_AUTOTUNE_CACHE", str(tmp_path / "at.json"))
     monkeypatch.setattr(autotune, "_cache", None)
     assert autotune.bucket(1000) == 1024 and autotune.bucket(1024) == 1024 and autotune.bucket(1) == 1
-    assert autotune.ks_candidates(256) == [16, 32]
+    assert autotune.ks_candidates(256) == [16, 32, 64]
     assert autotune.ks_candidates(16) == [4]
     assert autotune.burgers_candidates(512) == [16]
     assert autotune.burgers_candidates(128) == [4, 8, 16]

@@ -12,10 +12,29 @@ import pytest
 import torch
 
 from oracle import burgers as ob
-from tests.golden_io import burgers_case, load, rel_l2
+from tests.golden_io import load, rel_l2
 
 pytestmark = pytest.mark.gpu
 HZ = load("hybrid_golden.npz")
+
+
+@pytest.fixture(autouse=True)
+def fp32_corrector():
+    """Keep the corrector's convolutions and matmuls in FP32 (cuDNN defaults to TF32)."""
+    saved = (torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32)
+    torch.backends.cudnn.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = False
+    yield
+    torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32 = saved
+
+
+def _hybrid_burgers(name):
+    g = lambda k: HZ[f"{name}.{k}"]  # noqa: E731
+    nu = g("nu")
+    p = ob.BurgersParams(resolution=int(g("N")), L=float(g("L")), dt=float(g("dt")),
+                         nu=(nu if nu.ndim else float(nu)), convection_term=str(g("conv")),
+                         equation_type=str(g("eq")))
+    return p, g("u0"), str(g("scheme"))
 
 
 def _net_from_golden(name, net):
@@ -36,7 +55,7 @@ def test_burgers_cnn_gradients_vs_reference(cuda, name, ckpt):
     from inc_b200.correctors import PeriodicCNN1D
     from inc_b200.rollout import simulate_rollout
     from inc_b200.solvers import BurgersSolverTorch
-    p, u0, _, _, scheme = burgers_case(HZ, name)
+    p, u0, scheme = _hybrid_burgers(name)
     B, N = u0.shape
     net = _net_from_golden(name, PeriodicCNN1D(channels=4, kernel=5, layers=4)).to(cuda).float()
     sp = SimpleNamespace(resolution=N, dt=p.dt, x=None, adaptive_CFL=None, L=p.L, nu=p.nu, device=cuda,

@@ -46,8 +46,8 @@ def test_golden_steps(cuda, name):
         assert rel_l2(u.cpu().numpy(), frames[:, k]) < TOL, (name, k)
 
 
-@pytest.mark.parametrize("N,tpp", [(16, 4), (32, 8), (64, 16), (64, 8), (128, 32), (128, 16), (256, 32), (256, 16),
-                                   (512, 32), (512, 16)])
+@pytest.mark.parametrize("N,tpp", [(16, 4), (32, 8), (64, 16), (64, 8), (128, 32), (128, 16), (256, 64), (256, 32),
+                                   (256, 16), (512, 64), (512, 32), (512, 16)])
 @pytest.mark.parametrize("mixed", [False, True])
 def test_shapes_vs_oracle(cuda, N, tpp, mixed):
     B = 7  # odd: one lone row
