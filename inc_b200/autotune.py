@@ -1,7 +1,7 @@
 """Kernel-shape autotuner for the Burgers and KS kernels.
 
 The free kernel parameters are the row layout across lanes: cells per lane
-(Burgers, 4 / 8 / 16; rows are n / cells lanes wide) and lanes per row pair (KS,
+(Burgers, 1 / 2 with one row per CTA, or 4 / 8 / 16 with a row inside a warp) and lanes per row pair (KS,
 4..64).  Narrow layouts give more instruction-level parallelism per lane and win
 on large batches; wide layouts give more warps per row and win on small
 batches.  ``tune_burgers`` / ``tune_ks`` time every valid layout on the current
@@ -22,7 +22,7 @@ import threading
 
 import torch
 
-BURGERS_CPT = (4, 8, 16)
+BURGERS_CPT = (1, 2, 4, 8, 16)
 KS_TPP = (4, 8, 16, 32, 64)
 KS_SHAPES = {(4, 4), (4, 8), (4, 16), (8, 8), (4, 32), (8, 16), (8, 32), (16, 16), (16, 32), (32, 16),
              (4, 64), (8, 64)}
@@ -81,7 +81,19 @@ def key(kind: str, n: int, rows: int, scheme: str, device=None) -> str:
 
 
 def burgers_candidates(n: int):
-    return [c for c in BURGERS_CPT if 2 <= n // c <= 32 and n % c == 0 and 8 <= n <= 512]
+    """Warp layouts (4/8/16 cells per lane, 2..32 lanes per row) and, for n >= 64,
+    the one-row-per-CTA layouts (1/2 cells per lane, up to 512 lanes)."""
+    if not (8 <= n <= 512 and n & (n - 1) == 0):
+        return []
+    warp_lanes = {4: (2, 32), 8: (4, 32), 16: (8, 32)}  # lanes per row with kernels built
+    out = []
+    for c in BURGERS_CPT:
+        if c <= 2:
+            if n >= 64 and n // c <= 512:
+                out.append(c)
+        elif warp_lanes[c][0] <= n // c <= warp_lanes[c][1]:
+            out.append(c)
+    return out
 
 
 def ks_candidates(n: int):

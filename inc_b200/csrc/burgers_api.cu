@@ -33,6 +33,23 @@ inline int pick_block(int rows, int tpr, Kind kind, int n, int K) {
 
 int dispatch(Kind kind, const Args& a, int cpt, cudaStream_t st) {
     const int n = a.n;
+    const bool fwd = kind == Kind::Step || kind == Kind::Rollout;
+    // Small batches: spread each row over a whole CTA (1-2 cells per lane).
+    if (cpt == 0 && fwd && a.rows <= 148 && n >= 64) cpt = n >= 256 ? 2 : 1;
+    if ((cpt == 1 || cpt == 2) && !fwd) cpt = 0;  // the adjoints use the warp layouts
+    if (cpt == 1 || cpt == 2) {
+        if (!is_pow2(n) || n < 64 || n / cpt > 512) {
+            set_error("burgers: cells_per_thread=%d needs n a power of two with 64 <= n/%d <= 512", cpt, cpt);
+            return INC_E_UNSUPPORTED;
+        }
+        const int tpr = n / cpt;
+#define INC_WIDE(C, T) \
+        if (cpt == C && tpr == T) return launch_wide<C, T>(kind, a, st);
+        INC_BURGERS_WIDE_SHAPES(INC_WIDE)
+#undef INC_WIDE
+        set_error("burgers: no wide kernel for n=%d cells_per_thread=%d", n, cpt);
+        return INC_E_UNSUPPORTED;
+    }
     if (cpt == 0) cpt = default_cpt(n);
     if (!valid_shape(n, cpt)) {
         set_error("burgers: unsupported n=%d / cells_per_thread=%d (n must be a power of two in [8,512])", n, cpt);

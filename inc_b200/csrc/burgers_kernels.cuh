@@ -137,7 +137,7 @@ INC_DEV void make_ctx(const Args& a, int row, int g, bool valid, Ctx<CPT>& cx) {
     cx.beta = a.beta_rows ? __ldg(a.beta_rows + r) : a.beta;
     cx.t = a.t_rows ? __ldg(a.t_rows + r) : a.t0;
     cx.has_s = a.s != nullptr;
-    if (cx.has_s) load_row_chunk<CPT>(cx.s, a.s + (int64_t)r * a.n + cx.cell0, valid);
+    if (cx.has_s && CPT % 4 == 0) load_row_chunk<CPT>(cx.s, a.s + (int64_t)r * a.n + cx.cell0, valid);
     else {
 #pragma unroll
         for (int c = 0; c < CPT; ++c) cx.s[c] = 0.f;
@@ -503,6 +503,133 @@ __global__ void __launch_bounds__(256) k_rollout_bwd(Args a) {
     if (a.g_s) store_row_chunk<CPT>(a.g_s + base, gs, valid);
 }
 
+// ---------------------------------------------------------------------------
+// Wide rows: one CTA per row, TPR = n / CPT lanes (64..512), CPT = 1 or 2
+// cells per lane.  For small batches this spreads a row over more lanes so a
+// step's dependency chain is shorter.  Halos and the alpha row max go through
+// a shared row buffer, double-buffered by RHS evaluation so that one block
+// barrier per evaluation suffices.
+// ---------------------------------------------------------------------------
+template <int CPT, int TPR>
+struct WideSmem {
+    float row[2][CPT * TPR];
+    float wmax[2][TPR / 32];
+};
+
+template <int CPT, int TPR>
+INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, float nu, float inv_dx, float inv_dx2,
+                           float inv_2dx, WideSmem<CPT, TPR>& sh, int parity, int g) {
+    constexpr int N = CPT * TPR;
+    float* row = sh.row[parity];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) row[g * CPT + c] = u[c];
+    float m = 0.f;
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
+    m = group_max<32>(m);
+    if ((g & 31) == 0) sh.wmax[parity][g >> 5] = m;
+    __syncthreads();
+    float w[CPT + 6];
+#pragma unroll
+    for (int k = 0; k < CPT + 6; ++k) w[k] = row[(g * CPT - 3 + k + N) & (N - 1)];
+    if (conv == INC_CONV_WENO) {
+        float alpha = 0.f;
+#pragma unroll
+        for (int i = 0; i < TPR / 32; ++i) alpha = fmaxf(alpha, sh.wmax[parity][i]);
+        float fp[CPT + 6], fm[CPT + 6];
+#pragma unroll
+        for (int k = 0; k < CPT + 6; ++k) {
+            const float fl = 0.5f * w[k] * w[k];
+            fp[k] = 0.5f * (fl + alpha * w[k]);
+            fm[k] = 0.5f * (fl - alpha * w[k]);
+        }
+        float hp_prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]);
+        float hm_prev = weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float hp = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]);
+            const float hm = weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+            const float nl = -((hp - hp_prev) * inv_dx + (hm - hm_prev) * inv_dx);
+            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
+            hp_prev = hp;
+            hm_prev = hm;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float nl = -w[c + 3] * ((w[c + 4] - w[c + 2]) * inv_2dx);
+            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
+        }
+    }
+}
+
+template <int CPT, int TPR>
+INC_DEV void full_rhs_wide(const Args& a, const Ctx<CPT>& cx, const float (&x)[CPT], float (&r)[CPT], float t,
+                           WideSmem<CPT, TPR>& sh, int& parity, int g) {
+    rhs_core_wide<CPT, TPR>(x, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, sh, parity, g);
+    parity ^= 1;
+    add_source<CPT>(a, cx, x, r, t);
+}
+
+template <int CPT, int TPR>
+INC_DEV void advance_wide(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], float t, WideSmem<CPT, TPR>& sh,
+                          int& parity, int g) {
+    float r[CPT];
+    const float dt = cx.dt;
+    if (a.scheme == INC_TS_EULER) {
+        full_rhs_wide<CPT, TPR>(a, cx, u, r, t, sh, parity, g);
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) u[c] = u[c] + dt * r[c];
+        return;
+    }
+    float u0[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) u0[c] = u[c];
+    full_rhs_wide<CPT, TPR>(a, cx, u, r, t, sh, parity, g);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) u[c] = u0[c] + dt * r[c];
+    full_rhs_wide<CPT, TPR>(a, cx, u, r, t + dt, sh, parity, g);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) u[c] = 0.75f * u0[c] + 0.25f * (u[c] + dt * r[c]);
+    full_rhs_wide<CPT, TPR>(a, cx, u, r, t + 0.5f * dt, sh, parity, g);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) u[c] = (1.f / 3.f) * u0[c] + (2.f / 3.f) * (u[c] + dt * r[c]);
+}
+
+template <int CPT>
+INC_DEV void load_cells(float (&r)[CPT], const float* __restrict__ p) {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) r[c] = __ldg(p + c);
+}
+template <int CPT>
+INC_DEV void store_cells(float* __restrict__ p, const float (&r)[CPT]) {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) p[c] = r[c];
+}
+
+// One step (steps == 1 && frames == nullptr) or a fused rollout, one row per CTA.
+template <int CPT, int TPR>
+__global__ void __launch_bounds__(TPR) k_rollout_wide(Args a, int single_step) {
+    __shared__ WideSmem<CPT, TPR> sh;
+    const int row = blockIdx.x, g = threadIdx.x;
+    Ctx<CPT> cx;
+    make_ctx<CPT, TPR>(a, row, g, true, cx);
+    if (cx.has_s) load_cells<CPT>(cx.s, a.s + (int64_t)row * a.n + g * CPT);
+    float u[CPT];
+    const int64_t base = (int64_t)row * a.n + g * CPT;
+    load_cells<CPT>(u, a.u + base);
+    int parity = 0;
+    const int steps = single_step ? 1 : a.steps;
+    const int nseg = a.ckpt_every > 0 ? (a.steps + a.ckpt_every - 1) / a.ckpt_every : 0;
+    for (int k = 0; k < steps; ++k) {
+        if (a.ckpts && k % a.ckpt_every == 0)
+            store_cells<CPT>(a.ckpts + ((int64_t)row * nseg + k / a.ckpt_every) * a.n + g * CPT, u);
+        advance_wide<CPT, TPR>(a, cx, u, cx.t + k * cx.dt, sh, parity, g);
+        if (a.frames) store_cells<CPT>(a.frames + ((int64_t)row * a.steps + k) * a.n + g * CPT, u);
+    }
+    if (a.out) store_cells<CPT>(a.out + base, u);
+}
+
 // weno_reconstruction(f, direction) as a standalone op (solver_1d.py:4-42).
 template <int CPT, int TPR>
 __global__ void __launch_bounds__(256) k_weno(const float* __restrict__ f, float* __restrict__ out, int rows,
@@ -561,6 +688,18 @@ int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     }
     return check_launch("burgers_bwd");
 }
+
+// Wide-row forward launchers (CPT 1 or 2), instantiated in burgers_fwd_wide.cu.
+template <int CPT, int TPR>
+int launch_wide(Kind kind, const Args& a, cudaStream_t st);
+
+template <int CPT, int TPR>
+int launch_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
+    k_rollout_wide<CPT, TPR><<<a.rows, TPR, 0, st>>>(a, kind == Kind::Step ? 1 : 0);
+    return check_launch("burgers_wide");
+}
+
+#define INC_BURGERS_WIDE_SHAPES(X) X(1, 64) X(1, 128) X(1, 256) X(1, 512) X(2, 64) X(2, 128) X(2, 256)
 
 template <int CPT, int TPR>
 int launch_weno(const float* f, float* out, int rows, int n, int dir, cudaStream_t st, int block);

@@ -76,7 +76,8 @@ def test_weno_reconstruction(cuda):
 
 
 @pytest.mark.parametrize("n,cpt", [(8, 4), (16, 4), (32, 4), (32, 8), (64, 4), (64, 8), (128, 4), (128, 8),
-                                   (128, 16), (256, 8), (256, 16), (512, 16)])
+                                   (128, 16), (256, 8), (256, 16), (512, 16),
+                                   (64, 1), (128, 1), (128, 2), (256, 1), (256, 2), (512, 1)])
 @pytest.mark.parametrize("scheme", ["euler", "ssprk3"])
 def test_shapes_vs_oracle(cuda, n, cpt, scheme):
     from inc_b200.solvers import BurgersSolverTorch

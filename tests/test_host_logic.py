@@ -70,8 +70,9 @@ def test_autotune_cache_roundtrip(tmp_path, monkeypatch):
     assert autotune.bucket(1000) == 1024 and autotune.bucket(1024) == 1024 and autotune.bucket(1) == 1
     assert autotune.ks_candidates(256) == [16, 32, 64]
     assert autotune.ks_candidates(16) == [4]
-    assert autotune.burgers_candidates(512) == [16]
-    assert autotune.burgers_candidates(128) == [4, 8, 16]
+    assert autotune.burgers_candidates(512) == [1, 2, 16]
+    assert autotune.burgers_candidates(128) == [1, 2, 4, 8, 16]
+    assert autotune.burgers_candidates(32) == [4, 8]
     k = autotune.key("ks", 256, 1000, "ETRK2", None)
     assert k.endswith("|ks|n256|b1024|ETRK2")
     autotune._load()[k] = {"threads_per_pair": 16}
