@@ -50,7 +50,9 @@ def parse_args():
                     default="ks_plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
-    ap.add_argument("--profile", action="store_true", help="one small fused launch for ncu (no JSON)")
+    ap.add_argument("--profile", nargs="?", const="ks", default=None,
+                    choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd"],
+                    help="a small case of one kernel for ncu (no JSON)")
     return ap.parse_args()
 
 
@@ -648,8 +650,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=dev)
     if args.profile:
-        from inc_b200.workloads import ks_plain_config  # noqa: F401
-        profile_small(dev)
+        profile_small(dev, args.profile)
         return
     if args.workload in ("burgers_diff", "ks_diff"):
         cfg, cells, times, extra = bench_diff(args, dev, world, args.workload)
@@ -730,10 +731,34 @@ def main():
         torch.distributed.destroy_process_group()
 
 
-def profile_small(dev):
-    """A small KS fused launch (B=512, 64 steps) for an ncu capture."""
+def profile_small(dev, which="ks"):
+    """Small cases for ncu captures: the KS fused rollout (B=512, N=256, 64 steps) and its
+    backward, the ragged Burgers batch (1024 rows, 20 steps) or the 32x128 Burgers rollout."""
     import torch
     from types import SimpleNamespace
+    if which == "burgers_ragged":
+        from inc_b200.batched import RaggedBurgers
+        from inc_b200.workloads import burgers_batched_config
+        cfg = burgers_batched_config(rows=1024, steps=20)
+        rb = RaggedBurgers(cfg["u0"], cfg["nu"], cfg["dt"], cfg["dx"], scheme="ssprk3", device=dev)
+        for _ in range(2):
+            rb.rollout(20)
+        torch.cuda.synchronize()
+        return
+    if which == "burgers_plain":
+        from inc_b200.rollout import burgers_rollout
+        from inc_b200.solvers import BurgersSolverTorch
+        from inc_b200.workloads import burgers_plain_config
+        cfg = burgers_plain_config()
+        sp = SimpleNamespace(resolution=cfg["N"], dt=cfg["dt"], x=None, adaptive_CFL=None, L=cfg["L"], nu=cfg["nu"],
+                             device=dev, convection_term="WENO", equation_type="viscosity", batch_size=cfg["B"],
+                             time_scheme="ssprk3", cells_per_thread=1)
+        u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=dev)
+        with torch.no_grad():
+            for _ in range(2):
+                burgers_rollout(BurgersSolverTorch(sp), u0, cfg["steps"])
+        torch.cuda.synchronize()
+        return
     from inc_b200.solvers import KSSolverTorch
     from inc_b200.workloads import ks_plain_config
     cfg = ks_plain_config(B=512, steps=64)
@@ -745,6 +770,16 @@ def profile_small(dev):
     s = torch.tensor(cfg["s"], dtype=torch.float32, device=dev)
     plan = solver.plan_for(u0, ds)
     frames = torch.empty(B, cfg["steps"], N, device=dev)
+    if which == "ks_bwd":
+        K = 8
+        ck = torch.empty(B, (cfg["steps"] + K - 1) // K, N, device=dev)
+        g = torch.randn(B, cfg["steps"], N, device=dev)
+        gu, gs = torch.empty_like(u0), torch.empty_like(u0)
+        for _ in range(2):
+            plan.rollout(u0, s, cfg["steps"], frames, None, K, ck)
+            plan.rollout_bwd(ck, s, cfg["steps"], K, g, None, gu, gs)
+        torch.cuda.synchronize()
+        return
     for _ in range(2):
         plan.rollout(u0, s, cfg["steps"], frames, None, 0, None)
     u = torch.empty_like(u0)

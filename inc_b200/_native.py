@@ -71,6 +71,7 @@ SIGNATURES = {
     "inc_ks_rollout_bwd": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp,
                                      _vp]),
     "inc_bench_fma": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp]),
+    "inc_energy_spectrum": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, _vp]),
     "inc_burgers_rollout_grad_noalloc": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, C.c_int32,
                                                    C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }

@@ -226,28 +226,27 @@ INC_DEV void full_rhs(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], 
     add_source<CPT>(a, cx, u, r, t);
 }
 
-// One step (Euler or SSP-RK3) of size cx.dt starting at time t.
+// Shu-Osher SSP-RK3 as stage coefficients: stage k evaluates the RHS at
+// t + kC[k] dt on the current stage value u and sets u = kA[k] u0 + kB[k] (u + dt R).
+INC_DEV float rk3_c(int k) { return k == 0 ? 0.f : (k == 1 ? 1.f : 0.5f); }
+INC_DEV float rk3_a(int k) { return k == 0 ? 0.f : (k == 1 ? 0.75f : 1.f / 3.f); }
+INC_DEV float rk3_b(int k) { return k == 0 ? 1.f : (k == 1 ? 0.25f : 2.f / 3.f); }
+
+// One step (Euler or SSP-RK3) of size cx.dt starting at time t.  The stages
+// run as a loop around one copy of the right-hand side (instruction cache).
 template <int CPT, int TPR>
 INC_DEV void advance(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], float t, int left, int right) {
-    float r[CPT];
+    float r[CPT], u0[CPT];
     const float dt = cx.dt;
-    if (a.scheme == INC_TS_EULER) {
-        full_rhs<CPT, TPR>(a, cx, u, r, t, left, right);
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) u[c] = u[c] + dt * r[c];
-    } else {
-        float u0[CPT];
+    for (int c = 0; c < CPT; ++c) u0[c] = u[c];
+#pragma unroll 1
+    for (int k = 0; k < stages; ++k) {
+        full_rhs<CPT, TPR>(a, cx, u, r, t + rk3_c(k) * dt, left, right);
+        const float ka = rk3_a(k), kb = rk3_b(k);
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) u0[c] = u[c];
-        full_rhs<CPT, TPR>(a, cx, u, r, t, left, right);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) u[c] = u0[c] + dt * r[c];
-        full_rhs<CPT, TPR>(a, cx, u, r, t + dt, left, right);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) u[c] = 0.75f * u0[c] + 0.25f * (u[c] + dt * r[c]);
-        full_rhs<CPT, TPR>(a, cx, u, r, t + 0.5f * dt, left, right);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) u[c] = (1.f / 3.f) * u0[c] + (2.f / 3.f) * (u[c] + dt * r[c]);
+        for (int c = 0; c < CPT; ++c) u[c] = ka * u0[c] + kb * (u[c] + dt * r[c]);
     }
 }
 
@@ -337,53 +336,47 @@ INC_DEV void rhs_vjp(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], c
 }
 
 // Backward of `advance`: given gu = dL/du_new (in), returns dL/du in gu and
-// accumulates dL/ds into gs.
+// accumulates dL/ds into gs.  Stage k maps u_k to
+// u_{k+1} = a_k u + b_k (u_k + dt R(u_k)), so in reverse:
+//   dL/du_k = b_k (g + dt J(u_k)^T g),  dL/du += a_k g,  dL/ds += b_k dt g.
+// The stage inputs u_1, u_2 are replayed from u first.
 template <int CPT, int TPR>
 INC_DEV void advance_bwd(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], float (&gu)[CPT],
                          float (&gs)[CPT], float t, int g, int left, int right) {
     const float dt = cx.dt;
-    float j[CPT];
-    if (a.scheme == INC_TS_EULER) {
-        rhs_vjp<CPT, TPR>(a, cx, u, gu, j, g, left, right);
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
+    float u1[CPT], u2[CPT], x[CPT], r[CPT];
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) { x[c] = u[c]; u1[c] = u[c]; u2[c] = u[c]; }
+#pragma unroll 1
+    for (int k = 0; k + 1 < stages; ++k) {  // replay u_1, u_2
+        full_rhs<CPT, TPR>(a, cx, x, r, t + rk3_c(k) * dt, left, right);
+        const float ka = rk3_a(k), kb = rk3_b(k);
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
-            gs[c] += dt * gu[c];
-            gu[c] = gu[c] + dt * j[c];
+            x[c] = ka * u[c] + kb * (x[c] + dt * r[c]);
+            if (k == 0) u1[c] = x[c];
+            else u2[c] = x[c];
         }
-        return;
     }
-    // recompute the stages
-    float u1[CPT], u2[CPT], r[CPT];
-    full_rhs<CPT, TPR>(a, cx, u, r, t, left, right);
+    float acc[CPT];
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) u1[c] = u[c] + dt * r[c];
-    full_rhs<CPT, TPR>(a, cx, u1, r, t + dt, left, right);
+    for (int c = 0; c < CPT; ++c) acc[c] = 0.f;
+#pragma unroll 1
+    for (int k = stages - 1; k >= 0; --k) {
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) u2[c] = 0.75f * u[c] + 0.25f * (u1[c] + dt * r[c]);
-    // u3 = 1/3 u + 2/3 (u2 + dt R(u2))
-    float acc[CPT], b[CPT];
-    rhs_vjp<CPT, TPR>(a, cx, u2, gu, j, g, left, right);
+        for (int c = 0; c < CPT; ++c) x[c] = k == 2 ? u2[c] : (k == 1 ? u1[c] : u[c]);
+        rhs_vjp<CPT, TPR>(a, cx, x, gu, r, g, left, right);
+        const float ka = rk3_a(k), kb = rk3_b(k);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-        acc[c] = (1.f / 3.f) * gu[c];
-        gs[c] += (2.f / 3.f) * dt * gu[c];
-        b[c] = (2.f / 3.f) * (gu[c] + dt * j[c]);  // dL/du2
+        for (int c = 0; c < CPT; ++c) {
+            gs[c] += kb * dt * gu[c];
+            acc[c] += ka * gu[c];
+            gu[c] = kb * (gu[c] + dt * r[c]);
+        }
     }
-    // u2 = 3/4 u + 1/4 (u1 + dt R(u1))
-    rhs_vjp<CPT, TPR>(a, cx, u1, b, j, g, left, right);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-        acc[c] += 0.75f * b[c];
-        gs[c] += 0.25f * dt * b[c];
-        b[c] = 0.25f * (b[c] + dt * j[c]);  // dL/du1
-    }
-    // u1 = u + dt R(u)
-    rhs_vjp<CPT, TPR>(a, cx, u, b, j, g, left, right);
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-        gs[c] += dt * b[c];
-        gu[c] = acc[c] + b[c] + dt * j[c];
-    }
+    for (int c = 0; c < CPT; ++c) gu[c] += acc[c];
 }
 
 // ---------------------------------------------------------------------------
@@ -571,6 +564,9 @@ INC_DEV void full_rhs_wide(const Args& a, const Ctx<CPT>& cx, const float (&x)[C
     add_source<CPT>(a, cx, x, r, t);
 }
 
+// The wide layout serves small, latency-bound batches: its stages stay
+// unrolled (straight-line code schedules better; one row per CTA keeps the
+// code footprint per SM small).
 template <int CPT, int TPR>
 INC_DEV void advance_wide(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], float t, WideSmem<CPT, TPR>& sh,
                           int& parity, int g) {
@@ -585,15 +581,13 @@ INC_DEV void advance_wide(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], fl
     float u0[CPT];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) u0[c] = u[c];
-    full_rhs_wide<CPT, TPR>(a, cx, u, r, t, sh, parity, g);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) u[c] = u0[c] + dt * r[c];
-    full_rhs_wide<CPT, TPR>(a, cx, u, r, t + dt, sh, parity, g);
+    for (int k = 0; k < 3; ++k) {
+        full_rhs_wide<CPT, TPR>(a, cx, u, r, t + rk3_c(k) * dt, sh, parity, g);
+        const float ka = rk3_a(k), kb = rk3_b(k);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) u[c] = 0.75f * u0[c] + 0.25f * (u[c] + dt * r[c]);
-    full_rhs_wide<CPT, TPR>(a, cx, u, r, t + 0.5f * dt, sh, parity, g);
-#pragma unroll
-    for (int c = 0; c < CPT; ++c) u[c] = (1.f / 3.f) * u0[c] + (2.f / 3.f) * (u[c] + dt * r[c]);
+        for (int c = 0; c < CPT; ++c) u[c] = ka * u0[c] + kb * (u[c] + dt * r[c]);
+    }
 }
 
 template <int CPT>

@@ -209,6 +209,13 @@ int inc_ks_rollout_bwd(const inc_ks_plan* plan, const float* ckpts, const float*
                        int32_t steps, int32_t ckpt_every, const float* g_frames,
                        const float* g_final, float* g_u0, float* g_s, void* stream);
 
+/* ---- analysis -------------------------------------------------------------- */
+/* Energy spectrum of each of `rows` real rows of length n (a power of two in
+ * [16, 512]): out[row][k] = |FFT(u)[k]|^2 for k in [0, n/2], bins 1..n/2-1
+ * doubled.  Replaces calculate_energy_spectrum (analysis/Plot_KS.py:196-235),
+ * which the reference runs on the CPU after a rollout.                        */
+int inc_energy_spectrum(const float* u, float* out, int32_t rows, int32_t n, void* stream);
+
 /* ---- measurement utility ------------------------------------------------ */
 /* FP32 FMA throughput probe used by bench.py for the roofline denominator:
  * `blocks` x 256 threads, each 128 * iters FMAs (2 flops each) in 8

@@ -351,10 +351,67 @@ def make_hybrid():
     np.savez_compressed(os.path.join(OUT, "hybrid_golden.npz"), **out)
 
 
+def _load_reference_module(relpath, name):
+    """Import one reference file; plotting libraries absent here are stubbed
+    (the functions used below only call numpy and torch)."""
+    import importlib.util
+    import types
+    from unittest import mock
+    for mod in ("matplotlib", "matplotlib.pyplot"):
+        sys.modules.setdefault(mod, mock.MagicMock(name=mod))
+    spec = importlib.util.spec_from_file_location(name, os.path.join(REF, relpath))
+    m = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(m)
+    return m
+
+
+def make_analysis_and_data():
+    """Energy spectrum (analysis/Plot_KS.py:196-235) and trajectory windows
+    (data/data_loader_1d.py:8-139) from the reference's own code."""
+    rng = np.random.default_rng(99)
+    out = {}
+    pks = _load_reference_module("analysis/Plot_KS.py", "ref_plot_ks")
+    for name, shape in (("spec_even", (3, 4, 64)), ("spec_even2d", (5, 32)), ("spec_256", (2, 3, 256))):
+        v = rng.standard_normal(shape).astype(np.float32)
+        e, k = pks.calculate_energy_spectrum(v)
+        out[f"{name}.v"] = v
+        out[f"{name}.energy"] = e.numpy().astype(np.float64)
+        out[f"{name}.k"] = k.numpy().astype(np.float64)
+    dl = _load_reference_module("data/data_loader_1d.py", "ref_data_loader")
+    B, T1, D, J = 3, 13, 16, 2
+    data = {"trajectories": torch.from_numpy(rng.standard_normal((B, T1, D))),
+            "nu": torch.from_numpy(rng.uniform(0.01, 0.05, (B, 1))),
+            "A": torch.from_numpy(rng.standard_normal((B, 1, J))), "omega": torch.from_numpy(rng.standard_normal((B, 1, J))),
+            "phi": torch.from_numpy(rng.standard_normal((B, 1, J))), "l": torch.from_numpy(rng.standard_normal((B, 1, J))),
+            "domain_size": torch.from_numpy(rng.uniform(20, 60, (B, 1))),
+            "metadata": {"gen_dt": 0.5}}
+    out["dl.trajectories"] = data["trajectories"].numpy()
+    for k in ("nu", "A", "omega", "phi", "l", "domain_size"):
+        out[f"dl.{k}"] = data[k].numpy()
+    cases = []
+    for cname, cls, dt, mstep, gap in (("bg_r1", dl.BurgersDataset, 0.5, 3, 1), ("bg_r2", dl.BurgersDataset, 1.0, 2, 3),
+                                       ("ks_r1", dl.KSDataset, 0.5, 4, 2), ("ks_r3", dl.KSDataset, 1.5, 2, 3)):
+        ds = cls(data, dt=dt, mstep=mstep, starts_gap=gap)
+        items = [ds[i] for i in range(len(ds))]
+        out[f"dl.{cname}.args"] = np.array([dt, mstep, -1 if gap is None else gap], dtype=np.float64)
+        out[f"dl.{cname}.len"] = np.int64(len(ds))
+        out[f"dl.{cname}.u_initial"] = torch.stack([it["u_initial"] for it in items]).numpy()
+        out[f"dl.{cname}.u_target"] = torch.stack([it["u_target"] for it in items]).numpy()
+        if cls is dl.BurgersDataset:
+            out[f"dl.{cname}.t"] = np.array([float(it["t"]) for it in items])
+            out[f"dl.{cname}.nu"] = torch.stack([it["nu"] for it in items]).numpy()
+        else:
+            out[f"dl.{cname}.domain_size"] = torch.stack([it["domain_size"] for it in items]).numpy()
+        cases.append(cname)
+    out["dl.cases"] = np.array(cases)
+    np.savez_compressed(os.path.join(OUT, "analysis_data_golden.npz"), **out)
+
+
 if __name__ == "__main__":
     torch.set_default_dtype(torch.float64)
     make_burgers()
     make_ks()
     make_hybrid()
-    for f in ("burgers_golden.npz", "ks_golden.npz", "hybrid_golden.npz"):
+    make_analysis_and_data()
+    for f in ("burgers_golden.npz", "ks_golden.npz", "hybrid_golden.npz", "analysis_data_golden.npz"):
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
