@@ -340,6 +340,9 @@ def bench_ks(args, dev, world):
         t_e2e = event_time(e2e, args.steps, flush)
 
     # --- roofline of the fused kernel ------------------------------------------------
+    # DRAM traffic of one launch of this workload, from one ncu capture
+    # (profiles/ks_rollout_fused_b1024_n256_dram.md): 3.07 MB read + 359.1 MB written.
+    extra_traffic = 362.2e6 if (B, N, steps) == (1024, 256, 400) else None
     peak = fp32_peak_tflops(dev)
     flops_cell = ks_flops_per_cell_step(N, cfg["scheme"])
     achieved = flops_cell * cells / (ms_fused * 1e-3) / 1e12
@@ -350,7 +353,7 @@ def bench_ks(args, dev, world):
     extra = dict(
         flops_per_cell_step=flops_cell, peak=peak, achieved=achieved,
         plain_hbm_gbs=plain_bytes_per_cell_step(True) * B * N / (plain_ms_step * 1e-3) / 1e9,
-        clocks=clk.summary(), h2d=2 * B * N * 4, d2h=B * N * 4, launches=args.steps,
+        clocks=clk.summary(), h2d=2 * B * N * 4, d2h=B * N * 4, launches=args.steps, traffic=extra_traffic,
     )
     return cfg, cells, times, extra
 
@@ -709,7 +712,10 @@ def main():
             "e2e": {"value": rate(times["e2e"]), "unit": "cell-steps/s", "h2d_bytes_per_step": extra["h2d"],
                     "d2h_bytes_per_step": extra["d2h"], "api": "inc_b200.rollout (fused launch)"},
             "roofline": {"bound": "fp32", "achieved": extra["achieved"], "peak": extra["peak"], "unit": "TFLOP/s",
-                         "frac": extra["achieved"] / extra["peak"], "traffic": None,
+                         "frac": extra["achieved"] / extra["peak"], "traffic": extra.get("traffic"),
+                         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch, "
+                                            "profiles/ks_rollout_fused_b1024_n256_dram.md")
+                         if extra.get("traffic") else None,
                          "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run",
                          "flops_per_cell_step": extra["flops_per_cell_step"]},
             "cpu_baseline": cpu_b,
