@@ -478,95 +478,7 @@ INC_DEV void load_pair_strided(float2 (&x)[P], const float* __restrict__ src, co
     }
 }
 
-// ---- the step -----------------------------------------------------------------
-// Forward FFT of physical v into scaled spectral storage (packed or split).
-template <int P, int T>
-INC_DEV void to_spec(const Args& a, float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t, bool scale) {
-    fft_fwd<P, T>(v, buf, tw, t);
-    if (scale) {
-#pragma unroll
-        for (int m = 0; m < P; ++m) v[m] = cscale(v[m], a.invN);
-    }
-    if (a.split) to_split<P, T>(v, t, buf.a);
-}
-
-// Inverse FFT of scaled spectral storage into physical values.
-template <int P, int T>
-INC_DEV void to_phys(const Args& a, float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t) {
-    if (a.split) to_packed<P, T>(v, t, buf.a);
-    fft_inv<P, T>(v, buf, tw, t);
-}
-
 INC_DEV float2 sq2(float2 x) { return make_float2(x.x * x.x, x.y * x.y); }
-
-// SS = phi1 * FFT(s) / N, held for the whole step (s enters stage 1 of each substep).
-template <int P, int T>
-INC_DEV void source_spec(const Args& a, const Ctx& c, float2 (&SS)[P], Buf buf, const Twiddles<P, T>& tw) {
-    if (!a.s) {
-#pragma unroll
-        for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
-        return;
-    }
-    load_pair<P, T>(SS, a.s, c, a.n);
-    to_spec<P, T>(a, SS, buf, tw, c.t, true);
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-        const Slot s = slot<P, T>(a, c, m, false);
-        SS[m] = rmul(SS[m], s.p1, s.p1b);
-    }
-}
-
-// One substep.  x: physical in/out; X: scaled spectrum of x in/out.
-// If xi != nullptr (ETRK2) the intermediate physical state is also returned.
-template <int P, int T>
-INC_DEV void substep(const Args& a, const Ctx& c, float2 (&x)[P], float2 (&X)[P], const float2 (&SS)[P],
-                     Buf buf, const Twiddles<P, T>& tw, float2 (*xi)[P]) {
-    const int t = c.t;
-    float2 v[P];
-#pragma unroll
-    for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
-    to_spec<P, T>(a, v, buf, tw, t, false);
-    if (a.scheme == INC_KS_ETD1) {
-#pragma unroll
-        for (int m = 0; m < P; ++m) {
-            const Slot s = slot<P, T>(a, c, m, false);
-            const float2 DV = dmul(v[m], s.d * a.invN);
-            X[m] = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
-            v[m] = X[m];
-        }
-        to_phys<P, T>(a, v, buf, tw, t);
-#pragma unroll
-        for (int m = 0; m < P; ++m) x[m] = v[m];
-        return;
-    }
-    // ETRK2 stage 1: Zi = E X + phi1 (D V + S);  carry Y = Zi - phi2 D V
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-        const Slot s = slot<P, T>(a, c, m, true);
-        const float2 DV = dmul(v[m], s.d * a.invN);
-        const float2 Zi = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
-        X[m] = csub(Zi, cscale(DV, s.p2));
-        v[m] = Zi;
-    }
-    to_phys<P, T>(a, v, buf, tw, t);
-    if (xi) {
-#pragma unroll
-        for (int m = 0; m < P; ++m) (*xi)[m] = v[m];
-    }
-    // stage 2: X' = Y + phi2 D V2
-#pragma unroll
-    for (int m = 0; m < P; ++m) v[m] = sq2(v[m]);
-    to_spec<P, T>(a, v, buf, tw, t, false);
-#pragma unroll
-    for (int m = 0; m < P; ++m) {
-        const Slot s = slot<P, T>(a, c, m, true);
-        X[m] = cadd(X[m], cscale(dmul(v[m], s.d * a.invN), s.p2));
-        v[m] = X[m];
-    }
-    to_phys<P, T>(a, v, buf, tw, t);
-#pragma unroll
-    for (int m = 0; m < P; ++m) x[m] = v[m];
-}
 
 // ---- shared memory ----------------------------------------------------------------
 // Per CTA: the twiddle table of the later passes ((passes-1) * N float2), then
@@ -607,8 +519,22 @@ INC_DEV Twiddles<P, T> setup_twiddles(const Args& a, float2* sm, int t) {
 enum Phase { PH_S, PH_U, PH_NL1, PH_NL2, PH_INV };
 
 template <int P, int T>
+INC_DEV void st_put(float2* st, const float2 (&v)[P], int t) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) st[m * T + t] = v[m];
+}
+template <int P, int T>
+INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) v[m] = st[m * T + t];
+}
+
+// seg (optional): shared memory receiving the state at the start of every step,
+// in lane layout [step][m][t] (the backward replay).  ckpt_on: store checkpoints.
+template <int P, int T>
 INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, Buf buf,
-                             const Twiddles<P, T>& tw, bool frames_on, int nseg) {
+                             const Twiddles<P, T>& tw, bool frames_on, int nseg, bool ckpt_on = true,
+                             float2* seg = nullptr) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
@@ -631,8 +557,11 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
             step = q / per_step;
             const int f = (q % per_step) % per_sub;
             kind = (f & 1) ? PH_INV : (f == 0 ? PH_NL1 : PH_NL2);
-            if (q % per_step == 0 && a.ckpts && step % a.ckpt_every == 0)
-                store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)(step / a.ckpt_every) * N);
+            if (q % per_step == 0) {
+                if (ckpt_on && a.ckpts && step % a.ckpt_every == 0)
+                    store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)(step / a.ckpt_every) * N);
+                if (seg) st_put<P, T>(seg + step * N, x, t);
+            }
         }
         // operand of this transform
         if (kind == PH_S) {
@@ -726,106 +655,212 @@ __global__ void __launch_bounds__(128) k_rollout(Args a) {
 
 // ---- adjoint ------------------------------------------------------------------
 // Per-group shared memory of the backward kernels, in lane layout [m][t]:
-//   st[0..3]: x0, xi1, x1, xi2 of the step being differentiated
-//   w2: scratch for the second-stage adjoint field
-INC_DEV int lidx(int T, int m, int t) { return m * T + t; }
+// st[0..3] = x1, xi1, xi2, w2 of the step being differentiated (x0 is read
+// where the caller keeps it).  The adjoint of one step() (the maths of the
+// forward run backwards, substep by substep):
+//   w2 = IFFT(d phi2 G);  Gi = G - FFT(2 xi w2)/N
+//   w1 = IFFT(d phi1 Gi); Sacc += phi1 Gi
+//   G  = E Gi + FFT(2 x (w2 - w1))/N      (ETD1: w2 = 0, Gi = G)
+// with x, xi the substep's start and intermediate states, replayed first.
+enum BPhase { B_GF, B_U, B_NL1, B_INV_XI1, B_NL2, B_INV_X1, B_NL1B, B_INV_XI2, B_W2, B_GI, B_W1, B_GP };
+
+INC_DEV int recompute_kind(bool rk2, int q) {
+    if (!rk2) return q == 0 ? B_U : (q == 1 ? B_NL1 : B_INV_X1);
+    switch (q) {
+        case 0: return B_U;
+        case 1: return B_NL1;
+        case 2: return B_INV_XI1;
+        case 3: return B_NL2;
+        case 4: return B_INV_X1;
+        case 5: return B_NL1B;
+        default: return B_INV_XI2;
+    }
+}
 
 template <int P, int T>
-INC_DEV void st_put(float2* st, const float2 (&v)[P], int t) {
+INC_DEV void pair_mul2(float2 (&v)[P], const float2 (&x)[P], float s) {
 #pragma unroll
-    for (int m = 0; m < P; ++m) st[m * T + t] = v[m];
-}
-template <int P, int T>
-INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
-#pragma unroll
-    for (int m = 0; m < P; ++m) v[m] = st[m * T + t];
+    for (int m = 0; m < P; ++m) v[m] = make_float2(s * x[m].x * v[m].x, s * x[m].y * v[m].y);
 }
 
-// Backward of one step() from its input state x0 (physical, correction_u
-// already added).  G: scaled adjoint spectrum w.r.t. the step output (in),
-// w.r.t. the step input (out).  Sacc accumulates phi1-weighted adjoints whose
-// inverse FFT is dL/ds.
+// Backward of one step() whose input state x0 (correction_u included) is at
+// x0s.  G: scaled adjoint spectrum w.r.t. the step output (in) and input
+// (out); Sacc accumulates phi1-weighted adjoints (IFFT(Sacc) = dL/ds).  If
+// gframe != nullptr the adjoint of this step's output frame is added first.
 template <int P, int T>
-INC_DEV void step_bwd(const Args& a, const Ctx& c, const float2 (&x0)[P], float2 (&G)[P], float2 (&Sacc)[P],
-                      const float2 (&SS)[P], Buf buf, const Twiddles<P, T>& tw, float2* st) {
+INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>& cc, const float2 (&SS)[P],
+                              float2 (&G)[P], float2 (&Sacc)[P], const float* gframe, int64_t gf_row_stride,
+                              int64_t gf_off, const float2* x0s, float2* st, Buf buf, const Twiddles<P, T>& tw) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
-    // forward recompute: states at the start of each substep and the ETRK2 intermediates
-    {
-        float2 x[P], X[P], xi[P];
+    const int lead = gframe ? 1 : 0;
+    const int nrec = rk2 ? 7 : 3;
+    const int per = rk2 ? 4 : 2;
+    const int total = lead + nrec + 2 * per;
+    float2* x1s = st;
+    float2* xi1s = st + N;
+    float2* xi2s = st + 2 * N;
+    float2* w2s = st + 3 * N;
+    float2 X[P], v[P], u[P];
+#pragma unroll 1
+    for (int ph = 0; ph < total; ++ph) {
+        const int q = ph - lead;
+        int kind, sub = 0;
+        if (q < 0) {
+            kind = B_GF;
+        } else if (q < nrec) {
+            kind = recompute_kind(rk2, q);
+        } else {
+            const int r = q - nrec;
+            sub = 1 - r / per;
+            const int f = r % per;
+            kind = rk2 ? (f == 0 ? B_W2 : (f == 1 ? B_GI : (f == 2 ? B_W1 : B_GP))) : (f == 0 ? B_W1 : B_GP);
+        }
+        // ---- operand of this transform
+        switch (kind) {
+            case B_GF: load_pair_strided<P, T>(v, gframe, c, N, gf_row_stride, gf_off); break;
+            case B_U: st_get<P, T>(v, x0s, t); break;
+            case B_NL1:
+                st_get<P, T>(v, x0s, t);
 #pragma unroll
-        for (int m = 0; m < P; ++m) { x[m] = x0[m]; X[m] = x0[m]; }
-        st_put<P, T>(st, x, t);
-        to_spec<P, T>(a, X, buf, tw, t, true);
-        substep<P, T>(a, c, x, X, SS, buf, tw, rk2 ? &xi : nullptr);
-        if (rk2) st_put<P, T>(st + N, xi, t);
-        st_put<P, T>(st + 2 * N, x, t);
-        if (rk2) {
-            // substep 2, stage 1 only (its intermediate state)
-            float2 v[P];
+                for (int m = 0; m < P; ++m) v[m] = sq2(v[m]);
+                break;
+            case B_NL2:
+            case B_NL1B:
+                st_get<P, T>(v, kind == B_NL2 ? xi1s : x1s, t);
 #pragma unroll
-            for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
-            to_spec<P, T>(a, v, buf, tw, t, false);
+                for (int m = 0; m < P; ++m) v[m] = sq2(v[m]);
+                break;
+            case B_W2:
+            case B_W1:
 #pragma unroll
-            for (int m = 0; m < P; ++m) {
-                const Slot s = slot<P, T>(a, c, m, false);
-                const float2 DV = dmul(v[m], s.d * a.invN);
-                v[m] = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
+                for (int m = 0; m < P; ++m) {
+                    const Slot sl = cc.get(a, c, m, kind == B_W2);
+                    v[m] = cscale(dmul(G[m], sl.d), kind == B_W2 ? sl.p2 : sl.p1);
+                    if (kind == B_W1) Sacc[m] = cadd(Sacc[m], rmul(G[m], sl.p1, sl.p1b));
+                }
+                if (a.split) to_packed<P, T>(v, t, buf.a);
+#pragma unroll
+                for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+                break;
+            case B_GI:  // v holds w2
+                st_get<P, T>(u, sub ? xi2s : xi1s, t);
+                pair_mul2<P, T>(v, u, 2.f);
+                break;
+            case B_GP:  // v holds w1
+                st_get<P, T>(u, sub ? x1s : x0s, t);
+                if (rk2) {
+                    float2 w2[P];
+                    st_get<P, T>(w2, w2s, t);
+#pragma unroll
+                    for (int m = 0; m < P; ++m) v[m] = csub(w2[m], v[m]);
+                    pair_mul2<P, T>(v, u, 2.f);
+                } else {
+                    pair_mul2<P, T>(v, u, -2.f);
+                }
+                break;
+            default: break;  // inverse transforms: v was prepared by the previous phase
+        }
+        fft_fwd<P, T>(v, buf, tw, t);
+        // ---- result
+        const bool inverse = kind == B_INV_XI1 || kind == B_INV_X1 || kind == B_INV_XI2 || kind == B_W2 || kind == B_W1;
+        if (inverse) {
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+            if (kind == B_INV_XI1) st_put<P, T>(xi1s, v, t);
+            else if (kind == B_INV_X1) st_put<P, T>(x1s, v, t);
+            else if (kind == B_INV_XI2) st_put<P, T>(xi2s, v, t);
+            else if (kind == B_W2) st_put<P, T>(w2s, v, t);
+            continue;  // B_W1 keeps w1 in v for B_GP
+        }
+        if (a.split) to_split<P, T>(v, t, buf.a);
+        switch (kind) {
+            case B_GF:
+#pragma unroll
+                for (int m = 0; m < P; ++m) G[m] = cadd(G[m], cscale(v[m], a.invN));
+                continue;
+            case B_U:
+#pragma unroll
+                for (int m = 0; m < P; ++m) X[m] = cscale(v[m], a.invN);
+                continue;
+            case B_GI:
+#pragma unroll
+                for (int m = 0; m < P; ++m) G[m] = csub(G[m], cscale(v[m], a.invN));
+                continue;
+            case B_GP:
+#pragma unroll
+                for (int m = 0; m < P; ++m) {
+                    const Slot sl = cc.get(a, c, m, false);
+                    G[m] = cadd(rmul(G[m], sl.E, sl.Eb), cscale(v[m], a.invN));
+                }
+                continue;
+            default: break;
+        }
+        // replay stages: next operand is an inverse transform
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const Slot sl = cc.get(a, c, m, rk2);
+            const float2 DV = dmul(v[m], sl.d * a.invN);
+            if (kind == B_NL2) {
+                X[m] = cadd(X[m], cscale(DV, sl.p2));
+                v[m] = X[m];
+            } else {
+                const float2 Zi = cadd(cadd(rmul(X[m], sl.E, sl.Eb), cscale(DV, sl.p1)), SS[m]);
+                if (kind == B_NL1) X[m] = rk2 ? csub(Zi, cscale(DV, sl.p2)) : Zi;
+                v[m] = Zi;
             }
-            to_phys<P, T>(a, v, buf, tw, t);
-            st_put<P, T>(st + 3 * N, v, t);
+        }
+        if (a.split) to_packed<P, T>(v, t, buf.a);
+#pragma unroll
+        for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+    }
+}
+
+// Spectra entering the adjoint: SS = phi1 FFT(s)/N and G = FFT(g)/N of an
+// adjoint field g (null: zero), as one loop around one transform.
+template <int P, int T>
+INC_DEV void adjoint_prologue(const Args& a, const Ctx& c, const SlotCache<P, T>& cc, const float* g,
+                              float2 (&SS)[P], float2 (&G)[P], Buf buf, const Twiddles<P, T>& tw) {
+    constexpr int N = P * T;
+#pragma unroll
+    for (int m = 0; m < P; ++m) { SS[m] = make_float2(0.f, 0.f); G[m] = make_float2(0.f, 0.f); }
+#pragma unroll 1
+    for (int k = 0; k < 2; ++k) {
+        const float* src = k == 0 ? a.s : g;
+        if (!src) continue;
+        float2 v[P];
+        load_pair<P, T>(v, src, c, N);
+        fft_fwd<P, T>(v, buf, tw, c.t);
+        if (a.split) to_split<P, T>(v, c.t, buf.a);
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const float2 z = cscale(v[m], a.invN);
+            if (k == 0) {
+                const Slot sl = cc.get(a, c, m, false);
+                SS[m] = rmul(z, sl.p1, sl.p1b);
+            } else {
+                G[m] = z;
+            }
         }
     }
-    float2* w2s = st + 4 * N;
+}
+
+// dL/du = IFFT(G) and dL/ds = IFFT(Sacc) stored to the caller's arrays.
+template <int P, int T>
+INC_DEV void adjoint_epilogue(const Args& a, const Ctx& c, const float2 (&G)[P], const float2 (&Sacc)[P], Buf buf,
+                              const Twiddles<P, T>& tw) {
+    constexpr int N = P * T;
 #pragma unroll 1
-    for (int sub = 1; sub >= 0; --sub) {
-        const float2* xs = st + (sub == 0 ? 0 : 2 * N);
-        const float2* xis = st + (sub == 0 ? N : 3 * N);
-        float2 v[P], u[P];
-        if (rk2) {
-            // w2 = IFFT(d phi2 G)
+    for (int k = 0; k < 2; ++k) {
+        float* dst = k == 0 ? a.g_u : a.g_s;
+        if (!dst) continue;
+        float2 v[P];
 #pragma unroll
-            for (int m = 0; m < P; ++m) {
-                const Slot s = slot<P, T>(a, c, m, true);
-                v[m] = cscale(dmul(G[m], s.d), s.p2);
-            }
-            to_phys<P, T>(a, v, buf, tw, t);
-            st_put<P, T>(w2s, v, t);
-            // Gi = G - FFT(2 xi w2)/N
-            st_get<P, T>(u, xis, t);
-#pragma unroll
-            for (int m = 0; m < P; ++m) v[m] = make_float2(2.f * u[m].x * v[m].x, 2.f * u[m].y * v[m].y);
-            to_spec<P, T>(a, v, buf, tw, t, true);
-#pragma unroll
-            for (int m = 0; m < P; ++m) G[m] = csub(G[m], v[m]);
-        }
-        // w1 = IFFT(d phi1 Gi); Sacc += phi1 Gi
-#pragma unroll
-        for (int m = 0; m < P; ++m) {
-            const Slot s = slot<P, T>(a, c, m, false);
-            v[m] = cscale(dmul(G[m], s.d), s.p1);
-            Sacc[m] = cadd(Sacc[m], rmul(G[m], s.p1, s.p1b));
-        }
-        to_phys<P, T>(a, v, buf, tw, t);
-        // ETRK2: P1 = 2 x (w2 - w1);  ETD1: P1 = -2 x w1
-        st_get<P, T>(u, xs, t);
-        if (rk2) {
-            float2 w2[P];
-            st_get<P, T>(w2, w2s, t);
-#pragma unroll
-            for (int m = 0; m < P; ++m)
-                v[m] = make_float2(2.f * u[m].x * (w2[m].x - v[m].x), 2.f * u[m].y * (w2[m].y - v[m].y));
-        } else {
-#pragma unroll
-            for (int m = 0; m < P; ++m) v[m] = make_float2(-2.f * u[m].x * v[m].x, -2.f * u[m].y * v[m].y);
-        }
-        to_spec<P, T>(a, v, buf, tw, t, true);
-#pragma unroll
-        for (int m = 0; m < P; ++m) {
-            const Slot s = slot<P, T>(a, c, m, false);
-            G[m] = cadd(rmul(G[m], s.E, s.Eb), v[m]);
-        }
+        for (int m = 0; m < P; ++m) v[m] = k == 0 ? G[m] : Sacc[m];
+        if (a.split) to_packed<P, T>(v, c.t, buf.a);
+        fft_inv<P, T>(v, buf, tw, c.t);
+        store_pair<P, T>(dst, v, c, N);
     }
 }
 
@@ -845,25 +880,24 @@ __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
-    float2 x0[P], G[P], Sacc[P], SS[P];
-    source_spec<P, T>(a, c, SS, buf, tw);
-    load_pair<P, T>(x0, a.u, c, N);
-    if (a.cu) add_pair<P, T>(x0, a.cu, c, N);
-    load_pair<P, T>(G, a.g_out, c, N);
-    to_spec<P, T>(a, G, buf, tw, t, true);
+    SlotCache<P, T> cc;
+    cc.load(a, c);
+    float2 G[P], Sacc[P], SS[P];
+    adjoint_prologue<P, T>(a, c, cc, a.g_out, SS, G, buf, tw);
+    {
+        float2 x0[P];
+        load_pair<P, T>(x0, a.u, c, N);
+        if (a.cu) add_pair<P, T>(x0, a.cu, c, N);
+        st_put<P, T>(st + 4 * N, x0, t);
+    }
 #pragma unroll
     for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
-    step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, tw, st);
-    to_phys<P, T>(a, G, buf, tw, t);
-    store_pair<P, T>(a.g_u, G, c, N);
-    if (a.g_s) {
-        to_phys<P, T>(a, Sacc, buf, tw, t);
-        store_pair<P, T>(a.g_s, Sacc, c, N);
-    }
+    step_bwd_program<P, T>(a, c, cc, SS, G, Sacc, nullptr, 0, 0, st + 4 * N, st, buf, tw);
+    adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
 
-// Backward of the fused rollout: segments of ckpt_every steps are replayed from
-// their checkpoint into shared memory, then differentiated step by step.
+// Backward of the fused rollout: each ckpt_every-step segment is replayed from
+// its checkpoint (states kept in shared memory), then differentiated step by step.
 template <int P, int T>
 __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     extern __shared__ float2 sm[];
@@ -878,14 +912,10 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
+    SlotCache<P, T> cc;
+    cc.load(a, c);
     float2 G[P], Sacc[P], SS[P];
-    source_spec<P, T>(a, c, SS, buf, tw);
-    if (a.g_final) load_pair<P, T>(G, a.g_final, c, N);
-    else {
-#pragma unroll
-        for (int m = 0; m < P; ++m) G[m] = make_float2(0.f, 0.f);
-    }
-    to_spec<P, T>(a, G, buf, tw, t, true);
+    adjoint_prologue<P, T>(a, c, cc, a.g_final, SS, G, buf, tw);
 #pragma unroll
     for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
     const int nseg = (a.steps + K - 1) / K;
@@ -893,39 +923,18 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
         const int k0 = sidx * K;
         const int len = min(K, a.steps - k0);
         {
-            float2 x[P], X[P];
+            float2 x[P];
             load_pair_strided<P, T>(x, a.ckpts, c, N, (int64_t)nseg * N, (int64_t)sidx * N);
-#pragma unroll
-            for (int m = 0; m < P; ++m) X[m] = x[m];
-            to_spec<P, T>(a, X, buf, tw, t, true);
-            for (int j = 0; j < len; ++j) {
-                st_put<P, T>(seg + j * N, x, t);
-                if (j + 1 < len) {
-#pragma unroll 1
-                    for (int sub = 0; sub < 2; ++sub) substep<P, T>(a, c, x, X, SS, buf, tw, nullptr);
-                }
-            }
+            forward_program<P, T>(a, c, x, len - 1, buf, tw, false, nseg, false, seg);
+            st_put<P, T>(seg + (len - 1) * N, x, t);
         }
         for (int j = len - 1; j >= 0; --j) {
             const int k = k0 + j;
-            if (a.g_frames) {
-                float2 gf[P];
-                load_pair_strided<P, T>(gf, a.g_frames, c, N, (int64_t)a.steps * N, (int64_t)k * N);
-                to_spec<P, T>(a, gf, buf, tw, t, true);
-#pragma unroll
-                for (int m = 0; m < P; ++m) G[m] = cadd(G[m], gf[m]);
-            }
-            float2 x0[P];
-            st_get<P, T>(x0, seg + j * N, t);
-            step_bwd<P, T>(a, c, x0, G, Sacc, SS, buf, tw, st);
+            step_bwd_program<P, T>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N,
+                                   seg + j * N, st, buf, tw);
         }
     }
-    to_phys<P, T>(a, G, buf, tw, t);
-    store_pair<P, T>(a.g_u, G, c, N);
-    if (a.g_s) {
-        to_phys<P, T>(a, Sacc, buf, tw, t);
-        store_pair<P, T>(a.g_s, Sacc, c, N);
-    }
+    adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
 
 // ---- launchers (instantiated per shape in ks_{fwd,bwd}_*.cu) ---------------------
