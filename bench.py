@@ -53,6 +53,8 @@ def parse_args():
     ap.add_argument("--profile", nargs="?", const="ks", default=None,
                     choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd"],
                     help="a small case of one kernel for ncu (no JSON)")
+    ap.add_argument("--profile-rows", type=int, default=1024, help="rows of the KS profile case")
+    ap.add_argument("--tpp", type=int, default=32, help="threads per row pair of the KS profile case")
     return ap.parse_args()
 
 
@@ -653,7 +655,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=dev)
     if args.profile:
-        profile_small(dev, args.profile)
+        profile_small(dev, args.profile, args.profile_rows, args.tpp)
         return
     if args.workload in ("burgers_diff", "ks_diff"):
         cfg, cells, times, extra = bench_diff(args, dev, world, args.workload)
@@ -737,9 +739,10 @@ def main():
         torch.distributed.destroy_process_group()
 
 
-def profile_small(dev, which="ks"):
-    """Small cases for ncu captures: the KS fused rollout (B=512, N=256, 64 steps) and its
-    backward, the ragged Burgers batch (1024 rows, 20 steps) or the 32x128 Burgers rollout."""
+def profile_small(dev, which="ks", rows=1024, tpp=32):
+    """Small cases for ncu captures: the KS fused rollout (rows x 256, 64 steps, `tpp` threads
+    per row pair) and its backward, the ragged Burgers batch (1024 rows, 20 steps) or the
+    32x128 Burgers rollout."""
     import torch
     from types import SimpleNamespace
     if which == "burgers_ragged":
@@ -767,11 +770,12 @@ def profile_small(dev, which="ks"):
         return
     from inc_b200.solvers import KSSolverTorch
     from inc_b200.workloads import ks_plain_config
-    cfg = ks_plain_config(B=512, steps=64)
+    cfg = ks_plain_config(B=rows, steps=64)
     B, N = cfg["B"], cfg["N"]
     ds = torch.full((B,), cfg["L"], device=dev)
     solver = KSSolverTorch(SimpleNamespace(resolution=N, dt=cfg["dt"], device=dev, domain_size=ds,
-                                           alpha=torch.zeros(B, device=dev), time_scheme="ETRK2"))
+                                           alpha=torch.zeros(B, device=dev), time_scheme="ETRK2",
+                                           threads_per_pair=tpp))
     u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=dev)
     s = torch.tensor(cfg["s"], dtype=torch.float32, device=dev)
     plan = solver.plan_for(u0, ds)

@@ -120,7 +120,7 @@ int pick_block(Kind kind, int npairs, int T, int n, int K) {
     while (block > 32 && (int64_t)npairs * T / block < 2 * 148) block >>= 1;
     auto smem = [&](int b) {
         const int groups = b / T;
-        int64_t per = 2 * (n + 8);
+        int64_t per = 2 * (n + n / 4 + 64) + 16;  // bound on the exchange buffers' padded layouts
         if (kind == Kind::StepBwd || kind == Kind::RolloutBwd) per += 5 * n;
         if (kind == Kind::RolloutBwd) per += (int64_t)K * n;
         return (int64_t)(4 * n + groups * per) * 8;

@@ -1,11 +1,11 @@
 // Kuramoto-Sivashinsky pseudo-spectral ETRK2 / ETD1 stepper for sm_100a.
 //
 // Two rows a, b share one complex FFT of length N: z = u_a + i u_b.  A row pair
-// is owned by a group of T lanes (T <= 32, inside one warp); lane t holds the
+// is owned by a group of T lanes (T <= 64; a group wider than a warp syncs on the CTA barrier); lane t holds the
 // P = N/T values z[t + T*m] in register m, for physical and spectral data
-// alike.  An FFT is two Stockham passes: a P-point DFT in registers, one
-// exchange through a swizzled shared-memory tile, then T-point DFTs in
-// registers with FP64-derived twiddles.  Every operator of the step is a
+// alike.  An FFT is a P-point DFT in registers followed by Stockham passes
+// of radix <= P, each reading the previous pass's output through a padded
+// shared-memory buffer, with FP64-derived twiddles.  Every operator of the step is a
 // Fourier multiplier or a pointwise product, so the whole step (both
 // substeps) runs in registers with four FFTs per substep.
 //
@@ -21,10 +21,23 @@
 // is zero at the Nyquist bin: the reference's value there is purely imaginary
 // and is discarded by ifft(.).real, so the two are the same map.
 #pragma once
+#include <utility>
+
 #include "common.cuh"
 
 namespace inc {
 namespace ks {
+
+// Compile-time loop: f(std::integral_constant<int, i>) for i in [0, N), so
+// that indices derived from i are constant expressions (shared-memory offsets).
+template <typename F, int... I>
+INC_DEV void static_for_impl(F&& f, std::integer_sequence<int, I...>) {
+    (f(std::integral_constant<int, I>{}), ...);
+}
+template <int N, typename F>
+INC_DEV void static_for(F&& f) {
+    static_for_impl(f, std::make_integer_sequence<int, N>{});
+}
 
 // ---- complex helpers ---------------------------------------------------------
 INC_DEV float2 cadd(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
@@ -147,9 +160,86 @@ INC_DEV constexpr bool twiddles_in_registers() { return lane_twiddles(P, T) <= 1
 template <int P, int T>
 INC_DEV constexpr int reg_twiddles() { return twiddles_in_registers<P, T>() ? lane_twiddles(P, T) : 1; }
 
-INC_DEV constexpr int padx(int i) { return i + (i >> 4); }
-template <int N>
-INC_DEV constexpr int buf_len() { return N + N / 16 + 8; }  // + 8 staggers the groups of a warp
+// Shared-memory layout of the exchanges.  Exchange e is the buffer written by
+// the pass with span ex_span(e) (e = 0: the register pass) and read by the
+// next pass.  Each exchange has its own linear map lay(e, i) = sum of
+// weight(e, j) over the set bits j of the logical index i: the weights are
+// superincreasing (so the map is injective) and, modulo the 16 float2 banks,
+// send the index bits that vary across the lanes of a half-warp to distinct
+// bank bits for both the write pattern and the read pattern of that exchange.
+// Every access is then conflict-free, and because the map is additive over
+// disjoint bits, every address is a per-lane base plus a compile-time constant.
+// Groups narrower than 16 lanes share a half-warp; their stride supplies the
+// remaining bank bits (group_stride).
+INC_DEV constexpr int ilog2(int x) {
+    int r = 0;
+    while ((2 << r) <= x) ++r;
+    return r;
+}
+INC_DEV constexpr int ex_span(int P, int T, int e) {
+    int ns = 1, R = P;
+    for (int k = 0; k < e; ++k) { ns *= R; R = pass_radix(P, T, ns); }
+    return ns;
+}
+INC_DEV constexpr int ex_radix(int P, int T, int e) {
+    int ns = 1, R = P;
+    for (int k = 0; k < e; ++k) { ns *= R; R = pass_radix(P, T, ns); }
+    return R;
+}
+// lane-varying bits of one half-warp: 4, or log2(T) for narrower groups
+INC_DEV constexpr int lane_bits(int T) { return T >= 16 ? 4 : ilog2(T); }
+// bank weight (a power of two, or 0) of index bit j in exchange e
+INC_DEV constexpr int lay_bank(int P, int T, int e, int j) {
+    const int lgNS = ilog2(ex_span(P, T, e)), lgR = ilog2(ex_radix(P, T, e)), nb = lane_bits(T);
+    int sw = 0;  // index bits the write pattern varies across a half-warp
+    for (int b = 0; b < nb; ++b) sw |= 1 << (b < lgNS ? b : b + lgR);
+    if (j < nb) return 1 << j;  // the read pattern varies bits [0, nb)
+    if (!((sw >> j) & 1)) return 0;
+    int used = sw & ((1 << nb) - 1);
+    for (int k = nb; k <= j; ++k) {
+        if (!((sw >> k) & 1)) continue;
+        int nx = 0;
+        while ((used >> nx) & 1) ++nx;
+        if (k == j) return 1 << nx;
+        used |= 1 << nx;
+    }
+    return 0;
+}
+INC_DEV constexpr int lay_weight(int P, int T, int e, int j) {
+    int sum = 0, w = 0;
+    for (int k = 0; k <= j; ++k) {
+        const int base = (1 << k) > sum + 1 ? (1 << k) : sum + 1;
+        w = base + (((lay_bank(P, T, e, k) - base) % 16) + 16) % 16;
+        sum += w;
+    }
+    return w;
+}
+INC_DEV constexpr int lay(int P, int T, int e, int i) {
+    int out = 0;
+    for (int j = 0; (1 << j) < P * T; ++j)
+        if ((i >> j) & 1) out += lay_weight(P, T, e, j);
+    return out;
+}
+// written index of the lane-dependent part j of a pass with span ns, radix R
+INC_DEV constexpr int spread(int j, int ns, int R) { return (j / ns) * ns * R + j % ns; }
+INC_DEV constexpr int num_exchanges(int P, int T) { return num_later_passes(P, T); }
+template <int P, int T>
+INC_DEV constexpr int buf_len() {
+    int len = P * T;  // buffer a doubles as the mirror scratch
+    for (int e = 0; e < num_exchanges(P, T); ++e) {
+        const int l = lay(P, T, e, P * T - 1) + 1;
+        len = l > len ? l : len;
+    }
+    return len;
+}
+// per-group shared size rounded so that groups of one half-warp land on distinct bank bits
+template <int T>
+INC_DEV constexpr int group_stride(int size) {
+    const int r = T >= 16 ? 0 : (1 << ilog2(T)) % 16;
+    int s = size;
+    while (s % 16 != r) ++s;
+    return s;
+}
 
 template <int T>
 INC_DEV void group_sync() {
@@ -157,10 +247,37 @@ INC_DEV void group_sync() {
     else __syncthreads();
 }
 
+// A group's two exchange buffers and this lane's bases in them: w[e] where
+// the pass writing exchange e stores, r[e] where the next pass loads.
+template <int P, int T>
 struct Buf {
+    static constexpr int NE = num_exchanges(P, T) > 0 ? num_exchanges(P, T) : 1;
     float2* a;
     float2* b;
+    float2* w[NE];
+    const float2* r[NE];
 };
+
+template <int P, int T, int E>
+INC_DEV int lay_rt(int i) {
+    int out = 0;
+    static_for<ilog2(P * T)>([&](auto jc) {
+        constexpr int j = decltype(jc)::value;
+        constexpr int w = lay_weight(P, T, E, j);
+        out += ((i >> j) & 1) * w;
+    });
+    return out;
+}
+
+template <int P, int T, int E>
+INC_DEV void set_lane_bases(Buf<P, T>& b, int t) {
+    if constexpr (E < num_exchanges(P, T)) {
+        float2* base = (E % 2) ? b.b : b.a;
+        b.w[E] = base + lay_rt<P, T, E>(spread(t, ex_span(P, T, E), ex_radix(P, T, E)));
+        b.r[E] = base + lay_rt<P, T, E>(t);
+        set_lane_bases<P, T, E + 1>(b, t);
+    }
+}
 
 // Twiddles of the later passes: in registers (reg) or in the shared table (sm).
 template <int P, int T>
@@ -186,61 +303,73 @@ INC_DEV void load_lane_twiddles(Twiddles<P, T>& tw, const float2* table, int t) 
 }
 
 template <int P, int T, int NS>
-INC_DEV void fft_later(float2 (&v)[P], float2* src, float2* dst, const Twiddles<P, T>& tw, int t) {
+INC_DEV void fft_later(float2 (&v)[P], const Buf<P, T>& buf, const Twiddles<P, T>& tw, int t) {
     constexpr int N = P * T;
     if constexpr (NS < N) {
         constexpr int R = pass_radix(P, T, NS);
         constexpr int Q = P / R;
         constexpr bool LAST = NS * R == N;
         constexpr int TOFF = lane_twiddle_offset(P, T, NS);
-        const float2* twp = tw.sm + pass_index(P, T, NS) * N;
+        constexpr int E = pass_index(P, T, NS);  // the exchange this pass reads
+        const float2* twp = tw.sm + E * N;
         group_sync<T>();
-#pragma unroll
-        for (int q = 0; q < Q; ++q) {
-            const int j = t + T * q;
-            const float2* rd = src + padx(j);
+        static_for<Q>([&](auto qc) {
+            constexpr int q = decltype(qc)::value;
             float2 w[R];
-#pragma unroll
-            for (int r = 0; r < R; ++r) {
-                float2 y = rd[padx(r * (N / R))];
-                if (r > 0) {
+            static_for<R>([&](auto rc) {
+                constexpr int r = decltype(rc)::value;
+                constexpr int off = lay(P, T, E, T * q + r * (N / R));
+                float2 y = buf.r[E][off];
+                if constexpr (r > 0) {
                     if constexpr (twiddles_in_registers<P, T>()) y = cmul(y, tw.reg[TOFF + q * (R - 1) + r - 1]);
                     else y = cmul(y, twp[(q * R + r) * T + t]);
                 }
                 w[r] = y;
-            }
+            });
             dft_reg<R, false>(w);
             if constexpr (LAST) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) v[q + Q * r] = w[r];
             } else {
-                float2* wr = dst + padx((j / NS) * NS * R + (j % NS));
-#pragma unroll
-                for (int r = 0; r < R; ++r) wr[padx(r * NS)] = w[r];
+                static_for<R>([&](auto rc) {
+                    constexpr int r = decltype(rc)::value;
+                    constexpr int off = lay(P, T, E + 1, spread(T * q, NS, R) + r * NS);
+                    buf.w[E + 1][off] = w[r];
+                });
             }
-        }
-        if constexpr (!LAST) fft_later<P, T, NS * R>(v, dst, src, tw, t);
+        });
+        if constexpr (!LAST) fft_later<P, T, NS * R>(v, buf, tw, t);
     }
 }
 
+// Unnormalised forward DFT of the group's row pair, natural order in and out.
 template <int P, int T>
-INC_DEV void fft_fwd(float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t) {
+INC_DEV void fft_fwd(float2 (&v)[P], const Buf<P, T>& buf, const Twiddles<P, T>& tw, int t) {
     dft_reg<P, false>(v);
-    group_sync<T>();  // the previous transform's last reads are done
-    float2* wr = buf.a + padx(t * P);
-#pragma unroll
-    for (int r = 0; r < P; ++r) wr[padx(r)] = v[r];
-    fft_later<P, T, P>(v, buf.a, buf.b, tw, t);
+    // With an odd number of exchanges the previous transform's last pass read
+    // buffer a, which this one writes first; with an even number a was last
+    // read before that pass's barrier.
+    if constexpr (num_exchanges(P, T) % 2 == 1 || num_exchanges(P, T) == 0) group_sync<T>();
+    if constexpr (num_exchanges(P, T) > 0) {
+        static_for<P>([&](auto rc) {
+            constexpr int r = decltype(rc)::value;
+            constexpr int off = lay(P, T, 0, r);
+            buf.w[0][off] = v[r];
+        });
+        fft_later<P, T, P>(v, buf, tw, t);
+    }
 }
 
-// Unnormalised inverse FFT: conj(FFT(conj(v))).
+// (re, im) -> (im, re): the unnormalised inverse DFT is swap(FFT(swap(v))).
+INC_DEV float2 cswap(float2 z) { return make_float2(z.y, z.x); }
+
 template <int P, int T>
-INC_DEV void fft_inv(float2 (&v)[P], Buf buf, const Twiddles<P, T>& tw, int t) {
+INC_DEV void fft_inv(float2 (&v)[P], const Buf<P, T>& buf, const Twiddles<P, T>& tw, int t) {
 #pragma unroll
-    for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+    for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
     fft_fwd<P, T>(v, buf, tw, t);
 #pragma unroll
-    for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+    for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
 }
 
 // ---- mirror exchange: slot k <-> slot N-k --------------------------------------
@@ -268,6 +397,7 @@ INC_DEV void mirror(const float2 (&v)[P], float2 (&mv)[P], int t, float2* scratc
         group_sync<T>();
 #pragma unroll
         for (int m = 0; m < P; ++m) mv[m] = scratch[(N - (t + T * m)) & (N - 1)];
+        group_sync<T>();  // the scratch is exchange buffer a, which the next transform may write first
     }
 }
 
@@ -482,12 +612,14 @@ INC_DEV float2 sq2(float2 x) { return make_float2(x.x * x.x, x.y * x.y); }
 
 // ---- shared memory ----------------------------------------------------------------
 // Per CTA: the twiddle table of the later passes ((passes-1) * N float2), then
-// per group its two FFT buffers (N + 8 each; the 8-entry pad staggers the
-// groups of one warp across banks) and, for the backward kernels, state slots.
+// per group its two exchange buffers and, for the backward kernels, state slots.
 template <int P, int T>
 INC_DEV constexpr int tw_size() { return twiddles_in_registers<P, T>() ? 0 : num_later_passes(P, T) * P * T; }
+// Per group: the two exchange buffers, then (backward kernels) state slots.
 template <int P, int T>
-INC_DEV constexpr int fft_buf_size() { return 2 * buf_len<P * T>(); }
+INC_DEV constexpr int fwd_group_smem() { return group_stride<T>(2 * buf_len<P, T>()); }
+template <int P, int T>
+INC_DEV constexpr int bwd_group_smem(int K) { return group_stride<T>(2 * buf_len<P, T>() + (5 + K) * P * T); }
 
 template <int P, int T>
 INC_DEV float2* group_smem(float2* sm, int per_group) {
@@ -495,8 +627,12 @@ INC_DEV float2* group_smem(float2* sm, int per_group) {
 }
 
 template <int P, int T>
-INC_DEV Buf group_buf(float2* g) {
-    return Buf{g, g + buf_len<P * T>()};
+INC_DEV Buf<P, T> group_buf(float2* g, int t) {
+    Buf<P, T> b;
+    b.a = g;
+    b.b = g + buf_len<P, T>();
+    set_lane_bases<P, T, 0>(b, t);
+    return b;
 }
 
 // The block's shared twiddle table (when lanes do not hold them in registers)
@@ -532,35 +668,47 @@ INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
 // seg (optional): shared memory receiving the state at the start of every step,
 // in lane layout [step][m][t] (the backward replay).  ckpt_on: store checkpoints.
 template <int P, int T>
-INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, Buf buf,
+INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, const Buf<P, T>& buf,
                              const Twiddles<P, T>& tw, bool frames_on, int nseg, bool ckpt_on = true,
                              float2* seg = nullptr) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
     const int per_sub = rk2 ? 4 : 2;
-    const int per_step = 2 * per_sub;
     const int pro = a.s ? 2 : 1;
-    const int total = pro + steps * per_step;
+    const int total = pro + steps * 2 * per_sub;
     float2 X[P], SS[P], v[P];
     SlotCache<P, T> cc;
     cc.load(a, c);
 #pragma unroll
     for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
+    // Position of the next phase: f-th transform of substep `sub` of step()
+    // `step`; the checkpoint countdown runs alongside (no divisions in the loop).
+    int f = 0, sub = 0, step = 0, ck_left = 0, ck_idx = 0;
 #pragma unroll 1
     for (int ph = 0; ph < total; ++ph) {
-        int kind, step = 0, q = 0;
+        int kind, cur = 0;
+        bool step_end = false;
         if (ph < pro) {
             kind = (ph == 0 && a.s) ? PH_S : PH_U;
         } else {
-            q = ph - pro;
-            step = q / per_step;
-            const int f = (q % per_step) % per_sub;
+            cur = step;
             kind = (f & 1) ? PH_INV : (f == 0 ? PH_NL1 : PH_NL2);
-            if (q % per_step == 0) {
-                if (ckpt_on && a.ckpts && step % a.ckpt_every == 0)
-                    store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)(step / a.ckpt_every) * N);
+            if (f == 0 && sub == 0) {
+                if (ckpt_on && a.ckpts) {
+                    if (ck_left == 0) {
+                        store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)ck_idx * N);
+                        ++ck_idx;
+                        ck_left = a.ckpt_every;
+                    }
+                    --ck_left;
+                }
                 if (seg) st_put<P, T>(seg + step * N, x, t);
+            }
+            step_end = sub == 1 && f == per_sub - 1;
+            if (++f == per_sub) {
+                f = 0;
+                if (++sub == 2) { sub = 0; ++step; }
             }
         }
         // operand of this transform
@@ -576,9 +724,9 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
         fft_fwd<P, T>(v, buf, tw, t);
         if (kind == PH_INV) {
 #pragma unroll
-            for (int m = 0; m < P; ++m) x[m] = make_float2(v[m].x, -v[m].y);
-            if (frames_on && (q % per_step) == per_step - 1)
-                store_pair_strided<P, T>(a.frames, x, c, N, (int64_t)a.steps * N, (int64_t)step * N);
+            for (int m = 0; m < P; ++m) x[m] = cswap(v[m]);
+            if (frames_on && step_end)
+                store_pair_strided<P, T>(a.frames, x, c, N, (int64_t)a.steps * N, (int64_t)cur * N);
             continue;
         }
         if (a.split) to_split<P, T>(v, t, buf.a);
@@ -614,7 +762,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
         }
         if (a.split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
-        for (int m = 0; m < P; ++m) v[m].y = -v[m].y;  // the next transform is an inverse
+        for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);  // the next transform is an inverse
     }
 }
 
@@ -624,7 +772,7 @@ __global__ void __launch_bounds__(128) k_step(Args a) {
     constexpr int N = P * T;
     const int t = threadIdx.x % T;
     const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
-    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
+    const Buf<P, T> buf = group_buf<P, T>(group_smem<P, T>(sm, fwd_group_smem<P, T>()), t);
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
@@ -642,7 +790,7 @@ __global__ void __launch_bounds__(128) k_rollout(Args a) {
     constexpr int N = P * T;
     const int t = threadIdx.x % T;
     const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
-    const Buf buf = group_buf<P, T>(group_smem<P, T>(sm, fft_buf_size<P, T>()));
+    const Buf<P, T> buf = group_buf<P, T>(group_smem<P, T>(sm, fwd_group_smem<P, T>()), t);
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
@@ -690,7 +838,7 @@ INC_DEV void pair_mul2(float2 (&v)[P], const float2 (&x)[P], float s) {
 template <int P, int T>
 INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>& cc, const float2 (&SS)[P],
                               float2 (&G)[P], float2 (&Sacc)[P], const float* gframe, int64_t gf_row_stride,
-                              int64_t gf_off, const float2* x0s, float2* st, Buf buf, const Twiddles<P, T>& tw) {
+                              int64_t gf_off, const float2* x0s, float2* st, const Buf<P, T>& buf, const Twiddles<P, T>& tw) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
@@ -703,19 +851,18 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
     float2* xi2s = st + 2 * N;
     float2* w2s = st + 3 * N;
     float2 X[P], v[P], u[P];
+    int f = 0, sub = 1;  // adjoint phases: f-th transform of substep `sub` (second substep first)
 #pragma unroll 1
     for (int ph = 0; ph < total; ++ph) {
         const int q = ph - lead;
-        int kind, sub = 0;
+        int kind, cur = sub;
         if (q < 0) {
             kind = B_GF;
         } else if (q < nrec) {
             kind = recompute_kind(rk2, q);
         } else {
-            const int r = q - nrec;
-            sub = 1 - r / per;
-            const int f = r % per;
             kind = rk2 ? (f == 0 ? B_W2 : (f == 1 ? B_GI : (f == 2 ? B_W1 : B_GP))) : (f == 0 ? B_W1 : B_GP);
+            if (++f == per) { f = 0; --sub; }
         }
         // ---- operand of this transform
         switch (kind) {
@@ -742,14 +889,14 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
                 }
                 if (a.split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
-                for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+                for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
                 break;
             case B_GI:  // v holds w2
-                st_get<P, T>(u, sub ? xi2s : xi1s, t);
+                st_get<P, T>(u, cur ? xi2s : xi1s, t);
                 pair_mul2<P, T>(v, u, 2.f);
                 break;
             case B_GP:  // v holds w1
-                st_get<P, T>(u, sub ? x1s : x0s, t);
+                st_get<P, T>(u, cur ? x1s : x0s, t);
                 if (rk2) {
                     float2 w2[P];
                     st_get<P, T>(w2, w2s, t);
@@ -767,7 +914,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
         const bool inverse = kind == B_INV_XI1 || kind == B_INV_X1 || kind == B_INV_XI2 || kind == B_W2 || kind == B_W1;
         if (inverse) {
 #pragma unroll
-            for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+            for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
             if (kind == B_INV_XI1) st_put<P, T>(xi1s, v, t);
             else if (kind == B_INV_X1) st_put<P, T>(x1s, v, t);
             else if (kind == B_INV_XI2) st_put<P, T>(xi2s, v, t);
@@ -813,7 +960,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
         }
         if (a.split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
-        for (int m = 0; m < P; ++m) v[m].y = -v[m].y;
+        for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
     }
 }
 
@@ -821,7 +968,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
 // adjoint field g (null: zero), as one loop around one transform.
 template <int P, int T>
 INC_DEV void adjoint_prologue(const Args& a, const Ctx& c, const SlotCache<P, T>& cc, const float* g,
-                              float2 (&SS)[P], float2 (&G)[P], Buf buf, const Twiddles<P, T>& tw) {
+                              float2 (&SS)[P], float2 (&G)[P], const Buf<P, T>& buf, const Twiddles<P, T>& tw) {
     constexpr int N = P * T;
 #pragma unroll
     for (int m = 0; m < P; ++m) { SS[m] = make_float2(0.f, 0.f); G[m] = make_float2(0.f, 0.f); }
@@ -848,7 +995,7 @@ INC_DEV void adjoint_prologue(const Args& a, const Ctx& c, const SlotCache<P, T>
 
 // dL/du = IFFT(G) and dL/ds = IFFT(Sacc) stored to the caller's arrays.
 template <int P, int T>
-INC_DEV void adjoint_epilogue(const Args& a, const Ctx& c, const float2 (&G)[P], const float2 (&Sacc)[P], Buf buf,
+INC_DEV void adjoint_epilogue(const Args& a, const Ctx& c, const float2 (&G)[P], const float2 (&Sacc)[P], const Buf<P, T>& buf,
                               const Twiddles<P, T>& tw) {
     constexpr int N = P * T;
 #pragma unroll 1
@@ -864,9 +1011,6 @@ INC_DEV void adjoint_epilogue(const Args& a, const Ctx& c, const float2 (&G)[P],
     }
 }
 
-// Shared memory per group of the backward kernels: FFT buffers + 5 state slots.
-template <int P, int T>
-INC_DEV constexpr int bwd_group_smem() { return fft_buf_size<P, T>() + 5 * P * T; }
 
 template <int P, int T>
 __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
@@ -874,9 +1018,9 @@ __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
     constexpr int N = P * T;
     const int t = threadIdx.x % T;
     const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
-    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>());
-    const Buf buf = group_buf<P, T>(g);
-    float2* st = g + fft_buf_size<P, T>();
+    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>(0));
+    const Buf<P, T> buf = group_buf<P, T>(g, t);
+    float2* st = g + 2 * buf_len<P, T>();
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
@@ -905,9 +1049,9 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     const int t = threadIdx.x % T;
     const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
     const int K = a.ckpt_every;
-    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>() + K * N);
-    const Buf buf = group_buf<P, T>(g);
-    float2* st = g + fft_buf_size<P, T>();
+    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>(K));
+    const Buf<P, T> buf = group_buf<P, T>(g, t);
+    float2* st = g + 2 * buf_len<P, T>();
     float2* seg = st + 5 * N;
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
@@ -947,10 +1091,9 @@ int launch_bwd(Kind kind, const Args& a, cudaStream_t st, int block);
 
 template <int P, int T>
 size_t smem_bytes(Kind kind, int block, int K) {
-    constexpr int N = P * T;
     const int groups = block / T;
-    size_t per = (kind == Kind::Step || kind == Kind::Rollout) ? fft_buf_size<P, T>()
-               : (kind == Kind::StepBwd ? bwd_group_smem<P, T>() : bwd_group_smem<P, T>() + (size_t)K * N);
+    size_t per = (kind == Kind::Step || kind == Kind::Rollout) ? fwd_group_smem<P, T>()
+               : bwd_group_smem<P, T>(kind == Kind::StepBwd ? 0 : K);
     return (tw_size<P, T>() + groups * per) * sizeof(float2);
 }
 

@@ -37,7 +37,7 @@ __global__ void __launch_bounds__(128) k_spectrum(const float* __restrict__ v, f
     Twiddles<P, T> tw;
     tw.sm = nullptr;
     compute_lane_twiddles<P, T>(tw, t);
-    const Buf buf = group_buf<P, T>(sm + (threadIdx.x / T) * fft_buf_size<P, T>());
+    const Buf<P, T> buf = group_buf<P, T>(sm + (threadIdx.x / T) * fwd_group_smem<P, T>(), t);
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     const int ra = 2 * pair, rb = 2 * pair + 1 < rows ? 2 * pair + 1 : -1;
     const bool valid = ra < rows;
@@ -72,7 +72,7 @@ int launch_spectrum(const float* v, float* out, int rows, cudaStream_t st) {
     const int block = T > 32 ? T : 128;
     const int gpb = block / T;
     const int grid = (npairs + gpb - 1) / gpb;
-    const size_t smem = (size_t)gpb * fft_buf_size<P, T>() * sizeof(float2);
+    const size_t smem = (size_t)gpb * fwd_group_smem<P, T>() * sizeof(float2);
     k_spectrum<P, T><<<grid, block, smem, st>>>(v, out, rows);
     return check_launch("energy_spectrum");
 }
