@@ -477,6 +477,7 @@ INC_DEV void make_ctx(const Args& a, int pair, int t, bool valid, Ctx& c) {
 // storage, whose .x belongs to row a and .y to row b (real multipliers there).
 struct Slot {
     float E, p1, p2, d;  // d: derivative multiplier is -i*d (unscaled)
+    float dn;            // d / N
     float Eb, p1b, p2b;
     bool sp;
 };
@@ -496,6 +497,7 @@ INC_DEV Slot slot(const Args& a, const Ctx& c, int m, bool need_p2) {
     int f = (k < N / 2) ? k : (k == N / 2 ? 0 : k - N);
     if (a.dealias && 3 * abs(f) > N) f = 0;
     s.d = (float)f * ((a.split && up) ? c.dRb : c.dRa);
+    s.dn = s.d * a.invN;
     s.sp = a.split && (k == 0 || k == N / 2);
     if (s.sp) {
         const float* cb = a.coef + (int64_t)c.rbc * 3 * a.nhp;
@@ -514,7 +516,7 @@ template <int P, int T>
 struct SlotCache {
     static constexpr bool ON = P <= 8;
     static constexpr int M = ON ? P : 1;
-    float E[M], p1[M], p2[M], d[M];
+    float E[M], p1[M], p2[M], d[M], dn[M];
     float Eb[2], p1b[2], p2b[2];  // row b at slots 0 and N/2 (split storage)
 
     INC_DEV void load(const Args& a, const Ctx& c) {
@@ -522,7 +524,7 @@ struct SlotCache {
 #pragma unroll
             for (int m = 0; m < P; ++m) {
                 const Slot s = slot<P, T>(a, c, m, true);
-                E[m] = s.E; p1[m] = s.p1; p2[m] = s.p2; d[m] = s.d;
+                E[m] = s.E; p1[m] = s.p1; p2[m] = s.p2; d[m] = s.d; dn[m] = s.dn;
                 if (m == 0 || m == P / 2) {
                     const int i = m == 0 ? 0 : 1;
                     Eb[i] = s.Eb; p1b[i] = s.p1b; p2b[i] = s.p2b;
@@ -534,7 +536,7 @@ struct SlotCache {
     INC_DEV Slot get(const Args& a, const Ctx& c, int m, bool need_p2) const {
         if constexpr (ON) {
             Slot s;
-            s.E = E[m]; s.p1 = p1[m]; s.p2 = p2[m]; s.d = d[m];
+            s.E = E[m]; s.p1 = p1[m]; s.p2 = p2[m]; s.d = d[m]; s.dn = dn[m];
             if (m == 0 || m == P / 2) {
                 const int i = m == 0 ? 0 : 1;
                 s.Eb = Eb[i]; s.p1b = p1b[i]; s.p2b = p2b[i];
@@ -648,12 +650,11 @@ INC_DEV Twiddles<P, T> setup_twiddles(const Args& a, float2* sm, int t) {
 }
 
 // ---- the forward program ------------------------------------------------------------
-// A rollout is a sequence of FFT phases: [FFT(s)] FFT(u), then per step() and
-// substep FFT(u^2) -> stage 1 -> IFFT -> [FFT(ui^2) -> stage 2 -> IFFT] (the
-// bracketed half for ETRK2).  Running them as one loop around a single FFT
-// keeps one copy of the transform in the kernel's code.
-enum Phase { PH_S, PH_U, PH_NL1, PH_NL2, PH_INV };
-
+// A rollout is a prologue ([FFT(s)], FFT(u)) and then a loop of half-substeps,
+// each FFT(x^2) -> stage multiplier -> IFFT -> x: stage 1 then stage 2 per
+// ETRK2 substep (stage 1 alone for ETD1), two substeps per step() call.  The
+// loop body holds the two transforms of one half-substep, so the phase of the
+// program is one bit (the stage) and a step counter.
 template <int P, int T>
 INC_DEV void st_put(float2* st, const float2 (&v)[P], int t) {
 #pragma unroll
@@ -674,95 +675,85 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
-    const int per_sub = rk2 ? 4 : 2;
-    const int pro = a.s ? 2 : 1;
-    const int total = pro + steps * 2 * per_sub;
-    float2 X[P], SS[P], v[P];
+    float2 X[P], SS[P];
     SlotCache<P, T> cc;
     cc.load(a, c);
 #pragma unroll
     for (int m = 0; m < P; ++m) SS[m] = make_float2(0.f, 0.f);
-    // Position of the next phase: f-th transform of substep `sub` of step()
-    // `step`; the checkpoint countdown runs alongside (no divisions in the loop).
-    int f = 0, sub = 0, step = 0, ck_left = 0, ck_idx = 0;
+    // prologue: SS = phi1 FFT(s)/N, X = FFT(u)/N
 #pragma unroll 1
-    for (int ph = 0; ph < total; ++ph) {
-        int kind, cur = 0;
-        bool step_end = false;
-        if (ph < pro) {
-            kind = (ph == 0 && a.s) ? PH_S : PH_U;
-        } else {
-            cur = step;
-            kind = (f & 1) ? PH_INV : (f == 0 ? PH_NL1 : PH_NL2);
-            if (f == 0 && sub == 0) {
-                if (ckpt_on && a.ckpts) {
-                    if (ck_left == 0) {
-                        store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)ck_idx * N);
-                        ++ck_idx;
-                        ck_left = a.ckpt_every;
-                    }
-                    --ck_left;
-                }
-                if (seg) st_put<P, T>(seg + step * N, x, t);
-            }
-            step_end = sub == 1 && f == per_sub - 1;
-            if (++f == per_sub) {
-                f = 0;
-                if (++sub == 2) { sub = 0; ++step; }
-            }
-        }
-        // operand of this transform
-        if (kind == PH_S) {
+    for (int k = a.s ? 0 : 1; k < 2; ++k) {
+        float2 v[P];
+        if (k == 0) {
             load_pair<P, T>(v, a.s, c, N);
-        } else if (kind == PH_U) {
+        } else {
 #pragma unroll
             for (int m = 0; m < P; ++m) v[m] = x[m];
-        } else if (kind != PH_INV) {
-#pragma unroll
-            for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
         }
         fft_fwd<P, T>(v, buf, tw, t);
-        if (kind == PH_INV) {
-#pragma unroll
-            for (int m = 0; m < P; ++m) x[m] = cswap(v[m]);
-            if (frames_on && step_end)
-                store_pair_strided<P, T>(a.frames, x, c, N, (int64_t)a.steps * N, (int64_t)cur * N);
-            continue;
-        }
         if (a.split) to_split<P, T>(v, t, buf.a);
-        if (kind == PH_S) {
 #pragma unroll
-            for (int m = 0; m < P; ++m) {
-                const Slot s = cc.get(a, c, m, false);
-                SS[m] = rmul(cscale(v[m], a.invN), s.p1, s.p1b);
+        for (int m = 0; m < P; ++m) {
+            const float2 z = cscale(v[m], a.invN);
+            if (k == 0) {
+                const Slot sl = cc.get(a, c, m, false);
+                SS[m] = rmul(z, sl.p1, sl.p1b);
+            } else {
+                X[m] = z;
             }
-            continue;
         }
-        if (kind == PH_U) {
+    }
+    const int per_step = rk2 ? 4 : 2;  // half-substeps per step() call
+    const int64_t frame_stride = (int64_t)a.steps * N;
+    int h = 0, step = 0, ck_left = 0, ck_idx = 0;
+    bool stage2 = false;
+#pragma unroll 1
+    for (int it = steps * per_step; it > 0; --it) {
+        if (h == 0) {
+            if (ckpt_on && a.ckpts) {
+                if (ck_left == 0) {
+                    store_pair_strided<P, T>(a.ckpts, x, c, N, (int64_t)nseg * N, (int64_t)ck_idx * N);
+                    ++ck_idx;
+                    ck_left = a.ckpt_every;
+                }
+                --ck_left;
+            }
+            if (seg) st_put<P, T>(seg + step * N, x, t);
+        }
+        float2 v[P];
 #pragma unroll
-            for (int m = 0; m < P; ++m) X[m] = cscale(v[m], a.invN);
-            continue;
-        }
-        if (kind == PH_NL1) {
+        for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
+        fft_fwd<P, T>(v, buf, tw, t);
+        if (a.split) to_split<P, T>(v, t, buf.a);
+        if (!stage2) {  // Zi = E X + phi1 (D V + S);  ETRK2 carries Y = Zi - phi2 D V
 #pragma unroll
             for (int m = 0; m < P; ++m) {
-                const Slot s = cc.get(a, c, m, rk2);
-                const float2 DV = dmul(v[m], s.d * a.invN);
-                const float2 Zi = cadd(cadd(rmul(X[m], s.E, s.Eb), cscale(DV, s.p1)), SS[m]);
-                X[m] = rk2 ? csub(Zi, cscale(DV, s.p2)) : Zi;  // ETRK2 carries Y = Zi - phi2 D V
+                const Slot sl = cc.get(a, c, m, rk2);
+                const float2 DV = dmul(v[m], sl.dn);
+                const float2 Zi = cadd(cadd(rmul(X[m], sl.E, sl.Eb), cscale(DV, sl.p1)), SS[m]);
+                X[m] = rk2 ? csub(Zi, cscale(DV, sl.p2)) : Zi;
                 v[m] = Zi;
             }
-        } else {  // PH_NL2: X' = Y + phi2 D V2
+        } else {  // X' = Y + phi2 D V2
 #pragma unroll
             for (int m = 0; m < P; ++m) {
-                const Slot s = cc.get(a, c, m, true);
-                X[m] = cadd(X[m], cscale(dmul(v[m], s.d * a.invN), s.p2));
+                const Slot sl = cc.get(a, c, m, true);
+                X[m] = cadd(X[m], cscale(dmul(v[m], sl.dn), sl.p2));
                 v[m] = X[m];
             }
         }
         if (a.split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
-        for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);  // the next transform is an inverse
+        for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);  // inverse transform by swapping
+        fft_fwd<P, T>(v, buf, tw, t);
+#pragma unroll
+        for (int m = 0; m < P; ++m) x[m] = cswap(v[m]);
+        if (rk2) stage2 = !stage2;
+        if (++h == per_step) {
+            if (frames_on) store_pair_strided<P, T>(a.frames, x, c, N, frame_stride, (int64_t)step * N);
+            h = 0;
+            ++step;
+        }
     }
 }
 
@@ -948,7 +939,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
 #pragma unroll
         for (int m = 0; m < P; ++m) {
             const Slot sl = cc.get(a, c, m, rk2);
-            const float2 DV = dmul(v[m], sl.d * a.invN);
+            const float2 DV = dmul(v[m], sl.dn);
             if (kind == B_NL2) {
                 X[m] = cadd(X[m], cscale(DV, sl.p2));
                 v[m] = X[m];
