@@ -801,21 +801,6 @@ __global__ void __launch_bounds__(128) k_rollout(Args a) {
 //   w1 = IFFT(d phi1 Gi); Sacc += phi1 Gi
 //   G  = E Gi + FFT(2 x (w2 - w1))/N      (ETD1: w2 = 0, Gi = G)
 // with x, xi the substep's start and intermediate states, replayed first.
-enum BPhase { B_GF, B_U, B_NL1, B_INV_XI1, B_NL2, B_INV_X1, B_NL1B, B_INV_XI2, B_W2, B_GI, B_W1, B_GP };
-
-INC_DEV int recompute_kind(bool rk2, int q) {
-    if (!rk2) return q == 0 ? B_U : (q == 1 ? B_NL1 : B_INV_X1);
-    switch (q) {
-        case 0: return B_U;
-        case 1: return B_NL1;
-        case 2: return B_INV_XI1;
-        case 3: return B_NL2;
-        case 4: return B_INV_X1;
-        case 5: return B_NL1B;
-        default: return B_INV_XI2;
-    }
-}
-
 template <int P, int T>
 INC_DEV void pair_mul2(float2 (&v)[P], const float2 (&x)[P], float s) {
 #pragma unroll
@@ -826,6 +811,13 @@ INC_DEV void pair_mul2(float2 (&v)[P], const float2 (&x)[P], float s) {
 // x0s.  G: scaled adjoint spectrum w.r.t. the step output (in) and input
 // (out); Sacc accumulates phi1-weighted adjoints (IFFT(Sacc) = dL/ds).  If
 // gframe != nullptr the adjoint of this step's output frame is added first.
+//
+// After the prologue transforms (frame adjoint, FFT(x0)) the program is a
+// loop of two-transform units: replay units (FFT(x^2) -> stage -> IFFT,
+// storing xi1, x1, xi2; ETD1 stores x1 only), then per substep, second first,
+// the adjoint units  w2 = IFFT(d phi2 G) -> G -= FFT(2 xi w2)/N  and
+// Sacc += phi1 G, w1 = IFFT(d phi1 G) -> G = E G + FFT(2 x (w2 - w1))/N
+// (ETD1: the second unit alone with w2 = 0).
 template <int P, int T>
 INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>& cc, const float2 (&SS)[P],
                               float2 (&G)[P], float2 (&Sacc)[P], const float* gframe, int64_t gf_row_stride,
@@ -833,61 +825,84 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
-    const int lead = gframe ? 1 : 0;
-    const int nrec = rk2 ? 7 : 3;
-    const int per = rk2 ? 4 : 2;
-    const int total = lead + nrec + 2 * per;
     float2* x1s = st;
     float2* xi1s = st + N;
     float2* xi2s = st + 2 * N;
     float2* w2s = st + 3 * N;
-    float2 X[P], v[P], u[P];
-    int f = 0, sub = 1;  // adjoint phases: f-th transform of substep `sub` (second substep first)
+    float2 X[P];
 #pragma unroll 1
-    for (int ph = 0; ph < total; ++ph) {
-        const int q = ph - lead;
-        int kind, cur = sub;
-        if (q < 0) {
-            kind = B_GF;
-        } else if (q < nrec) {
-            kind = recompute_kind(rk2, q);
-        } else {
-            kind = rk2 ? (f == 0 ? B_W2 : (f == 1 ? B_GI : (f == 2 ? B_W1 : B_GP))) : (f == 0 ? B_W1 : B_GP);
-            if (++f == per) { f = 0; --sub; }
+    for (int k = gframe ? 0 : 1; k < 2; ++k) {
+        float2 v[P];
+        if (k == 0) load_pair_strided<P, T>(v, gframe, c, N, gf_row_stride, gf_off);
+        else st_get<P, T>(v, x0s, t);
+        fft_fwd<P, T>(v, buf, tw, t);
+        if (a.split) to_split<P, T>(v, t, buf.a);
+#pragma unroll
+        for (int m = 0; m < P; ++m) {
+            const float2 z = cscale(v[m], a.invN);
+            if (k == 0) G[m] = cadd(G[m], z);
+            else X[m] = z;
         }
-        // ---- operand of this transform
-        switch (kind) {
-            case B_GF: load_pair_strided<P, T>(v, gframe, c, N, gf_row_stride, gf_off); break;
-            case B_U: st_get<P, T>(v, x0s, t); break;
-            case B_NL1:
-                st_get<P, T>(v, x0s, t);
+    }
+    const int nrec = rk2 ? 3 : 1;
+    const int nunits = nrec + (rk2 ? 4 : 2);
+#pragma unroll 1
+    for (int k = 0; k < nunits; ++k) {
+        const bool rec = k < nrec;
+        const int j = k - nrec;                        // adjoint unit
+        const bool unit_w2 = rk2 && !rec && !(j & 1);  // w2 unit (ETRK2 only)
+        const bool sub1 = rk2 ? j < 2 : j < 1;         // second substep first
+        float2 v[P];
+        // ---- operand of the first transform
+        if (rec) {
+            st_get<P, T>(v, k == 0 ? x0s : (k == 1 ? xi1s : x1s), t);
 #pragma unroll
-                for (int m = 0; m < P; ++m) v[m] = sq2(v[m]);
-                break;
-            case B_NL2:
-            case B_NL1B:
-                st_get<P, T>(v, kind == B_NL2 ? xi1s : x1s, t);
+            for (int m = 0; m < P; ++m) v[m] = sq2(v[m]);
+        } else {
 #pragma unroll
-                for (int m = 0; m < P; ++m) v[m] = sq2(v[m]);
-                break;
-            case B_W2:
-            case B_W1:
+            for (int m = 0; m < P; ++m) {
+                const Slot sl = cc.get(a, c, m, unit_w2);
+                v[m] = cscale(dmul(G[m], sl.d), unit_w2 ? sl.p2 : sl.p1);
+                if (!unit_w2) Sacc[m] = cadd(Sacc[m], rmul(G[m], sl.p1, sl.p1b));
+            }
+            if (a.split) to_packed<P, T>(v, t, buf.a);
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
+        }
+        fft_fwd<P, T>(v, buf, tw, t);
+        // ---- operand of the second transform
+        if (rec) {
+            if (a.split) to_split<P, T>(v, t, buf.a);
+            if (rk2 && k == 1) {  // stage 2
 #pragma unroll
                 for (int m = 0; m < P; ++m) {
-                    const Slot sl = cc.get(a, c, m, kind == B_W2);
-                    v[m] = cscale(dmul(G[m], sl.d), kind == B_W2 ? sl.p2 : sl.p1);
-                    if (kind == B_W1) Sacc[m] = cadd(Sacc[m], rmul(G[m], sl.p1, sl.p1b));
+                    const Slot sl = cc.get(a, c, m, true);
+                    X[m] = cadd(X[m], cscale(dmul(v[m], sl.dn), sl.p2));
+                    v[m] = X[m];
                 }
-                if (a.split) to_packed<P, T>(v, t, buf.a);
+            } else {  // stage 1
 #pragma unroll
-                for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
-                break;
-            case B_GI:  // v holds w2
-                st_get<P, T>(u, cur ? xi2s : xi1s, t);
+                for (int m = 0; m < P; ++m) {
+                    const Slot sl = cc.get(a, c, m, rk2);
+                    const float2 DV = dmul(v[m], sl.dn);
+                    const float2 Zi = cadd(cadd(rmul(X[m], sl.E, sl.Eb), cscale(DV, sl.p1)), SS[m]);
+                    X[m] = rk2 ? csub(Zi, cscale(DV, sl.p2)) : Zi;
+                    v[m] = Zi;
+                }
+            }
+            if (a.split) to_packed<P, T>(v, t, buf.a);
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
+        } else {
+            float2 u[P];
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);  // w2 or w1
+            if (unit_w2) {
+                st_put<P, T>(w2s, v, t);
+                st_get<P, T>(u, sub1 ? xi2s : xi1s, t);
                 pair_mul2<P, T>(v, u, 2.f);
-                break;
-            case B_GP:  // v holds w1
-                st_get<P, T>(u, cur ? x1s : x0s, t);
+            } else {
+                st_get<P, T>(u, sub1 ? x1s : x0s, t);
                 if (rk2) {
                     float2 w2[P];
                     st_get<P, T>(w2, w2s, t);
@@ -897,61 +912,27 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
                 } else {
                     pair_mul2<P, T>(v, u, -2.f);
                 }
-                break;
-            default: break;  // inverse transforms: v was prepared by the previous phase
+            }
         }
         fft_fwd<P, T>(v, buf, tw, t);
         // ---- result
-        const bool inverse = kind == B_INV_XI1 || kind == B_INV_X1 || kind == B_INV_XI2 || kind == B_W2 || kind == B_W1;
-        if (inverse) {
+        if (rec) {
 #pragma unroll
             for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
-            if (kind == B_INV_XI1) st_put<P, T>(xi1s, v, t);
-            else if (kind == B_INV_X1) st_put<P, T>(x1s, v, t);
-            else if (kind == B_INV_XI2) st_put<P, T>(xi2s, v, t);
-            else if (kind == B_W2) st_put<P, T>(w2s, v, t);
-            continue;  // B_W1 keeps w1 in v for B_GP
-        }
-        if (a.split) to_split<P, T>(v, t, buf.a);
-        switch (kind) {
-            case B_GF:
-#pragma unroll
-                for (int m = 0; m < P; ++m) G[m] = cadd(G[m], cscale(v[m], a.invN));
-                continue;
-            case B_U:
-#pragma unroll
-                for (int m = 0; m < P; ++m) X[m] = cscale(v[m], a.invN);
-                continue;
-            case B_GI:
+            st_put<P, T>(rk2 ? (k == 0 ? xi1s : (k == 1 ? x1s : xi2s)) : x1s, v, t);
+        } else {
+            if (a.split) to_split<P, T>(v, t, buf.a);
+            if (unit_w2) {
 #pragma unroll
                 for (int m = 0; m < P; ++m) G[m] = csub(G[m], cscale(v[m], a.invN));
-                continue;
-            case B_GP:
+            } else {
 #pragma unroll
                 for (int m = 0; m < P; ++m) {
                     const Slot sl = cc.get(a, c, m, false);
                     G[m] = cadd(rmul(G[m], sl.E, sl.Eb), cscale(v[m], a.invN));
                 }
-                continue;
-            default: break;
-        }
-        // replay stages: next operand is an inverse transform
-#pragma unroll
-        for (int m = 0; m < P; ++m) {
-            const Slot sl = cc.get(a, c, m, rk2);
-            const float2 DV = dmul(v[m], sl.dn);
-            if (kind == B_NL2) {
-                X[m] = cadd(X[m], cscale(DV, sl.p2));
-                v[m] = X[m];
-            } else {
-                const float2 Zi = cadd(cadd(rmul(X[m], sl.E, sl.Eb), cscale(DV, sl.p1)), SS[m]);
-                if (kind == B_NL1) X[m] = rk2 ? csub(Zi, cscale(DV, sl.p2)) : Zi;
-                v[m] = Zi;
             }
         }
-        if (a.split) to_packed<P, T>(v, t, buf.a);
-#pragma unroll
-        for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
     }
 }
 
