@@ -90,35 +90,73 @@ INC_DEV float sin32(int m) {
     }
 }
 
-// b * exp(-+ 2 pi i m / 32) (forward: minus, inverse: plus).
+// a + w b and a - w b in six FMAs (the difference as 2a - (a + w b)).
+INC_DEV void bfly_w(float2 a, float2 b, float2 w, float2& s, float2& d) {
+    s.x = fmaf(w.x, b.x, fmaf(-w.y, b.y, a.x));
+    s.y = fmaf(w.x, b.y, fmaf(w.y, b.x, a.y));
+    d.x = fmaf(2.f, a.x, -s.x);
+    d.y = fmaf(2.f, a.y, -s.y);
+}
+
+// a +- b * exp(-+ 2 pi i m / 32) (forward: minus, inverse: plus).  m = 0 and
+// m = 8 need no multiply; m = 4, 12 scale a sum of +-b.x, +-b.y by cos(pi/4).
 template <bool INV>
-INC_DEV float2 rot32(float2 b, int m) {
-    if (m == 0) return b;
-    if (m == 8) return INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
-    const float c = cos32(m), s = INV ? sin32(m) : -sin32(m);
-    return make_float2(fmaf(b.x, c, -b.y * s), fmaf(b.x, s, b.y * c));
+INC_DEV void bfly_rot32(float2 a, float2 b, int m, float2& s, float2& d) {
+    if (m == 0) {
+        s = cadd(a, b);
+        d = csub(a, b);
+        return;
+    }
+    if (m == 8) {
+        const float2 r = INV ? make_float2(-b.y, b.x) : make_float2(b.y, -b.x);
+        s = cadd(a, r);
+        d = csub(a, r);
+        return;
+    }
+    const float c = cos32(m), sn = INV ? sin32(m) : -sin32(m);
+    if (m == 4 || m == 12) {
+        const float k = cos32(4);
+        const float cs = c > 0.f ? 1.f : -1.f, ss = sn > 0.f ? 1.f : -1.f;
+        const float tr = cs * b.x - ss * b.y, ti = ss * b.x + cs * b.y;
+        s = make_float2(fmaf(k, tr, a.x), fmaf(k, ti, a.y));
+        d = make_float2(fmaf(-k, tr, a.x), fmaf(-k, ti, a.y));
+        return;
+    }
+    bfly_w(a, b, make_float2(c, sn), s, d);
 }
 
 // In-register DFT of P <= 32 points, natural order in and out: radix-2
 // Stockham autosort (every index is arithmetic on unrolled loop counters, so
-// the whole transform stays in registers).
-template <int P, bool INV>
+// the whole transform stays in registers), from the stage of span NS0 on.
+template <int P, bool INV, int NS0 = 1>
 INC_DEV void dft_reg(float2 (&v)[P]) {
 #pragma unroll
-    for (int ns = 1; ns < P; ns *= 2) {
+    for (int ns = NS0; ns < P; ns *= 2) {
         float2 w[P];
 #pragma unroll
         for (int j = 0; j < P / 2; ++j) {
             const int k = j % ns;
-            const float2 a = v[j];
-            const float2 b = rot32<INV>(v[j + P / 2], k * (16 / ns));
             const int idx = (j / ns) * ns * 2 + k;
-            w[idx] = cadd(a, b);
-            w[idx + ns] = csub(a, b);
+            bfly_rot32<INV>(v[j], v[j + P / 2], k * (16 / ns), w[idx], w[idx + ns]);
         }
 #pragma unroll
         for (int i = 0; i < P; ++i) v[i] = w[i];
     }
+}
+
+// R-point forward DFT of tw[r] * y[r] (tw[0] = 1, not read): the twiddles of
+// the first stage's second operands are applied inside its butterflies.
+template <int R>
+INC_DEV void dft_tw(float2 (&y)[R], const float2 (&tw)[R]) {
+    float2 w[R];
+#pragma unroll
+    for (int j = 0; j < R / 2; ++j) {
+        const float2 a = j == 0 ? y[0] : cmul(y[j], tw[j]);
+        bfly_w(a, y[j + R / 2], tw[j + R / 2], w[2 * j], w[2 * j + 1]);
+    }
+#pragma unroll
+    for (int i = 0; i < R; ++i) y[i] = w[i];
+    dft_reg<R, false, 2>(y);
 }
 
 // ---- FFT -------------------------------------------------------------------------
@@ -315,18 +353,25 @@ INC_DEV void fft_later(float2 (&v)[P], const Buf<P, T>& buf, const Twiddles<P, T
         group_sync<T>();
         static_for<Q>([&](auto qc) {
             constexpr int q = decltype(qc)::value;
-            float2 w[R];
+            float2 w[R], twv[R];
             static_for<R>([&](auto rc) {
                 constexpr int r = decltype(rc)::value;
                 constexpr int off = lay(P, T, E, T * q + r * (N / R));
-                float2 y = buf.r[E][off];
+                w[r] = buf.r[E][off];
                 if constexpr (r > 0) {
-                    if constexpr (twiddles_in_registers<P, T>()) y = cmul(y, tw.reg[TOFF + q * (R - 1) + r - 1]);
-                    else y = cmul(y, twp[(q * R + r) * T + t]);
+                    if constexpr (twiddles_in_registers<P, T>()) twv[r] = tw.reg[TOFF + q * (R - 1) + r - 1];
+                    else twv[r] = twp[(q * R + r) * T + t];
+                } else {
+                    twv[r] = make_float2(1.f, 0.f);
                 }
-                w[r] = y;
             });
-            dft_reg<R, false>(w);
+            if constexpr (P >= 8) {
+                dft_tw<R>(w, twv);
+            } else {  // four values per lane: separate twiddle products keep the chains short
+#pragma unroll
+                for (int r = 1; r < R; ++r) w[r] = cmul(w[r], twv[r]);
+                dft_reg<R, false>(w);
+            }
             if constexpr (LAST) {
 #pragma unroll
                 for (int r = 0; r < R; ++r) v[q + Q * r] = w[r];
@@ -523,7 +568,7 @@ struct SlotCache {
         if constexpr (ON) {
 #pragma unroll
             for (int m = 0; m < P; ++m) {
-                const Slot s = slot<P, T>(a, c, m, true);
+                const Slot s = slot<P, T>(a, c, m, a.scheme == INC_KS_ETRK2);  // phi2 = 0 for ETD1
                 E[m] = s.E; p1[m] = s.p1; p2[m] = s.p2; d[m] = s.d; dn[m] = s.dn;
                 if (m == 0 || m == P / 2) {
                     const int i = m == 0 ? 0 : 1;
@@ -731,7 +776,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
                 const Slot sl = cc.get(a, c, m, rk2);
                 const float2 DV = dmul(v[m], sl.dn);
                 const float2 Zi = cadd(cadd(rmul(X[m], sl.E, sl.Eb), cscale(DV, sl.p1)), SS[m]);
-                X[m] = rk2 ? csub(Zi, cscale(DV, sl.p2)) : Zi;
+                X[m] = csub(Zi, cscale(DV, sl.p2));  // phi2 = 0 for ETD1
                 v[m] = Zi;
             }
         } else {  // X' = Y + phi2 D V2
@@ -886,7 +931,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
                     const Slot sl = cc.get(a, c, m, rk2);
                     const float2 DV = dmul(v[m], sl.dn);
                     const float2 Zi = cadd(cadd(rmul(X[m], sl.E, sl.Eb), cscale(DV, sl.p1)), SS[m]);
-                    X[m] = rk2 ? csub(Zi, cscale(DV, sl.p2)) : Zi;
+                    X[m] = csub(Zi, cscale(DV, sl.p2));  // phi2 = 0 for ETD1
                     v[m] = Zi;
                 }
             }
