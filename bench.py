@@ -54,7 +54,8 @@ def parse_args():
                     choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd"],
                     help="a small case of one kernel for ncu (no JSON)")
     ap.add_argument("--profile-rows", type=int, default=1024, help="rows of the KS profile case")
-    ap.add_argument("--tpp", type=int, default=32, help="threads per row pair of the KS profile case")
+    ap.add_argument("--tpp", type=int, default=None,
+                    help="KS threads per row pair (default: autotuned; the profile case uses 32)")
     return ap.parse_args()
 
 
@@ -230,8 +231,12 @@ def bench_ks(args, dev, world):
     cfg = ks_plain_config()
     B, N, steps, L, dt = cfg["B"], cfg["N"], cfg["steps"], cfg["L"], cfg["dt"]
     cells = B * N * steps
-    tpp, tune_ms = autotune.tune_ks(N, B, cfg["scheme"], device=dev, L=L, dt=dt)  # outside the timed regions
-    cfg["layout"] = {"threads_per_pair": tpp, "autotune_ms_per_50_steps": tune_ms}
+    if args.tpp:  # pinned layout (e.g. for a profiler run, whose timings would mislead the autotuner)
+        tpp = args.tpp
+        cfg["layout"] = {"threads_per_pair": tpp, "autotune": "skipped (--tpp)"}
+    else:
+        tpp, tune_ms = autotune.tune_ks(N, B, cfg["scheme"], device=dev, L=L, dt=dt)  # outside the timed regions
+        cfg["layout"] = {"threads_per_pair": tpp, "autotune_ms_per_50_steps": tune_ms}
     ds = torch.full((B,), L, device=dev)
     solver = KSSolverTorch(SimpleNamespace(resolution=N, dt=dt, device=dev, domain_size=ds,
                                            alpha=torch.zeros(B, device=dev), time_scheme=cfg["scheme"],
@@ -655,7 +660,7 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300),
                                              device_id=dev)
     if args.profile:
-        profile_small(dev, args.profile, args.profile_rows, args.tpp)
+        profile_small(dev, args.profile, args.profile_rows, args.tpp or 32)
         return
     if args.workload in ("burgers_diff", "ks_diff"):
         cfg, cells, times, extra = bench_diff(args, dev, world, args.workload)
