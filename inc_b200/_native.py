@@ -74,8 +74,11 @@ SIGNATURES = {
     "inc_energy_spectrum": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, _vp]),
     "inc_burgers_rollout_grad_noalloc": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, C.c_int32,
                                                    C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "inc_burgers_cnn_rollout": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, C.c_int32, _vp, _vp,
+                                          _vp, _vp]),
 }
 INC_NOALLOC_CKPT_FLOATS = 2 * 1024 * 1024
+INC_CNN_WEIGHT_FLOATS = 10657
 
 _lib = None
 _lock = threading.Lock()

@@ -109,6 +109,10 @@ def simulate_rollout(model, solver, u_initial, mstep, correction_term, L=None, c
             return burgers_rollout(solver, u_initial, mstep), None
     elif correction_term != "INC":
         raise ValueError(f"Invalid correction term: {correction_term}")
+    elif not torch.is_grad_enabled():
+        from . import fused
+        if fused.cnn_supported(model, solver, u_initial):  # evaluation: corrector inside the solver kernel
+            return fused.burgers_cnn_rollout(model, solver, u_initial, mstep)
 
     model_fn = (lambda u: model(u)) if L is None else (lambda u: model(u, L))
     step_fn = (lambda u: solver.step(u)) if L is None else (lambda u: solver.step(u, L))

@@ -122,6 +122,13 @@ class _BurgersLaunch:
                                                nat.ptr(ckpts), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_rollout")
 
+    def cnn_rollout(self, weights, u0, steps, frames, corrections, u_final):
+        with torch.cuda.device(self.dev):
+            rc = nat.lib().inc_burgers_cnn_rollout(C.byref(self.desc), weights.data_ptr(), u0.data_ptr(),
+                                                   nat.ptr(self.t_rows), self.t0, steps, nat.ptr(frames),
+                                                   nat.ptr(corrections), nat.ptr(u_final), nat.stream_of(self.dev))
+        nat.check(rc, "inc_burgers_cnn_rollout")
+
     def rollout_bwd(self, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s):
         with torch.cuda.device(self.dev):
             rc = nat.lib().inc_burgers_rollout_bwd(C.byref(self.desc), ckpts.data_ptr(), nat.ptr(s),

@@ -183,6 +183,24 @@ int inc_burgers_rollout_grad_noalloc(const inc_burgers_desc* d, const float* u0,
                                      float* frames, float* u_final, float* g_u0,
                                      float* g_s, void* stream);
 
+/* Hybrid rollout with the corrector evaluated inside the kernel: per step
+ * s = CNN(u), then u = step(u, s) -- simulate_rollout with correction "INC"
+ * (trainer/trainer_1d.py:154-183) and the benchmark's periodic CNN corrector
+ * (PeriodicCNN1D: Conv1d 1 -> 32 -> 32 -> 32 -> 1, kernel 5, circular padding,
+ * erf GELU between layers), forward only.  It replaces the per-step pair
+ * `s = model(u); u = solver.step(u)` of the reference loop, for evaluation
+ * rollouts.  weights: device, INC_CNN_WEIGHT_FLOATS floats, 16-byte aligned,
+ * packed as w1[co][k], b1[co], w2[ci][co][k], b2[co], w3[ci][co][k], b3[co],
+ * w4[ci][k], b4 (torch's Conv1d weight is [co][ci][k]; the hidden layers are
+ * stored input-channel major).  frames, corrections ([rows][steps][n]) and
+ * u_final may be NULL.  n: 64, 128, 256 or 512 (else INC_E_UNSUPPORTED);
+ * desc->cells_per_thread is ignored.                                        */
+#define INC_CNN_WEIGHT_FLOATS 10657
+int inc_burgers_cnn_rollout(const inc_burgers_desc* d, const float* weights,
+                            const float* u0, const float* t_rows, double t0,
+                            int32_t steps, float* frames, float* corrections,
+                            float* u_final, void* stream);
+
 /* ---- Kuramoto-Sivashinsky --------------------------------------------- */
 /* Bytes of device memory a plan needs.                                       */
 int64_t inc_ks_plan_size(int32_t rows, int32_t n);

@@ -1,0 +1,185 @@
+"""Burgers rollout with the periodic CNN corrector inside the kernel (GPU).
+
+The fused kernel (inc_burgers_cnn_rollout) must reproduce the per-step loop
+of simulate_rollout (trainer_1d.py:154-183): s = model(u); u = step(u, s).
+Checked against (a) that loop in FP64 on the CPU (torch's Conv1d in float64
+plus the oracle's Burgers step) and (b) the same loop on the GPU in FP32
+(cuDNN convolutions with TF32 off plus the CUDA solver), over all supported
+widths, both time schemes, both convection schemes and the reference's
+source terms, with batches that leave the last CTA partly empty."""
+import math
+from types import SimpleNamespace
+
+import numpy as np
+import pytest
+import torch
+
+from oracle import burgers as ob
+from tests.golden_io import burgers_case, load, rel_l2
+
+pytestmark = pytest.mark.gpu
+BZ = load("burgers_golden.npz")
+TOL = 1e-5  # relative L2 of FP32 vs FP64 frames / corrections
+
+
+@pytest.fixture(autouse=True)
+def fp32_convs():
+    saved = (torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32)
+    torch.backends.cudnn.allow_tf32 = False
+    torch.backends.cuda.matmul.allow_tf32 = False
+    yield
+    torch.backends.cudnn.allow_tf32, torch.backends.cuda.matmul.allow_tf32 = saved
+
+
+def _params(N, eq="viscosity", conv="WENO", B=1, seed=0):
+    rng = np.random.default_rng(seed)
+    L = 2 * math.pi
+    kw = dict(resolution=N, L=L, dt=0.25 * L / N / 1.5, nu=0.01, convection_term=conv, equation_type=eq)
+    if eq == "linear":
+        kw["beta"] = 0.1
+    if eq == "learning":
+        J = 3
+        kw.update(A=rng.uniform(-0.5, 0.5, (B, 1, J)), omega=rng.uniform(-0.4, 0.4, (B, 1, J)),
+                  phi=rng.uniform(0, 2 * np.pi, (B, 1, J)), l=rng.integers(1, 4, (B, 1, J)).astype(np.float64),
+                  x=np.arange(N) * (L / N))
+    return ob.BurgersParams(**kw)
+
+
+def _sim_params(p, B, scheme, device):
+    f = lambda a: None if a is None else torch.as_tensor(a, dtype=torch.float32, device=device)  # noqa: E731
+    arr = lambda a: f(a) if isinstance(a, np.ndarray) else a  # noqa: E731
+    return SimpleNamespace(resolution=p.resolution, dt=p.dt, x=f(p.x) if p.x is not None else None,
+                           adaptive_CFL=None, L=p.L, nu=arr(p.nu), device=device, convection_term=p.convection_term,
+                           equation_type=p.equation_type, batch_size=B,
+                           beta=arr(p.beta), J=(p.A.shape[-1] if p.A is not None else 0), A=f(p.A),
+                           omega=f(p.omega), phi=f(p.phi), l=f(p.l), time_scheme=scheme)
+
+
+def _u0(B, N, seed):
+    rng = np.random.default_rng(seed)
+    x = np.arange(N) * (2 * np.pi / N)
+    a = rng.uniform(-0.5, 0.5, (B, 5))
+    ph = rng.uniform(0, 2 * np.pi, (B, 5))
+    k = np.arange(1, 6)
+    return (a[:, :, None] * np.sin(k[None, :, None] * x[None, None, :] + ph[:, :, None])).sum(1)
+
+
+def _net(seed=0):
+    from inc_b200.correctors import PeriodicCNN1D
+    torch.manual_seed(seed)
+    net = PeriodicCNN1D()
+    with torch.no_grad():  # larger corrections than the default init, so that s matters
+        for c in net.convs:
+            c.weight.mul_(3.0)
+    return net
+
+
+def _fp64_loop(net, p, u0, steps, scheme, t0=0.0):
+    """The per-step loop in float64 on the CPU: torch corrector + oracle step."""
+    net64 = net.double().cpu()
+    u, t = u0.astype(np.float64), t0
+    frames, corr = [], []
+    with torch.no_grad():
+        for _ in range(steps):
+            s = net64(torch.from_numpy(u)).numpy()
+            u, t = (ob.step_ssprk3 if scheme == "ssprk3" else ob.step_euler)(u, p, t, s)
+            frames.append(u)
+            corr.append(s)
+    return np.stack(frames, 1), np.stack(corr, 1)
+
+
+@pytest.mark.parametrize("N,B", [(64, 3), (128, 5), (256, 7), (512, 2)])
+@pytest.mark.parametrize("scheme", ["euler", "ssprk3"])
+def test_fused_cnn_rollout_vs_fp64_loop(cuda, N, B, scheme):
+    from inc_b200.fused import burgers_cnn_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    p = _params(N)
+    u0 = _u0(B, N, seed=N + B)
+    net = _net()
+    steps = 12
+    ref_f, ref_c = _fp64_loop(net, p, u0, steps, scheme)
+    solver = BurgersSolverTorch(_sim_params(p, B, scheme, cuda))
+    frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver, torch.tensor(u0, dtype=torch.float32,
+                                                                                  device=cuda), steps)
+    assert rel_l2(frames.cpu().numpy(), ref_f) < TOL
+    assert rel_l2(corr.cpu().numpy(), ref_c) < TOL
+    assert np.max(np.abs(corr.cpu().numpy())) > 1e-2  # the corrector is not negligible
+    assert abs(float(solver.t) - steps * p.dt) < 1e-9
+
+
+@pytest.mark.parametrize("eq,conv", [("viscosity", "FDM"), ("linear", "WENO"), ("learning", "WENO"),
+                                     ("homogeneous", "WENO")])
+def test_fused_cnn_rollout_sources_and_convection(cuda, eq, conv):
+    from inc_b200.fused import burgers_cnn_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    N, B, steps = 128, 9, 10
+    p = _params(N, eq=eq, conv=conv, B=B, seed=1)
+    u0 = _u0(B, N, seed=3)
+    net = _net(1)
+    ref_f, ref_c = _fp64_loop(net, p, u0, steps, "ssprk3", t0=0.3)
+    solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+    solver.t = 0.3
+    frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver,
+                                       torch.tensor(u0, dtype=torch.float32, device=cuda), steps)
+    assert rel_l2(frames.cpu().numpy(), ref_f) < TOL
+    assert rel_l2(corr.cpu().numpy(), ref_c) < TOL
+
+
+def test_fused_matches_per_step_gpu_loop_and_dispatch(cuda):
+    """simulate_rollout under no_grad takes the fused kernel; with grad on it runs the per-step loop."""
+    from inc_b200.rollout import simulate_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    N, B, steps = 256, 37, 16
+    p = _params(N)
+    u0 = torch.tensor(_u0(B, N, seed=5), dtype=torch.float32, device=cuda)
+    net = _net(2).float().to(cuda)
+    s1 = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+    with torch.no_grad():
+        f1, c1 = simulate_rollout(net, s1, u0, steps, "INC")
+    s2 = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+    f2, c2 = simulate_rollout(net, s2, u0, steps, "INC")  # grad enabled: per-step path
+    assert f2.requires_grad  # the per-step graph was built
+    assert rel_l2(f1.cpu().numpy(), f2.detach().cpu().numpy()) < TOL
+    assert rel_l2(c1.cpu().numpy(), c2.detach().cpu().numpy()) < TOL
+    assert abs(float(s1.t) - float(s2.t)) < 1e-9
+    assert torch.equal(s1.correction_s, c1[:, -1])
+
+
+def test_fused_golden_learning_case(cuda):
+    """A reference golden configuration (forcing source, per-row t) with a corrector in the loop."""
+    from inc_b200.fused import burgers_cnn_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    p, u0, t0, _, scheme = burgers_case(BZ, "rk3_learning_s")
+    B, N = u0.shape
+    net = _net(4)
+    steps = 8
+    t_start = np.asarray(t0, dtype=np.float64).reshape(B, 1) if np.ndim(t0) else float(t0)
+    ref_f, ref_c = _fp64_loop(net, p, u0, steps, "ssprk3", t0=t_start)
+    solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+    solver.t = torch.tensor(t_start, dtype=torch.float32, device=cuda) if np.ndim(t0) else float(t0)
+    frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver,
+                                       torch.tensor(u0, dtype=torch.float32, device=cuda), steps)
+    assert rel_l2(frames.cpu().numpy(), ref_f) < TOL
+    assert rel_l2(corr.cpu().numpy(), ref_c) < TOL
+
+
+def test_fused_rejects_unsupported(cuda):
+    from inc_b200.correctors import PeriodicCNN1D
+    from inc_b200.fused import burgers_cnn_rollout, cnn_supported
+    from inc_b200.rollout import simulate_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    p = _params(32)
+    solver = BurgersSolverTorch(_sim_params(p, 2, "euler", cuda))
+    u = torch.zeros(2, 32, device=cuda)
+    net = PeriodicCNN1D().to(cuda)
+    assert not cnn_supported(net, solver, u)
+    with pytest.raises(ValueError):
+        burgers_cnn_rollout(net, solver, u, 4)
+    small = PeriodicCNN1D(channels=16).to(cuda)
+    p = _params(64)
+    solver = BurgersSolverTorch(_sim_params(p, 2, "euler", cuda))
+    u = torch.tensor(_u0(2, 64, 1), dtype=torch.float32, device=cuda)
+    assert not cnn_supported(small, solver, u)
+    with torch.no_grad():
+        f, c = simulate_rollout(small, solver, u, 3, "INC")  # falls back to the per-step loop
+    assert f.shape == (2, 3, 64) and c.shape == (2, 3, 64)

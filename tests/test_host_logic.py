@@ -118,3 +118,38 @@ def test_solver_errors_without_gpu():
     s = BurgersSolverTorch(SimpleNamespace(convection_term="WENO", **base))
     with pytest.raises(ValueError, match="CUDA"):
         s.step(torch.zeros(2, 64))                                  # no CPU path
+
+
+def test_cnn_weight_packing_layout():
+    """pack_cnn_weights: w1[co][k], b1, w2[ci][co][k], b2, w3[ci][co][k], b3, w4[ci][k], b4 (CPU)."""
+    import torch
+    from inc_b200 import _native as nat
+    from inc_b200.correctors import PeriodicCNN1D
+    from inc_b200.fused import pack_cnn_weights
+    torch.manual_seed(0)
+    net = PeriodicCNN1D()
+    w = pack_cnn_weights(net)
+    assert w.numel() == nat.INC_CNN_WEIGHT_FLOATS == 10657
+    c = net.convs
+    C, K = 32, 5
+    o_b1 = C * K
+    o_w2 = o_b1 + C
+    o_b2 = o_w2 + C * C * K
+    o_w3 = o_b2 + C
+    o_b3 = o_w3 + C * C * K
+    o_w4 = o_b3 + C
+    o_b4 = o_w4 + C * K
+    assert torch.equal(w[:o_b1].view(C, K), c[0].weight[:, 0, :])
+    assert torch.equal(w[o_b1:o_w2], c[0].bias)
+    for ci, co, k in [(0, 0, 0), (3, 17, 4), (31, 5, 2), (12, 31, 1)]:
+        assert w[o_w2 + (ci * C + co) * K + k] == c[1].weight[co, ci, k]
+        assert w[o_w3 + (ci * C + co) * K + k] == c[2].weight[co, ci, k]
+    assert torch.equal(w[o_b2:o_w3], c[1].bias) and torch.equal(w[o_b3:o_w4], c[2].bias)
+    assert torch.equal(w[o_w4:o_b4].view(C, K), c[3].weight[0])
+    assert w[o_b4] == c[3].bias[0]
+    bad = PeriodicCNN1D(channels=16)
+    try:
+        pack_cnn_weights(bad)
+        raise AssertionError("expected ValueError")
+    except ValueError:
+        pass
