@@ -572,19 +572,32 @@ def bench_diff(args, dev, world, which):
         opt.zero_grad(set_to_none=False)
         return loss
 
-    def forward_only():
+    def forward_only():  # evaluation rollout; for the CNN corrector simulate_rollout runs the fused kernel
+        if which == "burgers_diff":
+            solver.t = 0.0
         with torch.no_grad():
             simulate_rollout(net, solver, u0, steps, "INC", L)
+
+    def forward_loop():  # the reference's loop: one corrector call and one step() launch per step
+        if which == "burgers_diff":
+            solver.t = 0.0
+        u = u0
+        with torch.no_grad():
+            for _ in range(steps):
+                solver.correction_s = net(u) if L is None else net(u, L)
+                u = solver.step(u) if L is None else solver.step(u, L)
 
     for _ in range(args.warmup):
         train_step(8)
         train_step(None)
         forward_only()
+        forward_loop()
     torch.cuda.synchronize()
     with ClockSampler(dev.index) as clk:
         t_ck = event_time(lambda: train_step(8), args.steps)
     t_plain = event_time(lambda: train_step(None), args.steps)
     t_fwd = event_time(forward_only, args.steps)
+    t_loop = event_time(forward_loop, args.steps)
     # the whole training step captured in one CUDA graph
     side = torch.cuda.Stream(dev)
     side.wait_stream(torch.cuda.current_stream(dev))
@@ -599,8 +612,17 @@ def bench_diff(args, dev, world, which):
     torch.cuda.synchronize()
     t_graph = event_time(graph.replay, args.steps)
     ms = lambda t: sum(t) / len(t)  # noqa: E731
-    times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck))
+    times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop))
     extra = dict(clocks=clk.summary(), h2d=0, d2h=4, launches=None)
+    if which == "burgers_diff":  # the fused corrector rollout against the FP32 FMA peak
+        from inc_b200.roofline import burgers_cnn_flops_per_cell_step
+        fpc = burgers_cnn_flops_per_cell_step(cfg["scheme"])
+        achieved = cells * fpc / (ms(t_fwd) * 1e-3) / 1e12
+        peak = fp32_peak_tflops(dev)
+        extra["fused_inference_roofline"] = {
+            "kernel": "inc_burgers_cnn_rollout (k_cnn_rollout<256>)", "bound": "fp32", "achieved": achieved,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "flops_per_cell_step": fpc,
+            "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run"}
     cfg = dict(name=which, B=B, N=N, steps=steps, scheme=cfg["scheme"],
                corrector=("PeriodicCNN1D(4x32ch,k5,GELU)" if which == "burgers_diff" else "FNO1D(4 layers,w64,16 modes)"))
     return cfg, cells, times, extra
@@ -683,7 +705,11 @@ def main():
                            "value_is": "whole training step (rollout, loss, backward, Adam) in one CUDA graph"},
                 "eager": {"train_step_ckpt8": tot / (times["ckpt"] * 1e-3),
                           "train_step_no_ckpt": tot / (times["plain"] * 1e-3),
-                          "forward_only": tot / (times["fwd"] * 1e-3)},
+                          "forward_only": tot / (times["fwd"] * 1e-3),
+                          "forward_per_step_loop": tot / (times["loop"] * 1e-3)},
+                "forward_only_is": ("fused corrector + solver kernel (inc_burgers_cnn_rollout)"
+                                    if cfg["name"] == "burgers_diff" else "corrector in torch, solver step launches"),
+                "fused_inference_roofline": extra.get("fused_inference_roofline"),
                 "clocks": extra["clocks"]}), flush=True)
         if world > 1:
             torch.distributed.barrier()

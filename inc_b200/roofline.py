@@ -40,3 +40,12 @@ def plain_bytes_per_cell_step(with_s: bool) -> int:
 
 
 FUSED_BYTES_PER_CELL_STEP = 4
+
+# Periodic CNN corrector (Conv1d 1 -> 32 -> 32 -> 32 -> 1, kernel 5) per cell:
+# 2 * (32*5 + 2 * 32*32*5 + 32*5) multiply-adds-as-two = 21,120 flops (bias and
+# GELU not counted), evaluated once per step before the solver step.
+CNN_FLOPS_PER_CELL = 2 * (32 * 5 + 2 * 32 * 32 * 5 + 32 * 5)
+
+
+def burgers_cnn_flops_per_cell_step(scheme: str = "ssprk3") -> int:
+    return CNN_FLOPS_PER_CELL + BURGERS_FLOPS[scheme]
