@@ -32,6 +32,15 @@ struct Weno {
     float d0, e0, d1, e1, d2, e2;
 };
 
+// 1/x by the hardware reciprocal (PTX rcp.approx.ftz.f32, at most 1 ulp off).
+// The WENO denominators are >= (1e-6)^2, far from the subnormal range the
+// ftz form flushes; 1/inf = 0 as for a division.
+INC_DEV float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
 template <bool RIGHT>
 INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& w) {
     w.q0 = fmaf(1.f / 3.f, g0, fmaf(-7.f / 6.f, g1, (11.f / 6.f) * g2));
@@ -48,10 +57,10 @@ INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& 
     const float b2 = fmaf(13.f / 12.f * w.d2, w.d2, 0.25f * w.e2 * w.e2);
     w.s0 = kEps + b0; w.s1 = kEps + b1; w.s2 = kEps + b2;
     // alpha_k = gamma_k / (eps + beta_k)^2, gamma = (0.1, 0.6, 0.3)  (:22, :39)
-    w.a0 = __fdividef(0.1f, w.s0 * w.s0);
-    w.a1 = __fdividef(0.6f, w.s1 * w.s1);
-    w.a2 = __fdividef(0.3f, w.s2 * w.s2);
-    w.inv_sum = __fdividef(1.f, w.a0 + w.a1 + w.a2);
+    w.a0 = 0.1f * rcp_approx(w.s0 * w.s0);
+    w.a1 = 0.6f * rcp_approx(w.s1 * w.s1);
+    w.a2 = 0.3f * rcp_approx(w.s2 * w.s2);
+    w.inv_sum = rcp_approx(w.a0 + w.a1 + w.a2);
     w.h = (w.a0 * w.q0 + w.a1 * w.q1 + w.a2 * w.q2) * w.inv_sum;
 }
 
@@ -71,9 +80,9 @@ INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float h
     weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
     const float w0 = w.a0 * w.inv_sum, w1 = w.a1 * w.inv_sum, w2 = w.a2 * w.inv_sum;
     const float qb0 = hb * w0, qb1 = hb * w1, qb2 = hb * w2;
-    const float bb0 = -2.f * qb0 * (w.q0 - w.h) * __fdividef(1.f, w.s0);
-    const float bb1 = -2.f * qb1 * (w.q1 - w.h) * __fdividef(1.f, w.s1);
-    const float bb2 = -2.f * qb2 * (w.q2 - w.h) * __fdividef(1.f, w.s2);
+    const float bb0 = -2.f * qb0 * (w.q0 - w.h) * rcp_approx(w.s0);
+    const float bb1 = -2.f * qb1 * (w.q1 - w.h) * rcp_approx(w.s1);
+    const float bb2 = -2.f * qb2 * (w.q2 - w.h) * rcp_approx(w.s2);
     // beta_k = 13/12 d^2 + 1/4 e^2  ->  dbeta = 13/6 d dd + 1/2 e de
     const float A0 = 13.f / 6.f * w.d0 * bb0, E0 = 0.5f * w.e0 * bb0;
     const float A1 = 13.f / 6.f * w.d1 * bb1, E1 = 0.5f * w.e1 * bb1;
