@@ -772,14 +772,14 @@ def main():
 
 def profile_small(dev, which="ks", rows=1024, tpp=32):
     """Small cases for ncu captures: the KS fused rollout (rows x 256, 64 steps, `tpp` threads
-    per row pair) and its backward, the ragged Burgers batch (1024 rows, 20 steps) or the
-    32x128 Burgers rollout."""
+    per row pair) and its backward, the ragged Burgers batch (rows of n in {64..512}, 20 steps)
+    or the 32x128 Burgers rollout."""
     import torch
     from types import SimpleNamespace
     if which == "burgers_ragged":
         from inc_b200.batched import RaggedBurgers
         from inc_b200.workloads import burgers_batched_config
-        cfg = burgers_batched_config(rows=1024, steps=20)
+        cfg = burgers_batched_config(rows=rows, steps=20)
         rb = RaggedBurgers(cfg["u0"], cfg["nu"], cfg["dt"], cfg["dx"], scheme="ssprk3", device=dev)
         for _ in range(2):
             rb.rollout(20)

@@ -27,10 +27,22 @@ constexpr float kEps = 1e-6f;  // solver_1d.py:5
 // The two share q0..q2, beta0 and beta1 on the window; they differ only in the
 // second term of beta2: (3g2 - 4g3 + g4) for left, (g2 - 4g3 + 3g4) for right.
 // ---------------------------------------------------------------------------
+// The evaluation uses scaled quantities that need fewer products; the scale
+// factors cancel in the normalised weights w_k = alpha_k / sum(alpha):
+//   beta'_k = (12/13) beta_k = d_k^2 + (3/13) e_k^2,
+//   s'_k    = (12/13) (eps + beta_k) = (12/13) eps + beta'_k,
+//   r_k     = 1 / s'_k^2  (= (13/12)^2 / (eps + beta_k)^2),
+//   h       = sum_k (gamma_k q_k) r_k / sum_k gamma_k r_k,
+// with gamma_k folded into the candidate polynomials' coefficients (qg_k).
 struct Weno {
-    float q0, q1, q2, s0, s1, s2, a0, a1, a2, inv_sum, h;
+    float qg0, qg1, qg2;  // gamma_k q_k
+    float s0, s1, s2;     // s'_k
+    float r0, r1, r2;     // 1 / s'_k^2
+    float inv_den, h;
     float d0, e0, d1, e1, d2, e2;
 };
+
+constexpr float kEpsScaled = kEps * (12.f / 13.f);
 
 // 1/x by the hardware reciprocal (PTX rcp.approx.ftz.f32, at most 1 ulp off).
 // The WENO denominators are >= (1e-6)^2, far from the subnormal range the
@@ -43,25 +55,24 @@ INC_DEV float rcp_approx(float x) {
 
 template <bool RIGHT>
 INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& w) {
-    w.q0 = fmaf(1.f / 3.f, g0, fmaf(-7.f / 6.f, g1, (11.f / 6.f) * g2));
-    w.q1 = fmaf(-1.f / 6.f, g1, fmaf(5.f / 6.f, g2, (1.f / 3.f) * g3));
-    w.q2 = fmaf(1.f / 3.f, g2, fmaf(5.f / 6.f, g3, (-1.f / 6.f) * g4));
+    // gamma = (0.1, 0.6, 0.3) times q0 = (1/3, -7/6, 11/6), q1 = (-1/6, 5/6, 1/3), q2 = (1/3, 5/6, -1/6)
+    w.qg0 = fmaf(0.0333333333f, g0, fmaf(-0.1166666667f, g1, 0.1833333333f * g2));
+    w.qg1 = fmaf(-0.1f, g1, fmaf(0.5f, g2, 0.2f * g3));
+    w.qg2 = fmaf(0.1f, g2, fmaf(0.25f, g3, -0.05f * g4));
     w.d0 = fmaf(-2.f, g1, g0) + g2;
     w.e0 = fmaf(-4.f, g1, g0) + 3.f * g2;
     w.d1 = fmaf(-2.f, g2, g1) + g3;
     w.e1 = g1 - g3;
     w.d2 = fmaf(-2.f, g3, g2) + g4;
     w.e2 = RIGHT ? (fmaf(-4.f, g3, g2) + 3.f * g4) : (fmaf(-4.f, g3, 3.f * g2) + g4);
-    const float b0 = fmaf(13.f / 12.f * w.d0, w.d0, 0.25f * w.e0 * w.e0);
-    const float b1 = fmaf(13.f / 12.f * w.d1, w.d1, 0.25f * w.e1 * w.e1);
-    const float b2 = fmaf(13.f / 12.f * w.d2, w.d2, 0.25f * w.e2 * w.e2);
-    w.s0 = kEps + b0; w.s1 = kEps + b1; w.s2 = kEps + b2;
-    // alpha_k = gamma_k / (eps + beta_k)^2, gamma = (0.1, 0.6, 0.3)  (:22, :39)
-    w.a0 = 0.1f * rcp_approx(w.s0 * w.s0);
-    w.a1 = 0.6f * rcp_approx(w.s1 * w.s1);
-    w.a2 = 0.3f * rcp_approx(w.s2 * w.s2);
-    w.inv_sum = rcp_approx(w.a0 + w.a1 + w.a2);
-    w.h = (w.a0 * w.q0 + w.a1 * w.q1 + w.a2 * w.q2) * w.inv_sum;
+    w.s0 = kEpsScaled + fmaf(w.d0, w.d0, (3.f / 13.f) * w.e0 * w.e0);
+    w.s1 = kEpsScaled + fmaf(w.d1, w.d1, (3.f / 13.f) * w.e1 * w.e1);
+    w.s2 = kEpsScaled + fmaf(w.d2, w.d2, (3.f / 13.f) * w.e2 * w.e2);
+    w.r0 = rcp_approx(w.s0 * w.s0);
+    w.r1 = rcp_approx(w.s1 * w.s1);
+    w.r2 = rcp_approx(w.s2 * w.s2);
+    w.inv_den = rcp_approx(fmaf(0.1f, w.r0, fmaf(0.6f, w.r1, 0.3f * w.r2)));
+    w.h = fmaf(w.qg0, w.r0, fmaf(w.qg1, w.r1, w.qg2 * w.r2)) * w.inv_den;
 }
 
 template <bool RIGHT>
@@ -72,17 +83,19 @@ INC_DEV float weno5(float g0, float g1, float g2, float g3, float g4) {
 }
 
 // Adds hb * d h / d g_m to acc[0..4] (the vector-Jacobian product of weno5).
-// With w_k = a_k / S:  dh/dq_k = w_k,  dh/dbeta_k = -2 w_k (q_k - h) / s_k.
+// With w_k = alpha_k / S:  dh/dq_k = w_k,  dh/dbeta_k = -2 w_k (q_k - h) / (eps + beta_k).
 template <bool RIGHT>
 INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float hb,
                        float& c0, float& c1, float& c2, float& c3, float& c4) {
     Weno w;
     weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
-    const float w0 = w.a0 * w.inv_sum, w1 = w.a1 * w.inv_sum, w2 = w.a2 * w.inv_sum;
+    const float w0 = 0.1f * w.r0 * w.inv_den, w1 = 0.6f * w.r1 * w.inv_den, w2 = 0.3f * w.r2 * w.inv_den;
+    const float q0 = 10.f * w.qg0, q1 = w.qg1 * (1.f / 0.6f), q2 = w.qg2 * (1.f / 0.3f);
     const float qb0 = hb * w0, qb1 = hb * w1, qb2 = hb * w2;
-    const float bb0 = -2.f * qb0 * (w.q0 - w.h) * rcp_approx(w.s0);
-    const float bb1 = -2.f * qb1 * (w.q1 - w.h) * rcp_approx(w.s1);
-    const float bb2 = -2.f * qb2 * (w.q2 - w.h) * rcp_approx(w.s2);
+    // 1 / (eps + beta_k) = (12/13) / s'_k
+    const float bb0 = (-24.f / 13.f) * qb0 * (q0 - w.h) * rcp_approx(w.s0);
+    const float bb1 = (-24.f / 13.f) * qb1 * (q1 - w.h) * rcp_approx(w.s1);
+    const float bb2 = (-24.f / 13.f) * qb2 * (q2 - w.h) * rcp_approx(w.s2);
     // beta_k = 13/12 d^2 + 1/4 e^2  ->  dbeta = 13/6 d dd + 1/2 e de
     const float A0 = 13.f / 6.f * w.d0 * bb0, E0 = 0.5f * w.e0 * bb0;
     const float A1 = 13.f / 6.f * w.d1 * bb1, E1 = 0.5f * w.e1 * bb1;
@@ -99,6 +112,13 @@ INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float h
     c2 += (1.f / 3.f) * qb2 + A2 + (RIGHT ? 1.f : 3.f) * E2;
     c3 += (5.f / 6.f) * qb2 - 2.f * A2 - 4.f * E2;
     c4 += (-1.f / 6.f) * qb2 + A2 + (RIGHT ? 3.f : 1.f) * E2;
+}
+
+// Lax-Friedrichs flux splitting of f = u^2 / 2 (solver_1d.py:134-137):
+// f+- = (f +- alpha u) / 2 = u (u / 4 +- alpha / 2);  ha = alpha / 2.
+INC_DEV void flux_split(float u, float ha, float& fp, float& fm) {
+    fp = u * fmaf(0.25f, u, ha);
+    fm = u * fmaf(0.25f, u, -ha);
 }
 
 // ---------------------------------------------------------------------------
@@ -165,6 +185,37 @@ INC_DEV void halo_window(const float (&u)[CPT], float (&w)[CPT + 6], int left, i
     w[CPT + 5] = shfl<TPR>(u[2], right);
 }
 
+// r[c] for the CPT cells of a window w (3 halo cells each side):
+// -(Dminus f+ + Dminus f-)/dx + nu D2 u, with f+- reconstructed at i+1/2
+// (solver_1d.py:129-146; the dense D2 matmul is the 3-point stencil).
+template <int CPT>
+INC_DEV void weno_rhs(const float (&w)[CPT + 6], float alpha, float nu_dx2, float inv_dx, float (&r)[CPT]) {
+    const float ha = 0.5f * alpha;
+    float fp[CPT + 6], fm[CPT + 6];
+#pragma unroll
+    for (int k = 0; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
+    // hs = h+ + h- at i+1/2; the difference of the two sums is the flux difference
+    float hs_prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]) + weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        const float hs = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
+                         weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+        const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
+        r[c] = fmaf(inv_dx, hs_prev - hs, nu_dx2 * lap);
+        hs_prev = hs;
+    }
+}
+
+// central-difference convection (calc_nonlinear_FDM, solver_1d.py:125-127) + diffusion
+template <int CPT>
+INC_DEV void fdm_rhs(const float (&w)[CPT + 6], float nu_dx2, float inv_2dx, float (&r)[CPT]) {
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) {
+        const float nl = -w[c + 3] * ((w[c + 4] - w[c + 2]) * inv_2dx);
+        r[c] = fmaf(nu_dx2, fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]), nl);
+    }
+}
+
 // r = nonlinear + linear (no source): calc_nonlinear_weno / _FDM + calc_linear.
 template <int CPT, int TPR>
 INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu,
@@ -176,30 +227,9 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
 #pragma unroll
         for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
         const float alpha = group_max<TPR>(m);  // per-row max |u|, solver_1d.py:133
-        float fp[CPT + 6], fm[CPT + 6];
-#pragma unroll
-        for (int k = 0; k < CPT + 6; ++k) {
-            const float fl = 0.5f * w[k] * w[k];  // flux = 0.5 u^2
-            fp[k] = 0.5f * (fl + alpha * w[k]);
-            fm[k] = 0.5f * (fl - alpha * w[k]);
-        }
-        float hp_prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]);
-        float hm_prev = weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-            const float hp = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]);
-            const float hm = weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
-            const float nl = -((hp - hp_prev) * inv_dx + (hm - hm_prev) * inv_dx);
-            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
-            hp_prev = hp;
-            hm_prev = hm;
-        }
+        weno_rhs<CPT>(w, alpha, nu * inv_dx2, inv_dx, r);
     } else {
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-            const float nl = -w[c + 3] * ((w[c + 4] - w[c + 2]) * inv_2dx);
-            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
-        }
+        fdm_rhs<CPT>(w, nu * inv_dx2, inv_2dx, r);
     }
 }
 
@@ -280,11 +310,7 @@ INC_DEV void rhs_vjp(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], c
         const float alpha = m;
         float fp[CPT + 6], fm[CPT + 6];
 #pragma unroll
-        for (int k = 0; k < CPT + 6; ++k) {
-            const float fl = 0.5f * w[k] * w[k];
-            fp[k] = 0.5f * (fl + alpha * w[k]);
-            fm[k] = 0.5f * (fl - alpha * w[k]);
-        }
+        for (int k = 0; k < CPT + 6; ++k) flux_split(w[k], 0.5f * alpha, fp[k], fm[k]);
         float accp[CPT + 5], accm[CPT + 5];  // index e <-> cell cell0 - 2 + e
 #pragma unroll
         for (int e = 0; e < CPT + 5; ++e) { accp[e] = 0.f; accm[e] = 0.f; }
@@ -538,30 +564,9 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
         float alpha = 0.f;
 #pragma unroll
         for (int i = 0; i < TPR / 32; ++i) alpha = fmaxf(alpha, sh.wmax[parity][i]);
-        float fp[CPT + 6], fm[CPT + 6];
-#pragma unroll
-        for (int k = 0; k < CPT + 6; ++k) {
-            const float fl = 0.5f * w[k] * w[k];
-            fp[k] = 0.5f * (fl + alpha * w[k]);
-            fm[k] = 0.5f * (fl - alpha * w[k]);
-        }
-        float hp_prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]);
-        float hm_prev = weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-            const float hp = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]);
-            const float hm = weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
-            const float nl = -((hp - hp_prev) * inv_dx + (hm - hm_prev) * inv_dx);
-            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
-            hp_prev = hp;
-            hm_prev = hm;
-        }
+        weno_rhs<CPT>(w, alpha, nu * inv_dx2, inv_dx, r);
     } else {
-#pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-            const float nl = -w[c + 3] * ((w[c + 4] - w[c + 2]) * inv_2dx);
-            r[c] = nl + nu * ((w[c + 2] - 2.f * w[c + 3] + w[c + 4]) * inv_dx2);
-        }
+        fdm_rhs<CPT>(w, nu * inv_dx2, inv_2dx, r);
     }
 }
 
