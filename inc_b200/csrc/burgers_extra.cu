@@ -3,7 +3,8 @@
 // Ragged batch: rows of different n / nu / dt / dx packed back to back.  A
 // persistent grid of warps pulls row indices from one atomic counter
 // (fetch-and-add only, no waiting) in the caller's longest-first order; each
-// warp advances its row through all steps with the state in registers.
+// warp advances its row (or, for rows narrower than 128, 32 / (n/4) rows of one
+// width, one per lane group) through all steps with the state in registers.
 //
 // Adaptive step (solver_1d.py:148-179): Euler substeps with
 // dt_local = min(remaining, CFL * dx / max|u|) where the max runs over the
@@ -27,27 +28,45 @@ struct RaggedArgs {
     int rows, steps, scheme, conv;
 };
 
+// Advance this lane's row (row < 0: the lane's group is idle).  Groups of TPR
+// lanes are independent: a warp holds 32 / TPR rows of one width at a time.
 template <int CPT, int TPR>
-INC_DEV void ragged_row(const RaggedArgs& ra, int row, int lane) {
+INC_DEV void ragged_rows(const RaggedArgs& ra, int row, int lane) {
     const int g = lane % TPR;
-    const bool valid = lane < TPR;  // the first TPR lanes hold the row
+    const bool valid = row >= 0;
+    const int r = valid ? row : 0;
     const int left = (g + TPR - 1) & (TPR - 1), right = (g + 1) & (TPR - 1);
     Args a;
     memset(&a, 0, sizeof(a));
     a.rows = 1; a.n = CPT * TPR; a.scheme = ra.scheme; a.conv = ra.conv; a.src = INC_SRC_NONE;
-    const float dx = __ldg(ra.dx_rows + row);
+    const float dx = __ldg(ra.dx_rows + r);
     a.dx = dx; a.inv_dx = 1.f / dx; a.inv_dx2 = 1.f / (dx * dx); a.inv_2dx = 0.5f / dx;
     Ctx<CPT> cx;
-    cx.nu = __ldg(ra.nu_rows + row);
-    cx.dt = __ldg(ra.dt_rows + row);
-    cx.beta = 0.f; cx.t = 0.f; cx.has_s = false; cx.cell0 = g * CPT; cx.row = row; cx.valid = valid;
+    cx.nu = __ldg(ra.nu_rows + r);
+    cx.dt = __ldg(ra.dt_rows + r);
+    cx.beta = 0.f; cx.t = 0.f; cx.has_s = false; cx.cell0 = g * CPT; cx.row = r; cx.valid = valid;
 #pragma unroll
     for (int c = 0; c < CPT; ++c) cx.s[c] = 0.f;
-    const int64_t base = __ldg(ra.offsets + row) + g * CPT;
+    const int64_t base = __ldg(ra.offsets + r) + g * CPT;
     float u[CPT];
     load_row_chunk<CPT>(u, ra.u0 + base, valid);
     for (int k = 0; k < ra.steps; ++k) advance<CPT, TPR>(a, cx, u, 0.f, left, right);
     store_row_chunk<CPT>(ra.out + base, u, valid);
+}
+
+// Rows of width n: one per warp from n = 128 on (4, 8, 16 cells per lane);
+// narrower rows (4 cells per lane, n/4 lanes each) fill the warp, one row per
+// group of lanes.  `row` is this lane's row (or -1).
+INC_DEV void ragged_dispatch(const RaggedArgs& ra, int n, int row, int lane) {
+    switch (n) {
+        case 8: ragged_rows<4, 2>(ra, row, lane); break;
+        case 16: ragged_rows<4, 4>(ra, row, lane); break;
+        case 32: ragged_rows<4, 8>(ra, row, lane); break;
+        case 64: ragged_rows<4, 16>(ra, row, lane); break;
+        case 128: ragged_rows<4, 32>(ra, row, lane); break;
+        case 256: ragged_rows<8, 32>(ra, row, lane); break;
+        default: ragged_rows<16, 32>(ra, row, lane); break;  // 512 (checked on the host)
+    }
 }
 
 __global__ void __launch_bounds__(256) k_ragged(RaggedArgs ra) {
@@ -58,14 +77,34 @@ __global__ void __launch_bounds__(256) k_ragged(RaggedArgs ra) {
         item = __shfl_sync(0xffffffffu, item, 0);
         if (item >= ra.rows) break;
         const int row = __ldg(ra.order + item);
-        switch (__ldg(ra.n_rows + row)) {
-            case 8: ragged_row<4, 2>(ra, row, lane); break;
-            case 16: ragged_row<4, 4>(ra, row, lane); break;
-            case 32: ragged_row<4, 8>(ra, row, lane); break;
-            case 64: ragged_row<4, 16>(ra, row, lane); break;
-            case 128: ragged_row<4, 32>(ra, row, lane); break;
-            case 256: ragged_row<8, 32>(ra, row, lane); break;
-            default: ragged_row<16, 32>(ra, row, lane); break;  // 512 (checked on the host)
+        const int n = __ldg(ra.n_rows + row);
+        if (n >= 128) {
+            ragged_dispatch(ra, n, row, lane);
+            continue;
+        }
+        // Narrow rows: claim per - 1 more items for the other lane groups.  The
+        // order is longest first, so they are usually of the same width; any
+        // that are not run afterwards, one per warp.
+        const int tpr = n / 4, per = 32 / tpr;
+        int first = 0;
+        if (lane == 0) first = atomicAdd(ra.queue, per - 1);
+        first = __shfl_sync(0xffffffffu, first, 0);
+        const int j = lane / tpr;
+        int mine = -1;
+        if (j == 0) {
+            mine = row;
+        } else if (first + j - 1 < ra.rows) {
+            const int r = __ldg(ra.order + first + j - 1);
+            if (__ldg(ra.n_rows + r) == n) mine = r;
+        }
+        ragged_dispatch(ra, n, mine, lane);
+        for (int jj = 1; jj < per; ++jj) {
+            const int it = first + jj - 1;
+            if (it >= ra.rows) break;
+            const int r = __ldg(ra.order + it);
+            const int nn = __ldg(ra.n_rows + r);
+            if (nn == n) continue;
+            ragged_dispatch(ra, nn, (lane < (nn >= 128 ? 32 : nn / 4)) ? r : -1, lane);
         }
     }
 }

@@ -256,6 +256,32 @@ def test_ragged_batch_vs_oracle(cuda):
         assert rel_l2(got.cpu().numpy(), ref[0]) < TOL, n
 
 
+def test_ragged_narrow_rows_share_warps(cuda):
+    """Rows narrower than 128 run several per warp (one per lane group); widths mixed so
+    that some warps claim rows of another width and run them afterwards."""
+    from inc_b200.batched import RaggedBurgers
+    rng = np.random.default_rng(21)
+    ns = list(rng.choice([8, 16, 32, 64], size=61)) + [128, 256, 512]
+    rows = []
+    for i, n in enumerate(ns):
+        n = int(n)
+        nu = float(np.exp(rng.uniform(np.log(1e-3), np.log(5e-2))))
+        u0 = _rand_u0(1, n, 300 + i)[0]
+        dx = 2 * math.pi / n
+        dt = 0.4 * min(dx / np.abs(u0).max(), dx * dx / nu)
+        rows.append((u0, nu, dt, dx))
+    rb = RaggedBurgers([r[0] for r in rows], [r[1] for r in rows], [r[2] for r in rows], [r[3] for r in rows],
+                       scheme="ssprk3", device=cuda)
+    out = rb.rollout(steps=12)
+    for (u0, nu, dt, dx), got in zip(rows, rb.unpack(out)):
+        n = u0.shape[0]
+        p = ob.BurgersParams(resolution=n, L=dx * n, dt=dt, nu=nu)
+        ref, t = u0[None], 0.0
+        for _ in range(12):
+            ref, t = ob.step_ssprk3(ref, p, t)
+        assert rel_l2(got.cpu().numpy(), ref[0]) < TOL, n
+
+
 def test_errors(cuda):
     from inc_b200.solvers import BurgersSolverTorch
     p = ob.BurgersParams(resolution=96, L=2 * math.pi, dt=0.01, nu=0.01)
