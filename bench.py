@@ -222,7 +222,7 @@ def fp32_peak_tflops(device):
 def bench_ks(args, dev, world):
     import torch
     from types import SimpleNamespace
-    from inc_b200.roofline import ks_flops_per_cell_step, plain_bytes_per_cell_step
+    from inc_b200.roofline import ks_flops_per_cell_step, ks_impl_flops_per_cell_step, plain_bytes_per_cell_step
     from inc_b200.rollout import ks_rollout
     from inc_b200.solvers import KSSolverTorch
     from inc_b200.workloads import ks_plain_config
@@ -351,14 +351,18 @@ def bench_ks(args, dev, world):
     # (profiles/ks_rollout_fused_b1024_n256_dram.md): 3.07 MB read + 359.1 MB written.
     extra_traffic = 362.2e6 if (B, N, steps) == (1024, 256, 400) else None
     peak = fp32_peak_tflops(dev)
-    flops_cell = ks_flops_per_cell_step(N, cfg["scheme"])
+    flops_cell = ks_flops_per_cell_step(N, cfg["scheme"])  # the reference algorithm's frozen count
     achieved = flops_cell * cells / (ms_fused * 1e-3) / 1e12
+    impl_cell = ks_impl_flops_per_cell_step(N, cfg["scheme"])  # what this kernel executes
+    impl_achieved = impl_cell * cells / (ms_fused * 1e-3) / 1e12
     plain_ms_step = sum(t_plain) / len(t_plain) / steps
     times = dict(fused=ms_fused, plain=sum(t_plain) / len(t_plain), graph=sum(t_graph) / len(t_graph),
                  fused_fb=sum(t_ffb) / len(t_ffb), plain_fb=sum(t_pfb) / len(t_pfb),
                  e2e=sum(t_e2e) / len(t_e2e))
     extra = dict(
         flops_per_cell_step=flops_cell, peak=peak, achieved=achieved,
+        implementation={"flops_per_cell_step": impl_cell, "achieved": impl_achieved, "frac": impl_achieved / peak,
+                        "note": "flops this kernel executes: two rows per complex FFT, FFT(s) once per launch"},
         plain_hbm_gbs=plain_bytes_per_cell_step(True) * B * N / (plain_ms_step * 1e-3) / 1e9,
         clocks=clk.summary(), h2d=2 * B * N * 4, d2h=B * N * 4, launches=args.steps, traffic=extra_traffic,
     )
@@ -750,7 +754,10 @@ def main():
                                             "profiles/ks_rollout_fused_b1024_n256_dram.md")
                          if extra.get("traffic") else None,
                          "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run",
-                         "flops_per_cell_step": extra["flops_per_cell_step"]},
+                         "flops_per_cell_step": extra["flops_per_cell_step"],
+                         "flops_source": ("frozen per-cell-step count of the reference algorithm "
+                                          "(inc_b200/roofline.py)"),
+                         "implementation": extra.get("implementation")},
             "cpu_baseline": cpu_b,
             "clocks": clk,
             "gpu_launches": extra["launches"],

@@ -11,11 +11,17 @@ Burgers WENO5-LF right-hand side, per cell (solver_1d.py:4-42, :129-146):
   flux splitting 8; flux differences 6; diffusion stencil 5; alpha max 1;
   source add 5 -> 165.  Euler step = 165 + 2; SSP-RK3 = 3 * 165 + 8.
 
-KS ETRK2 substep, per cell (solver_1d.py:257-278): four real FFTs of length N
-(FFT(u^2), IFFT, FFT(ui^2), IFFT) at 2.5 N log2 N flops each (half the
-5 N log2 N of a complex FFT) -> 10 log2 N; pointwise work 12 (two squares,
-and per half-spectrum bin the multipliers of stage 1 and 2).  One step() is
-two substeps.  ETD1 substep: two real FFTs -> 5 log2 N + 8.
+KS, the frozen count of the reference algorithm (the roofline numerator):
+per substep five complex length-N FFT-class ops (FFT(u^2), IFFT, FFT(u_i^2),
+IFFT and FFT(s), solver_1d.py:257-278) at 5 log2 N flops per cell each, plus
+~45 pointwise flops; one step() is two substeps: 2 (25 log2 N + 45) = 490 at
+N = 256, 540 at N = 512.  ETD1 by the same rule has four FFT-class ops and ~20
+pointwise flops per substep (solver_1d.py:242-255).
+
+KS, this implementation's own count (reported beside it): two rows share one
+complex FFT and s is transformed once per launch, so a substep is four real
+FFTs at 2.5 N log2 N flops each -> 10 log2 N per cell, plus 12 pointwise:
+2 (10 log2 N + 12) = 184 at N = 256 (ETD1: 2 (5 log2 N + 8)).
 
 Bytes per cell-step (FP32): a step() launch reads u and writes u' (8 B) and
 reads s when present (+4 B); a fused rollout writes one frame per step (4 B)
@@ -30,6 +36,14 @@ BURGERS_FLOPS = {"euler": BURGERS_RHS_FLOPS + 2, "ssprk3": 3 * BURGERS_RHS_FLOPS
 
 
 def ks_flops_per_cell_step(n: int, scheme: str = "ETRK2") -> float:
+    """Reference-algorithm flops per cell-step (the roofline numerator)."""
+    lg = math.log2(n)
+    sub = (25 * lg + 45) if scheme == "ETRK2" else (20 * lg + 20)
+    return 2 * sub
+
+
+def ks_impl_flops_per_cell_step(n: int, scheme: str = "ETRK2") -> float:
+    """Flops per cell-step this implementation executes (row pairs share one FFT)."""
     lg = math.log2(n)
     sub = (10 * lg + 12) if scheme == "ETRK2" else (5 * lg + 8)
     return 2 * sub

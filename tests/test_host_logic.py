@@ -98,10 +98,11 @@ def test_workloads_are_seeded_and_shaped():
 
 
 def test_roofline_counts():
-    from inc_b200.roofline import BURGERS_FLOPS, ks_flops_per_cell_step
+    from inc_b200.roofline import BURGERS_FLOPS, ks_flops_per_cell_step, ks_impl_flops_per_cell_step
     assert BURGERS_FLOPS["euler"] == 167 and BURGERS_FLOPS["ssprk3"] == 503
-    assert ks_flops_per_cell_step(256) == 184
-    assert ks_flops_per_cell_step(256, "ETD1") == 2 * (5 * 8 + 8)
+    assert ks_flops_per_cell_step(256) == 490 and ks_flops_per_cell_step(512) == 540  # frozen reference counts
+    assert ks_impl_flops_per_cell_step(256) == 184
+    assert ks_impl_flops_per_cell_step(256, "ETD1") == 2 * (5 * 8 + 8)
 
 
 def test_solver_errors_without_gpu():
