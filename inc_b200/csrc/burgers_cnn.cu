@@ -18,172 +18,11 @@
 // row at apad(x + 2) with x in [-2, N + 2) (the circular halo is stored); the
 // 4-float pad per 32 makes the float4 reads conflict-free.  All weights
 // (42.6 KB) sit in shared memory for the whole launch.
-#include "burgers_kernels.cuh"
+#include "burgers_cnn.cuh"
 
 namespace inc {
 namespace burgers {
-
-int fill_args(const inc_burgers_desc* d, Args& a);  // burgers_api.cu
-
 namespace cnn {
-
-constexpr int C = 32;   // hidden channels
-constexpr int KW = 5;   // kernel width
-// Packed weights (inc_burgers_cnn_rollout): w1[co][k], b1[co], w2[ci][co][k],
-// b2[co], w3[ci][co][k], b3[co], w4[ci][k], b4.
-constexpr int OFF_W1 = 0;
-constexpr int OFF_B1 = OFF_W1 + C * KW;
-constexpr int OFF_W2 = OFF_B1 + C;
-constexpr int OFF_B2 = OFF_W2 + C * C * KW;
-constexpr int OFF_W3 = OFF_B2 + C;
-constexpr int OFF_B3 = OFF_W3 + C * C * KW;
-constexpr int OFF_W4 = OFF_B3 + C;
-constexpr int OFF_B4 = OFF_W4 + C * KW;
-constexpr int W_FLOATS = OFF_B4 + 1;
-constexpr int W_SMEM = (W_FLOATS + 3) / 4 * 4;
-static_assert(INC_CNN_WEIGHT_FLOATS == W_FLOATS, "packed weight size");
-static_assert(OFF_W2 % 4 == 0 && OFF_W3 % 4 == 0 && OFF_B1 % 4 == 0 && OFF_B2 % 4 == 0 && OFF_B3 % 4 == 0,
-              "float4 weight loads");
-
-INC_DEV constexpr int apad(int p) { return p + ((p >> 5) << 2); }
-template <int N>
-INC_DEV constexpr int row_len() { return (apad(N + 3) + 1 + 3) / 4 * 4; }
-template <int N>
-INC_DEV constexpr int rows_per_cta() { return N >= 512 ? 1 : 512 / N; }
-
-template <int N>
-struct Smem {
-    float w[W_SMEM];
-    float act[2][rows_per_cta<N>()][C][row_len<N>()];
-    WideSmem<1, N> sh[rows_per_cta<N>()];
-};
-
-// torch.nn.functional.gelu, approximate='none'
-INC_DEV float gelu(float x) { return 0.5f * x * (1.f + erff(x * 0.70710678118654752f)); }
-
-INC_DEV float4 lds4(const float* p) { return *reinterpret_cast<const float4*>(p); }
-
-// cells 8L-2 .. 8L+9 of one activation row
-INC_DEV void load12(float (&a)[12], const float* row, int L) {
-    const float4 v0 = lds4(row + apad(8 * L)), v1 = lds4(row + apad(8 * L + 4)), v2 = lds4(row + apad(8 * L + 8));
-    a[0] = v0.x; a[1] = v0.y; a[2] = v0.z; a[3] = v0.w;
-    a[4] = v1.x; a[5] = v1.y; a[6] = v1.z; a[7] = v1.w;
-    a[8] = v2.x; a[9] = v2.y; a[10] = v2.z; a[11] = v2.w;
-}
-
-// cells 8L .. 8L+7 of one row, plus the halo copies the row's ends own
-template <int N>
-INC_DEV void store8(float* row, int L, const float (&v)[8]) {
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-        *reinterpret_cast<float2*>(row + apad(8 * L + 2 + 2 * i)) = make_float2(v[2 * i], v[2 * i + 1]);
-    if (L == 0) {  // x = 0, 1 -> x = N, N + 1
-        row[apad(N + 2)] = v[0];
-        row[apad(N + 3)] = v[1];
-    }
-    if (L == N / 8 - 1) {  // x = N - 2, N - 1 -> x = -2, -1
-        row[apad(0)] = v[6];
-        row[apad(1)] = v[7];
-    }
-}
-
-template <int N>
-INC_DEV void put_cell(float* row, int g, float v) {
-    row[apad(g + 2)] = v;
-    if (g < 2) row[apad(N + 2 + g)] = v;
-    if (g >= N - 2) row[apad(g - N + 2)] = v;
-}
-
-// Layer 1: one input channel -> channels 4 cg .. 4 cg + 3, GELU.
-template <int N>
-INC_DEV void conv_first(const float* w, const float* in, float (*out)[row_len<N>()], int cg, int L) {
-    float a[12];
-    load12(a, in, L);
-    const float4 b = lds4(w + OFF_B1 + 4 * cg);
-    const float bias[4] = {b.x, b.y, b.z, b.w};
-    float wv[20];
-#pragma unroll
-    for (int i = 0; i < 5; ++i) {
-        const float4 q = lds4(w + OFF_W1 + 20 * cg + 4 * i);
-        wv[4 * i] = q.x; wv[4 * i + 1] = q.y; wv[4 * i + 2] = q.z; wv[4 * i + 3] = q.w;
-    }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        float o[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) {
-            float acc = bias[c];
-#pragma unroll
-            for (int k = 0; k < KW; ++k) acc = fmaf(wv[c * KW + k], a[j + k], acc);
-            o[j] = gelu(acc);
-        }
-        store8<N>(out[4 * cg + c], L, o);
-    }
-}
-
-// Layers 2 and 3: 32 -> channels 4 cg .. 4 cg + 3, GELU.  wt is [ci][co][k].
-template <int N>
-INC_DEV void conv_mid(const float* wt, const float* bias_p, float (*in)[row_len<N>()],
-                      float (*out)[row_len<N>()], int cg, int L) {
-    float acc[4][8];
-    {
-        const float4 b = lds4(bias_p + 4 * cg);
-        const float bias[4] = {b.x, b.y, b.z, b.w};
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[c][j] = bias[c];
-    }
-#pragma unroll 2
-    for (int ci = 0; ci < C; ++ci) {
-        float a[12], wv[20];
-        load12(a, in[ci], L);
-        const float* wp = wt + ci * C * KW + 20 * cg;
-#pragma unroll
-        for (int i = 0; i < 5; ++i) {
-            const float4 q = lds4(wp + 4 * i);
-            wv[4 * i] = q.x; wv[4 * i + 1] = q.y; wv[4 * i + 2] = q.z; wv[4 * i + 3] = q.w;
-        }
-#pragma unroll
-        for (int c = 0; c < 4; ++c)
-#pragma unroll
-            for (int k = 0; k < KW; ++k)
-#pragma unroll
-                for (int j = 0; j < 8; ++j) acc[c][j] = fmaf(wv[c * KW + k], a[j + k], acc[c][j]);
-    }
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        float o[8];
-#pragma unroll
-        for (int j = 0; j < 8; ++j) o[j] = gelu(acc[c][j]);
-        store8<N>(out[4 * cg + c], L, o);
-    }
-}
-
-// Layer 4: channels 4 cg .. 4 cg + 3 -> partial sums of the single output
-// channel, stored in row cg of `part` (the other buffer); no bias, no GELU.
-template <int N>
-INC_DEV void conv_last_partial(const float* w4, float (*in)[row_len<N>()], float (*part)[row_len<N>()], int cg,
-                               int L) {
-    float acc[8];
-#pragma unroll
-    for (int j = 0; j < 8; ++j) acc[j] = 0.f;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        const int ci = 4 * cg + c;
-        float a[12];
-        load12(a, in[ci], L);
-#pragma unroll
-        for (int k = 0; k < KW; ++k) {
-            const float wk = w4[ci * KW + k];
-#pragma unroll
-            for (int j = 0; j < 8; ++j) acc[j] = fmaf(wk, a[j + k], acc[j]);
-        }
-    }
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-        *reinterpret_cast<float2*>(part[cg] + apad(8 * L + 2 + 2 * i)) = make_float2(acc[2 * i], acc[2 * i + 1]);
-}
 
 template <int N>
 __global__ void __launch_bounds__(512) k_cnn_rollout(Args a, const float* __restrict__ wts,
@@ -207,7 +46,10 @@ __global__ void __launch_bounds__(512) k_cnn_rollout(Args a, const float* __rest
     int parity = 0;
     float (*act0)[row_len<N>()] = S.act[0][rl];
     float (*act1)[row_len<N>()] = S.act[1][rl];
+    const int nseg = a.ckpt_every > 0 ? (a.steps + a.ckpt_every - 1) / a.ckpt_every : 0;
     for (int k = 0; k < a.steps; ++k) {
+        if (a.ckpts && valid && k % a.ckpt_every == 0)
+            a.ckpts[((int64_t)row * nseg + k / a.ckpt_every) * N + g] = u[0];
         put_cell<N>(act0[0], g, u[0]);
         __syncthreads();  // also: the weights are in place (first step)
         conv_first<N>(S.w, act0[0], act1, cg, L);
@@ -250,11 +92,15 @@ using namespace inc::burgers;
 
 extern "C" int inc_burgers_cnn_rollout(const inc_burgers_desc* d, const float* weights, const float* u0,
                                        const float* t_rows, double t0, int32_t steps, float* frames,
-                                       float* corrections, float* u_final, void* stream) {
+                                       float* corrections, float* u_final, int32_t ckpt_every, float* ckpts,
+                                       void* stream) {
     Args a;
     int rc = fill_args(d, a);
     if (rc) return rc;
     if (!weights || !u0 || steps < 0) { set_error("cnn_rollout: bad arguments"); return INC_E_INVALID; }
+    if (ckpts && ckpt_every <= 0) { set_error("cnn_rollout: ckpt_every must be positive with ckpts"); return INC_E_INVALID; }
+    a.ckpt_every = ckpt_every;
+    a.ckpts = ckpts;
     if (((reinterpret_cast<uintptr_t>(weights)) & 15u) != 0) {
         set_error("cnn_rollout: weights must be 16-byte aligned");
         return INC_E_INVALID;

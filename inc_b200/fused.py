@@ -5,10 +5,13 @@
 u = solver.step(u); results[:, k] = u``) for a ``PeriodicCNN1D`` corrector in
 one launch of ``inc_burgers_cnn_rollout``: the four convolutions run from
 shared memory before every step, so no per-step corrector launches remain.
-Forward only -- evaluation rollouts under ``torch.no_grad()``; training keeps
-the per-step graph (torch corrector plus the CUDA solver's autograd
-functions).  ``simulate_rollout`` dispatches here by itself when gradients are
-off and the model and solver qualify (``cnn_supported``).
+With gradients on (rows of 256 cells), the rollout is one autograd node
+whose backward is ``inc_burgers_cnn_rollout_bwd``: segment replay from
+checkpoints, the network's activations recomputed in shared memory, the
+solver's adjoint and the network's backward in one kernel, weight gradients
+summed over rows in a fixed order.  ``simulate_rollout`` dispatches here by
+itself when the model and solver qualify (``cnn_supported`` /
+``cnn_train_supported``); otherwise it keeps the per-step loop.
 """
 from __future__ import annotations
 
@@ -59,23 +62,104 @@ def pack_cnn_weights(model, device=None) -> torch.Tensor:
     return out
 
 
-def burgers_cnn_rollout(model, solver, u0, steps, corrections=True):
+CNN_TRAIN_N = 256
+MAX_CKPT_EVERY = 32
+
+
+def cnn_train_supported(model, solver, u) -> bool:
+    """True when the fused training kernel (forward + backward) covers this case."""
+    return cnn_supported(model, solver, u) and u.shape[1] == CNN_TRAIN_N
+
+
+def unpack_cnn_grads(g: torch.Tensor):
+    """Packed gradient -> (w1, b1, w2, b2, w3, b3, w4, b4) in torch's Conv1d shapes."""
+    C, K = 32, 5
+    o = [0]
+
+    def take(n):
+        v = g[o[0]:o[0] + n]
+        o[0] += n
+        return v
+    w1 = take(C * K).view(C, 1, K)
+    b1 = take(C)
+    w2 = take(C * C * K).view(C, C, K).transpose(0, 1).contiguous()
+    b2 = take(C)
+    w3 = take(C * C * K).view(C, C, K).transpose(0, 1).contiguous()
+    b3 = take(C)
+    w4 = take(C * K).view(1, C, K)
+    b4 = take(1)
+    return w1, b1, w2, b2, w3, b3, w4, b4
+
+
+class BurgersCNNRolloutFn(torch.autograd.Function):
+    """Frames and corrections of the fused hybrid rollout, differentiable w.r.t. u0 and
+    the eight parameters of the corrector."""
+
+    @staticmethod
+    def forward(ctx, u0, launch, steps, ckpt_every, *params):
+        B, N = u0.shape
+        w = _pack_params(params, u0.device)
+        frames = torch.empty(B, steps, N, device=u0.device, dtype=torch.float32)
+        corr = torch.empty_like(frames)
+        nseg = (steps + ckpt_every - 1) // ckpt_every
+        ckpts = torch.empty(B, nseg, N, device=u0.device, dtype=torch.float32)
+        launch.cnn_rollout(w, u0, steps, frames, corr, None, ckpt_every, ckpts)
+        ctx.save_for_backward(ckpts, corr, w)
+        ctx.launch, ctx.steps, ctx.ckpt_every, ctx.shape = launch, steps, ckpt_every, (B, N)
+        return frames, corr
+
+    @staticmethod
+    def backward(ctx, g_frames, g_corr):
+        ckpts, corr, w = ctx.saved_tensors
+        B, N = ctx.shape
+        dev = ckpts.device
+        g_u0 = torch.empty(B, N, device=dev, dtype=torch.float32)
+        g_w = torch.empty(nat.INC_CNN_WEIGHT_FLOATS, device=dev, dtype=torch.float32)
+        work = torch.empty(B, nat.INC_CNN_WEIGHT_FLOATS, device=dev, dtype=torch.float32)
+        gf = None if g_frames is None else g_frames.contiguous()
+        gc = None if g_corr is None else g_corr.contiguous()
+        ctx.launch.cnn_rollout_bwd(w, ckpts, corr, ctx.steps, ctx.ckpt_every, gf, gc, None, g_u0, g_w, work)
+        return (g_u0, None, None, None) + unpack_cnn_grads(g_w)
+
+
+def _pack_params(params, device):
+    w1, b1, w2, b2, w3, b3, w4, b4 = [p.detach().float() for p in params]
+    out = torch.cat([w1[:, 0, :].reshape(-1), b1, w2.transpose(0, 1).reshape(-1), b2,
+                     w3.transpose(0, 1).reshape(-1), b3, w4[0].reshape(-1), b4]).to(device).contiguous()
+    return out
+
+
+def burgers_cnn_rollout(model, solver, u0, steps, corrections=True, ckpt_every=8):
     """(frames [B, steps, N], corrections [B, steps, N] or None) of the hybrid rollout,
     as ``simulate_rollout(model, solver, u0, steps, "INC")`` computes them.
 
-    Advances ``solver.t`` by steps * dt and leaves the last correction in
-    ``solver.correction_s``, like the per-step loop."""
+    With gradients enabled (and u0 or the model's parameters requiring them) the
+    result is differentiable through the fused backward, which replays
+    ckpt_every-step segments (n = 256).  Advances ``solver.t`` by steps * dt and
+    leaves the last correction in ``solver.correction_s``, like the per-step loop."""
     if not cnn_supported(model, solver, u0):
         raise ValueError("burgers_cnn_rollout: needs a PeriodicCNN1D(32, 5, 4) corrector, a fixed-dt "
                          "BurgersSolverTorch and a CUDA float32 state of width 64, 128, 256 or 512")
-    u0 = u0.detach().contiguous()
     steps = int(steps)
-    launch = solver.launch_for(u0)
-    w = pack_cnn_weights(model, u0.device)
-    B, N = u0.shape
-    frames = torch.empty(B, steps, N, device=u0.device, dtype=torch.float32)
-    corr = torch.empty_like(frames) if corrections else None
-    launch.cnn_rollout(w, u0, steps, frames, corr, None)
+    params = [p for c in model.convs for p in (c.weight, c.bias)]
+    want = torch.is_grad_enabled() and (u0.requires_grad or any(p.requires_grad for p in params))
+    if want and steps > 0:
+        if u0.shape[1] != CNN_TRAIN_N:
+            raise ValueError(f"burgers_cnn_rollout: gradients need rows of {CNN_TRAIN_N} cells")
+        k = int(ckpt_every)
+        if not 1 <= k <= MAX_CKPT_EVERY:
+            raise ValueError(f"burgers_cnn_rollout: ckpt_every must be in [1, {MAX_CKPT_EVERY}]")
+        u0c = u0.contiguous()
+        launch = solver.launch_for(u0c)
+        frames, corr = BurgersCNNRolloutFn.apply(u0c, launch, steps, k, *params)
+    else:
+        u0c = u0.detach().contiguous()
+        launch = solver.launch_for(u0c)
+        w = pack_cnn_weights(model, u0c.device)
+        B, N = u0c.shape
+        frames = torch.empty(B, steps, N, device=u0c.device, dtype=torch.float32)
+        corr = torch.empty_like(frames) if corrections else None
+        launch.cnn_rollout(w, u0c, steps, frames, corr, None)
     solver.t += steps * solver.dt
     solver.correction_s = corr[:, -1] if (corr is not None and steps > 0) else None
-    return frames, corr
+    return frames, (corr if corrections else None)

@@ -109,10 +109,15 @@ def simulate_rollout(model, solver, u_initial, mstep, correction_term, L=None, c
             return burgers_rollout(solver, u_initial, mstep), None
     elif correction_term != "INC":
         raise ValueError(f"Invalid correction term: {correction_term}")
-    elif not torch.is_grad_enabled():
+    else:
         from . import fused
-        if fused.cnn_supported(model, solver, u_initial):  # evaluation: corrector inside the solver kernel
-            return fused.burgers_cnn_rollout(model, solver, u_initial, mstep)
+        if not torch.is_grad_enabled():
+            if fused.cnn_supported(model, solver, u_initial):  # evaluation: corrector inside the solver kernel
+                return fused.burgers_cnn_rollout(model, solver, u_initial, mstep)
+        elif fused.cnn_train_supported(model, solver, u_initial):  # training: fused forward and backward
+            k = int(checkpoint_every or 8)
+            if 1 <= k <= fused.MAX_CKPT_EVERY:
+                return fused.burgers_cnn_rollout(model, solver, u_initial, mstep, ckpt_every=k)
 
     model_fn = (lambda u: model(u)) if L is None else (lambda u: model(u, L))
     step_fn = (lambda u: solver.step(u)) if L is None else (lambda u: solver.step(u, L))

@@ -122,12 +122,22 @@ class _BurgersLaunch:
                                                nat.ptr(ckpts), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_rollout")
 
-    def cnn_rollout(self, weights, u0, steps, frames, corrections, u_final):
+    def cnn_rollout(self, weights, u0, steps, frames, corrections, u_final, ckpt_every=0, ckpts=None):
         with torch.cuda.device(self.dev):
             rc = nat.lib().inc_burgers_cnn_rollout(C.byref(self.desc), weights.data_ptr(), u0.data_ptr(),
                                                    nat.ptr(self.t_rows), self.t0, steps, nat.ptr(frames),
-                                                   nat.ptr(corrections), nat.ptr(u_final), nat.stream_of(self.dev))
+                                                   nat.ptr(corrections), nat.ptr(u_final), int(ckpt_every),
+                                                   nat.ptr(ckpts), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_cnn_rollout")
+
+    def cnn_rollout_bwd(self, weights, ckpts, corrections, steps, ckpt_every, g_frames, g_corrections, g_final,
+                        g_u0, g_weights, work):
+        with torch.cuda.device(self.dev):
+            rc = nat.lib().inc_burgers_cnn_rollout_bwd(
+                C.byref(self.desc), weights.data_ptr(), ckpts.data_ptr(), corrections.data_ptr(),
+                nat.ptr(self.t_rows), self.t0, steps, ckpt_every, nat.ptr(g_frames), nat.ptr(g_corrections),
+                nat.ptr(g_final), g_u0.data_ptr(), g_weights.data_ptr(), work.data_ptr(), nat.stream_of(self.dev))
+        nat.check(rc, "inc_burgers_cnn_rollout_bwd")
 
     def rollout_bwd(self, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s):
         with torch.cuda.device(self.dev):

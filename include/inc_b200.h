@@ -187,9 +187,10 @@ int inc_burgers_rollout_grad_noalloc(const inc_burgers_desc* d, const float* u0,
  * s = CNN(u), then u = step(u, s) -- simulate_rollout with correction "INC"
  * (trainer/trainer_1d.py:154-183) and the benchmark's periodic CNN corrector
  * (PeriodicCNN1D: Conv1d 1 -> 32 -> 32 -> 32 -> 1, kernel 5, circular padding,
- * erf GELU between layers), forward only.  It replaces the per-step pair
- * `s = model(u); u = solver.step(u)` of the reference loop, for evaluation
- * rollouts.  weights: device, INC_CNN_WEIGHT_FLOATS floats, 16-byte aligned,
+ * erf GELU between layers).  ckpts (with ckpt_every > 0) receives the state at
+ * the start of every ckpt_every-th step for the backward below, or is NULL.
+ * It replaces the per-step pair
+ * `s = model(u); u = solver.step(u)` of the reference loop.  weights: device, INC_CNN_WEIGHT_FLOATS floats, 16-byte aligned,
  * packed as w1[co][k], b1[co], w2[ci][co][k], b2[co], w3[ci][co][k], b3[co],
  * w4[ci][k], b4 (torch's Conv1d weight is [co][ci][k]; the hidden layers are
  * stored input-channel major).  frames, corrections ([rows][steps][n]) and
@@ -199,7 +200,24 @@ int inc_burgers_rollout_grad_noalloc(const inc_burgers_desc* d, const float* u0,
 int inc_burgers_cnn_rollout(const inc_burgers_desc* d, const float* weights,
                             const float* u0, const float* t_rows, double t0,
                             int32_t steps, float* frames, float* corrections,
-                            float* u_final, void* stream);
+                            float* u_final, int32_t ckpt_every, float* ckpts,
+                            void* stream);
+/* Backward of inc_burgers_cnn_rollout (the training step of the hybrid
+ * rollout): from the forward's checkpoints (ckpts [rows][ceil(steps/k)][n],
+ * written with ckpt_every = k) and corrections, and the adjoints of the
+ * frames and corrections (either may be NULL), it replays each k-step segment,
+ * recomputes the network's activations and returns dL/du0 (g_u0 [rows][n]) and
+ * dL/dweights (g_weights, INC_CNN_WEIGHT_FLOATS floats in the packed layout).
+ * work: rows * INC_CNN_WEIGHT_FLOATS floats of device scratch (per-row weight
+ * gradients, summed in a fixed order, so results are deterministic).
+ * n = 256 only (else INC_E_UNSUPPORTED); ckpt_every <= 32.                   */
+int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const float* weights,
+                                const float* ckpts, const float* corrections,
+                                const float* t_rows, double t0, int32_t steps,
+                                int32_t ckpt_every, const float* g_frames,
+                                const float* g_corrections, const float* g_final,
+                                float* g_u0, float* g_weights, float* work,
+                                void* stream);
 
 /* ---- Kuramoto-Sivashinsky --------------------------------------------- */
 /* Bytes of device memory a plan needs.                                       */

@@ -99,8 +99,9 @@ def test_fused_cnn_rollout_vs_fp64_loop(cuda, N, B, scheme):
     steps = 12
     ref_f, ref_c = _fp64_loop(net, p, u0, steps, scheme)
     solver = BurgersSolverTorch(_sim_params(p, B, scheme, cuda))
-    frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver, torch.tensor(u0, dtype=torch.float32,
-                                                                                  device=cuda), steps)
+    with torch.no_grad():
+        frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver,
+                                           torch.tensor(u0, dtype=torch.float32, device=cuda), steps)
     assert rel_l2(frames.cpu().numpy(), ref_f) < TOL
     assert rel_l2(corr.cpu().numpy(), ref_c) < TOL
     assert np.max(np.abs(corr.cpu().numpy())) > 1e-2  # the corrector is not negligible
@@ -119,14 +120,27 @@ def test_fused_cnn_rollout_sources_and_convection(cuda, eq, conv):
     ref_f, ref_c = _fp64_loop(net, p, u0, steps, "ssprk3", t0=0.3)
     solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
     solver.t = 0.3
-    frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver,
-                                       torch.tensor(u0, dtype=torch.float32, device=cuda), steps)
+    with torch.no_grad():
+        frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver,
+                                           torch.tensor(u0, dtype=torch.float32, device=cuda), steps)
     assert rel_l2(frames.cpu().numpy(), ref_f) < TOL
     assert rel_l2(corr.cpu().numpy(), ref_c) < TOL
 
 
+def _per_step_loop(net, solver, u0, steps):
+    """The reference's loop on the GPU: torch corrector + one CUDA step() per step."""
+    u, frames, corr = u0, [], []
+    for _ in range(steps):
+        c = net(u)
+        solver.correction_s = c
+        u = solver.step(u)
+        frames.append(u)
+        corr.append(c)
+    return torch.stack(frames, 1), torch.stack(corr, 1)
+
+
 def test_fused_matches_per_step_gpu_loop_and_dispatch(cuda):
-    """simulate_rollout under no_grad takes the fused kernel; with grad on it runs the per-step loop."""
+    """simulate_rollout takes the fused kernel with gradients off and on; both match the loop."""
     from inc_b200.rollout import simulate_rollout
     from inc_b200.solvers import BurgersSolverTorch
     N, B, steps = 256, 37, 16
@@ -137,12 +151,99 @@ def test_fused_matches_per_step_gpu_loop_and_dispatch(cuda):
     with torch.no_grad():
         f1, c1 = simulate_rollout(net, s1, u0, steps, "INC")
     s2 = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
-    f2, c2 = simulate_rollout(net, s2, u0, steps, "INC")  # grad enabled: per-step path
-    assert f2.requires_grad  # the per-step graph was built
-    assert rel_l2(f1.cpu().numpy(), f2.detach().cpu().numpy()) < TOL
-    assert rel_l2(c1.cpu().numpy(), c2.detach().cpu().numpy()) < TOL
-    assert abs(float(s1.t) - float(s2.t)) < 1e-9
+    f2, c2 = simulate_rollout(net, s2, u0, steps, "INC")  # grad enabled: fused training path
+    assert f2.requires_grad and f2.grad_fn is not None
+    s3 = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+    with torch.no_grad():
+        f3, c3 = _per_step_loop(net, s3, u0, steps)
+    for f, c in ((f1, c1), (f2.detach(), c2.detach())):
+        assert rel_l2(f.cpu().numpy(), f3.cpu().numpy()) < TOL
+        assert rel_l2(c.cpu().numpy(), c3.cpu().numpy()) < TOL
+    assert abs(float(s1.t) - float(s2.t)) < 1e-9 and abs(float(s1.t) - float(s3.t)) < 1e-9
     assert torch.equal(s1.correction_s, c1[:, -1])
+
+
+@pytest.mark.parametrize("scheme,K,eq", [("ssprk3", 8, "viscosity"), ("ssprk3", 5, "learning"),
+                                         ("euler", 1, "linear"), ("ssprk3", 32, "viscosity")])
+def test_fused_training_gradients_vs_per_step_loop(cuda, scheme, K, eq):
+    """Gradients of a loss on frames and corrections w.r.t. u0 and every network parameter:
+    fused backward (segment replay, recomputed activations) vs torch autograd through the loop."""
+    from inc_b200.fused import burgers_cnn_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    N, B, steps = 256, 5, 13
+    p = _params(N, eq=eq, B=B, seed=6)
+    u0_np = _u0(B, N, seed=7)
+    gen = torch.Generator().manual_seed(3)
+    wf = torch.randn(B, steps, N, generator=gen).to(cuda)
+    wc = torch.randn(B, steps, N, generator=gen).to(cuda)
+
+    def run(fused):
+        net = _net(5).float().to(cuda)
+        solver = BurgersSolverTorch(_sim_params(p, B, scheme, cuda))
+        solver.t = 0.2
+        u0 = torch.tensor(u0_np, dtype=torch.float32, device=cuda, requires_grad=True)
+        if fused:
+            f, c = burgers_cnn_rollout(net, solver, u0, steps, ckpt_every=K)
+        else:
+            f, c = _per_step_loop(net, solver, u0, steps)
+        loss = (f * wf).sum() + 3.0 * (c * wc).sum()
+        loss.backward()
+        return loss.item(), u0.grad.cpu().numpy(), [q.grad.cpu().numpy() for q in net.parameters()]
+
+    lf, gf, pf = run(True)
+    lr, gr, pr = run(False)
+    assert abs(lf - lr) <= 1e-5 * max(1.0, abs(lr))
+    assert rel_l2(gf, gr) < 1e-4
+    for a, b in zip(pf, pr):
+        assert rel_l2(a, b) < 1e-4
+    assert max(np.abs(b).max() for b in pr) > 0
+
+
+def test_fused_training_frames_only_loss_and_graph_capture(cuda):
+    """A loss on the frames alone (the corrections' adjoint is zero) and the whole training
+    step (fused forward + backward + optimizer) replayed from a CUDA graph."""
+    from inc_b200.fused import burgers_cnn_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    N, B, steps = 256, 6, 10
+    p = _params(N)
+    u0 = torch.tensor(_u0(B, N, seed=9), dtype=torch.float32, device=cuda)
+    target = torch.zeros(B, steps, N, device=cuda)
+    grads = []
+    for fused in (True, False):
+        net = _net(6).float().to(cuda)
+        solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+        f, _ = (burgers_cnn_rollout(net, solver, u0, steps, ckpt_every=4) if fused
+                else _per_step_loop(net, solver, u0, steps))
+        torch.mean((f - target) ** 2).backward()
+        grads.append([q.grad.clone() for q in net.parameters()])
+    for a, b in zip(*grads):
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-4
+    # graph capture of the training step
+    net = _net(6).float().to(cuda)
+    solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+    opt = torch.optim.SGD(net.parameters(), lr=1e-3)
+
+    def train_step():
+        solver.t = 0.0
+        f, _ = burgers_cnn_rollout(net, solver, u0, steps, ckpt_every=4)
+        torch.mean((f - target) ** 2).backward()
+        opt.step()
+        opt.zero_grad(set_to_none=False)
+
+    side = torch.cuda.Stream(cuda)
+    side.wait_stream(torch.cuda.current_stream(cuda))
+    with torch.cuda.stream(side):
+        for _ in range(2):
+            train_step()
+    torch.cuda.current_stream(cuda).wait_stream(side)
+    w_before = net.convs[1].weight.detach().clone()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        train_step()
+    graph.replay()
+    torch.cuda.synchronize()
+    assert not torch.equal(net.convs[1].weight.detach(), w_before)
+    assert torch.isfinite(net.convs[1].weight).all()
 
 
 def test_fused_golden_learning_case(cuda):
@@ -157,8 +258,9 @@ def test_fused_golden_learning_case(cuda):
     ref_f, ref_c = _fp64_loop(net, p, u0, steps, "ssprk3", t0=t_start)
     solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
     solver.t = torch.tensor(t_start, dtype=torch.float32, device=cuda) if np.ndim(t0) else float(t0)
-    frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver,
-                                       torch.tensor(u0, dtype=torch.float32, device=cuda), steps)
+    with torch.no_grad():
+        frames, corr = burgers_cnn_rollout(net.float().to(cuda), solver,
+                                           torch.tensor(u0, dtype=torch.float32, device=cuda), steps)
     assert rel_l2(frames.cpu().numpy(), ref_f) < TOL
     assert rel_l2(corr.cpu().numpy(), ref_c) < TOL
 
@@ -175,6 +277,11 @@ def test_fused_rejects_unsupported(cuda):
     assert not cnn_supported(net, solver, u)
     with pytest.raises(ValueError):
         burgers_cnn_rollout(net, solver, u, 4)
+    p128 = _params(128)
+    s128 = BurgersSolverTorch(_sim_params(p128, 2, "euler", cuda))
+    u128 = torch.tensor(_u0(2, 128, 2), dtype=torch.float32, device=cuda)
+    with pytest.raises(ValueError):  # gradients are built for rows of 256 cells
+        burgers_cnn_rollout(net, s128, u128, 4)
     small = PeriodicCNN1D(channels=16).to(cuda)
     p = _params(64)
     solver = BurgersSolverTorch(_sim_params(p, 2, "euler", cuda))
