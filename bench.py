@@ -51,7 +51,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--profile", nargs="?", const="ks", default=None,
-                    choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd"],
+                    choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd", "burgers_cnn"],
                     help="a small case of one kernel for ncu (no JSON)")
     ap.add_argument("--profile-rows", type=int, default=1024, help="rows of the KS profile case")
     ap.add_argument("--tpp", type=int, default=None,
@@ -790,6 +790,23 @@ def profile_small(dev, which="ks", rows=1024, tpp=32):
         rb = RaggedBurgers(cfg["u0"], cfg["nu"], cfg["dt"], cfg["dx"], scheme="ssprk3", device=dev)
         for _ in range(2):
             rb.rollout(20)
+        torch.cuda.synchronize()
+        return
+    if which == "burgers_cnn":  # fused CNN-corrected rollout and its backward (256 x 256, 32 steps)
+        import math
+        from inc_b200.correctors import PeriodicCNN1D
+        from inc_b200.fused import burgers_cnn_rollout
+        from inc_b200.solvers import BurgersSolverTorch
+        B = N = 256
+        sp = SimpleNamespace(resolution=N, dt=0.01, x=None, adaptive_CFL=None, L=2 * math.pi, nu=0.01, device=dev,
+                             convection_term="WENO", equation_type="viscosity", batch_size=B, time_scheme="ssprk3")
+        solver = BurgersSolverTorch(sp)
+        torch.manual_seed(0)
+        net = PeriodicCNN1D().to(dev)
+        u0 = 0.5 * torch.randn(B, N, device=dev)
+        for _ in range(2):
+            f, c = burgers_cnn_rollout(net, solver, u0, 32, ckpt_every=8)
+            (f.square().mean() + c.square().mean()).backward()
         torch.cuda.synchronize()
         return
     if which == "burgers_plain":

@@ -50,11 +50,15 @@ INC_DEV float gelu_grad(float z) {
     return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
 }
 
-// out = gelu(in) over every slot of a [C][BRL] buffer (halo copies included)
-INC_DEV void gelu_rows(float (*out)[BRL], float (*in)[BRL]) {
-    float* o = &out[0][0];
-    const float* i = &in[0][0];
-    for (int e = threadIdx.x; e < C * BRL; e += blockDim.x) o[e] = gelu(i[e]);
+// out = gelu(in) over every slot of a [C][BRL] buffer (halo copies included),
+// by threads first .. first + count - 1, four slots at a time
+INC_DEV void gelu_rows(float (*out)[BRL], float (*in)[BRL], int first = 0, int count = 256) {
+    float4* o = reinterpret_cast<float4*>(&out[0][0]);
+    const float4* i = reinterpret_cast<const float4*>(&in[0][0]);
+    for (int e = (int)threadIdx.x - first; e < C * BRL / 4; e += count) {
+        const float4 v = i[e];
+        o[e] = make_float4(gelu(v.x), gelu(v.y), gelu(v.z), gelu(v.w));
+    }
 }
 
 INC_DEV float2 lds2(const float* p) { return *reinterpret_cast<const float2*>(p); }
@@ -89,7 +93,11 @@ INC_DEV void dgrad_mid(const float* wt, float (*dz)[BRL], float (*zprev)[BRL], i
         float* row = zprev[4 * cg + c];
         float o[8];
 #pragma unroll
-        for (int j = 0; j < 8; ++j) o[j] = acc[c][j] * gelu_grad(row[apad(8 * L + 2 + j)]);
+        for (int i = 0; i < 4; ++i) {
+            const float2 z = lds2(row + apad(8 * L + 2 + 2 * i));
+            o[2 * i] = acc[c][2 * i] * gelu_grad(z.x);
+            o[2 * i + 1] = acc[c][2 * i + 1] * gelu_grad(z.y);
+        }
         store8<BN>(row, L, o);
     }
 }
@@ -221,7 +229,10 @@ __global__ void __launch_bounds__(256) k_cnn_rollout_bwd(Args a, const float* __
             gelu_rows(S.x, S.z[1]);
             __syncthreads();
             conv_mid<BN, false>(S.w + OFF_W3, S.w + OFF_B3, S.x, S.z[2], w, lane);
-            // ---- the solver step's adjoint (warp 0): u_bar through S and s_bar
+            __syncthreads();
+            // ---- the solver step's adjoint (warp 0): u_bar through S and s_bar; meanwhile
+            // warps 1-7 form layer 4's input gelu(z3)
+            if (w != 0) gelu_rows(S.x, S.z[2], 32, 224);
             if (w == 0) {
                 const int64_t at = ((int64_t)row * a.steps + k) * BN + 8 * lane;
                 if (a.g_frames) {
@@ -245,8 +256,6 @@ __global__ void __launch_bounds__(256) k_cnn_rollout_bwd(Args a, const float* __
             }
             __syncthreads();
             // ---- layer 4 (32 -> 1, no activation): dW4, db4, then dz3 in place of z3
-            gelu_rows(S.x, S.z[2]);
-            __syncthreads();
             wgrad_part(g4, S.d, S.x[lane], w);
             gb4 += row_part_sum(S.d, w);
             {
@@ -262,7 +271,13 @@ __global__ void __launch_bounds__(256) k_cnn_rollout_bwd(Args a, const float* __
                         float acc = 0.f;
 #pragma unroll
                         for (int kk = 0; kk < KW; ++kk) acc = fmaf(S.w[OFF_W4 + ci * KW + kk], dd[j2 + 4 - kk], acc);
-                        o[j2] = acc * gelu_grad(zr[apad(8 * lane + 2 + j2)]);
+                        o[j2] = acc;
+                    }
+#pragma unroll
+                    for (int i = 0; i < 4; ++i) {
+                        const float2 z = lds2(zr + apad(8 * lane + 2 + 2 * i));
+                        o[2 * i] *= gelu_grad(z.x);
+                        o[2 * i + 1] *= gelu_grad(z.y);
                     }
                     store8<BN>(zr, lane, o);
                 }
