@@ -51,7 +51,7 @@ def _save():
     path = cache_path()
     try:
         os.makedirs(os.path.dirname(path), exist_ok=True)
-        tmp = path + ".tmp"
+        tmp = f"{path}.{os.getpid()}.tmp"  # one per process: ranks of a multi-GPU run tune concurrently
         with open(tmp, "w") as f:
             json.dump(_cache, f, indent=1, sort_keys=True)
         os.replace(tmp, path)
