@@ -158,6 +158,17 @@ def tune_ks(n, rows, scheme="ETRK2", device="cuda", steps=50, L=64.0, dt=0.25):
     return best, times
 
 
+def tune_ragged(rb, steps=20):
+    """Time the persistent ragged launch at a few grid sizes; keep the fastest on `rb`."""
+    sms = torch.cuda.get_device_properties(rb.device).multi_processor_count
+    times = {}
+    for g in sorted({rb.default_grid(), 2 * sms, 3 * sms, 4 * sms}):
+        rb.grid_blocks = g
+        times[g] = _time(lambda: rb.rollout(steps))
+    rb.grid_blocks = min(times, key=times.get)
+    return rb.grid_blocks, times
+
+
 def best_burgers(n, rows, scheme, device) -> int:
     """Cached cells-per-lane for this problem, or 0 (library default)."""
     with _lock:

@@ -52,7 +52,17 @@ class RaggedBurgers:
         d.nu_rows, d.dt_rows, d.dx_rows = self.nu.data_ptr(), self.dt.data_ptr(), self.dx.data_ptr()
         d.order = self.order.data_ptr()
         self.desc = d
-        self.grid_blocks = int(grid_blocks)
+        self.grid_blocks = int(grid_blocks) or self.default_grid()
+
+    def default_grid(self) -> int:
+        """Blocks of the persistent launch: about (total cells / widest row) warps, so that a
+        warp's share of the work is about one widest row and the longest-first queue can even
+        out the tail, within 2 to 4 blocks of 4 warps per SM (more warps than that leave the
+        widest rows as the tail; fewer hide less latency)."""
+        sms = torch.cuda.get_device_properties(self.device).multi_processor_count
+        wpb = self.desc.warps_per_block or 4
+        blocks = int(round(self.total / max(self.ns) / wpb))
+        return max(2 * sms, min(4 * sms, blocks))
 
     def rollout(self, steps, u0=None, out=None):
         """All rows advanced `steps` steps; returns the packed final state."""
