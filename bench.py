@@ -640,6 +640,7 @@ def bench_diff(args, dev, world, which):
     ms = lambda t: sum(t) / len(t)  # noqa: E731
     times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop))
     extra = dict(clocks=clk.summary(), h2d=0, d2h=4, launches=None)
+    extra["checks"] = diff_checks(which, net, cfg, dev)
     if which == "burgers_diff":  # the fused corrector rollout against the FP32 FMA peak
         from inc_b200.roofline import burgers_cnn_flops_per_cell_step
         fpc = burgers_cnn_flops_per_cell_step(cfg["scheme"])
@@ -652,6 +653,102 @@ def bench_diff(args, dev, world, which):
     cfg = dict(name=which, B=B, N=N, steps=steps, scheme=cfg["scheme"],
                corrector=("PeriodicCNN1D(4x32ch,k5,GELU)" if which == "burgers_diff" else "FNO1D(4 layers,w64,16 modes)"))
     return cfg, cells, times, extra
+
+
+def diff_checks(which, net, cfg, dev, rows=4, fwd_steps=10, grad_steps=8, directions=4, h=1e-6):
+    """Accuracy of the differentiable workloads on a subset of rows, outside the timed region:
+    the forward error of `fwd_steps` corrected steps against the same loop in FP64 on the host
+    (the corrector in float64 torch, the oracle's step), and the gradient of a weighted sum of
+    `grad_steps` frames w.r.t. u0 and the network's parameters against FP64 central
+    differences (step h) along random directions."""
+    import copy
+    import numpy as np
+    import torch
+    from types import SimpleNamespace
+    from inc_b200.rollout import simulate_rollout
+    from inc_b200.solvers import BurgersSolverTorch, KSSolverTorch
+    from oracle import burgers as ob
+    from oracle import ks as oks
+
+    N = cfg["N"]
+    u0_np = np.asarray(cfg["u0"], dtype=np.float64)[:rows]
+    rng = np.random.default_rng(11)
+    net64 = copy.deepcopy(net).double().cpu()
+    params64 = list(net64.parameters())
+    if which == "burgers_diff":
+        p = ob.BurgersParams(resolution=N, L=cfg["L"], dt=cfg["dt"], nu=cfg["nu"])
+        step64 = ob.step_ssprk3 if cfg["scheme"] == "ssprk3" else ob.step_euler
+        L_dev = None
+
+        def mk():
+            return BurgersSolverTorch(SimpleNamespace(
+                resolution=N, dt=cfg["dt"], x=None, adaptive_CFL=None, L=cfg["L"], nu=cfg["nu"], device=dev,
+                convection_term="WENO", equation_type="viscosity", batch_size=rows, time_scheme=cfg["scheme"]))
+
+        def loop64(u, steps):
+            t, out = 0.0, []
+            for _ in range(steps):
+                sv = net64(torch.from_numpy(u)).detach().numpy()
+                u, t = step64(u, p, t, sv)
+                out.append(u)
+            return np.stack(out, 1)
+    else:
+        Ls = np.full(rows, float(cfg["L"]))
+        L_dev = torch.tensor(Ls, dtype=torch.float32, device=dev)
+        L_host = torch.tensor(Ls)
+
+        def mk():
+            return KSSolverTorch(SimpleNamespace(resolution=N, dt=cfg["dt"], device=dev, domain_size=L_dev,
+                                                 alpha=torch.zeros(rows, device=dev), time_scheme=cfg["scheme"]))
+
+        def loop64(u, steps):
+            out = []
+            for _ in range(steps):
+                sv = net64(torch.from_numpy(u), L_host).detach().numpy()
+                u = oks.step(u, Ls, cfg["dt"], cfg["scheme"], sv)
+                out.append(u)
+            return np.stack(out, 1)
+    # forward error
+    u0 = torch.tensor(u0_np, dtype=torch.float32, device=dev)
+    with torch.no_grad():
+        fr, _ = simulate_rollout(net, mk(), u0, fwd_steps, "INC", L_dev)
+    ref = loop64(u0_np, fwd_steps)
+    fwd_err = float(np.linalg.norm(fr.double().cpu().numpy() - ref) / np.linalg.norm(ref))
+    # gradient vs central differences
+    wgt = rng.standard_normal((rows, grad_steps, N))
+    u0g = torch.tensor(u0_np, dtype=torch.float32, device=dev, requires_grad=True)
+    net.zero_grad()
+    fr, _ = simulate_rollout(net, mk(), u0g, grad_steps, "INC", L_dev, checkpoint_every=4)
+    (fr * torch.tensor(wgt, dtype=torch.float32, device=dev)).sum().backward()
+    g_u = u0g.grad.double().cpu().numpy()
+    g_p = [q.grad.double().cpu().numpy() for q in net.parameters()]
+    net.zero_grad()
+
+    def loss64(u):
+        return float((loop64(u, grad_steps) * wgt).sum())
+    errs = []
+    with torch.no_grad():
+        for _ in range(directions):  # in u0
+            d = rng.standard_normal(u0_np.shape)
+            fd = (loss64(u0_np + h * d) - loss64(u0_np - h * d)) / (2 * h)
+            errs.append(abs(float((g_u * d).sum()) - fd) / max(abs(fd), 1e-12))
+        for _ in range(directions):  # in the parameters
+            ds = [rng.standard_normal(tuple(q.shape)) for q in params64]
+            base = [q.detach().clone() for q in params64]
+            vals = []
+            for sign in (1.0, -1.0):
+                for q, b, d in zip(params64, base, ds):
+                    q.copy_(b + sign * h * torch.from_numpy(d))
+                vals.append(loss64(u0_np))
+            for q, b in zip(params64, base):
+                q.copy_(b)
+            fd = (vals[0] - vals[1]) / (2 * h)
+            an = sum(float((g * d).sum()) for g, d in zip(g_p, ds))
+            errs.append(abs(an - fd) / max(abs(fd), 1e-12))
+    return {"rows": rows, "forward_steps": fwd_steps, "forward_rel_l2_vs_fp64": fwd_err,
+            "grad_steps": grad_steps, "fd_h": h, "fd_directions": {"u0": directions, "params": directions},
+            "grad_max_rel_err_vs_fp64_fd": max(errs),
+            "reference": "the same corrected loop in FP64 on the host: torch corrector in float64, oracle step"}
 
 
 # ----------------------------------------------------------------------------
@@ -736,6 +833,7 @@ def main():
                 "forward_only_is": ("fused corrector + solver kernel (inc_burgers_cnn_rollout)"
                                     if cfg["name"] == "burgers_diff" else "corrector in torch, solver step launches"),
                 "fused_inference_roofline": extra.get("fused_inference_roofline"),
+                "checks": extra.get("checks"),
                 "clocks": extra["clocks"]}), flush=True)
         if world > 1:
             torch.distributed.barrier()
