@@ -624,6 +624,11 @@ def bench_diff(args, dev, world, which):
     t_plain = event_time(lambda: train_step(None), args.steps)
     t_fwd = event_time(forward_only, args.steps)
     t_loop = event_time(forward_loop, args.steps)
+    # the evaluation loop replayed from one CUDA graph (inc_b200.graphs)
+    from inc_b200.graphs import GraphedRollout
+    gsolver = mk()
+    graphed = GraphedRollout(net, gsolver, u0, steps, domain_size=L)
+    t_gfwd = event_time(lambda: graphed(u0), args.steps)
     # the whole training step captured in one CUDA graph
     side = torch.cuda.Stream(dev)
     side.wait_stream(torch.cuda.current_stream(dev))
@@ -638,7 +643,8 @@ def bench_diff(args, dev, world, which):
     torch.cuda.synchronize()
     t_graph = event_time(graph.replay, args.steps)
     ms = lambda t: sum(t) / len(t)  # noqa: E731
-    times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop))
+    times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop),
+                 gfwd=ms(t_gfwd))
     extra = dict(clocks=clk.summary(), h2d=0, d2h=4, launches=None)
     extra["checks"] = diff_checks(which, net, cfg, dev)
     if which == "burgers_diff":  # the fused corrector rollout against the FP32 FMA peak
@@ -829,7 +835,8 @@ def main():
                 "eager": {"train_step_ckpt8": tot / (times["ckpt"] * 1e-3),
                           "train_step_no_ckpt": tot / (times["plain"] * 1e-3),
                           "forward_only": tot / (times["fwd"] * 1e-3),
-                          "forward_per_step_loop": tot / (times["loop"] * 1e-3)},
+                          "forward_per_step_loop": tot / (times["loop"] * 1e-3),
+                          "forward_graphed_loop": tot / (times["gfwd"] * 1e-3)},
                 "forward_only_is": ("fused corrector + solver kernel (inc_burgers_cnn_rollout)"
                                     if cfg["name"] == "burgers_diff" else "corrector in torch, solver step launches"),
                 "fused_inference_roofline": extra.get("fused_inference_roofline"),
