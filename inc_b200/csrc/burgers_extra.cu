@@ -142,7 +142,7 @@ __global__ void __launch_bounds__(1024) k_adaptive(AdaptArgs ad) {
 #pragma unroll
             for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
         }
-        m = group_max<32>(m);
+        m = group_max_nonneg<32>(m);
         if (lane == 0) red[warp] = m;
         __syncthreads();
         if (threadIdx.x == 0) {

@@ -226,7 +226,7 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
         float m = 0.f;
 #pragma unroll
         for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
-        const float alpha = group_max<TPR>(m);  // per-row max |u|, solver_1d.py:133
+        const float alpha = group_max_nonneg<TPR>(m);  // per-row max |u|, solver_1d.py:133
         weno_rhs<CPT>(w, alpha, nu * inv_dx2, inv_dx, r);
     } else {
         fdm_rhs<CPT>(w, nu * inv_dx2, inv_2dx, r);
@@ -299,14 +299,14 @@ INC_DEV void rhs_vjp(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], c
     const float v_l = shfl<TPR>(v[CPT - 1], left);
     const float nu = cx.nu;
     if (a.conv == INC_CONV_WENO) {
-        float m = -1.f;
-        int mi = 0;
+        float m = 0.f;  // as the forward's fmaxf: NaN cells are passed over
+        int mi = g * CPT;
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
             const float av = fabsf(u[c]);
             if (av > m) { m = av; mi = g * CPT + c; }
         }
-        group_argmax<TPR>(m, mi);
+        group_argmax_nonneg<TPR>(m, mi);
         const float alpha = m;
         float fp[CPT + 6], fm[CPT + 6];
 #pragma unroll
@@ -554,7 +554,7 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
     float m = 0.f;
 #pragma unroll
     for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
-    m = group_max<32>(m);
+    m = group_max_nonneg<32>(m);
     if ((g & 31) == 0) sh.wmax[parity][g >> 5] = m;
     __syncthreads();
     float w[CPT + 6];

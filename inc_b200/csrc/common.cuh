@@ -54,6 +54,32 @@ INC_DEV void group_argmax(float& v, int& idx) {
     }
 }
 
+// Lanes of this thread's group of W consecutive lanes.
+template <int W>
+INC_DEV unsigned group_mask() {
+    if constexpr (W == 32) return 0xffffffffu;
+    else return ((1u << W) - 1u) << ((threadIdx.x & 31) & ~(W - 1));
+}
+
+// Max over a group of non-negative values (|u|) in one redux.sync on the bit
+// patterns, which order like the values for non-negative floats.  A NaN is
+// larger than every finite pattern, so it wins, as in torch.max.
+template <int W>
+INC_DEV float group_max_nonneg(float v) {
+    return __uint_as_float(__reduce_max_sync(group_mask<W>(), __float_as_uint(v)));
+}
+
+// group_argmax for non-negative values: the max by redux.sync, then the lowest
+// lane holding it (lanes own consecutive cells, so the lowest lane holds the
+// first index; torch.max(dim) returns the first occurrence on the CPU).
+template <int W>
+INC_DEV void group_argmax_nonneg(float& v, int& idx) {
+    const unsigned best = __reduce_max_sync(group_mask<W>(), __float_as_uint(v));
+    const unsigned hit = __ballot_sync(0xffffffffu, __float_as_uint(v) == best) & group_mask<W>();
+    idx = __shfl_sync(0xffffffffu, idx, __ffs(hit) - 1);
+    v = __uint_as_float(best);
+}
+
 // ---- vector memory helpers ---------------------------------------------------
 template <int C>
 INC_DEV void load_row_chunk(float (&r)[C], const float* __restrict__ p, bool valid) {
