@@ -27,6 +27,7 @@ scaling, trajectories are independent, no data-path collective).
 from __future__ import annotations
 
 import argparse
+import copy
 import json
 import math
 import os
@@ -51,7 +52,7 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--profile", nargs="?", const="ks", default=None,
-                    choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd", "burgers_cnn"],
+                    choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd", "burgers_cnn", "spectral_conv"],
                     help="a small case of one kernel for ncu (no JSON)")
     ap.add_argument("--profile-rows", type=int, default=1024, help="rows of the KS profile case")
     ap.add_argument("--tpp", type=int, default=None,
@@ -584,6 +585,9 @@ def bench_diff(args, dev, world, which):
     with torch.no_grad():  # target: the uncorrected solver's trajectory
         target, _ = simulate_rollout(None, mk(), u0, steps, None, L)
         target = target + 0.01 * torch.randn_like(target)
+    # the accuracy checks run on the seeded network as built: after the timed Adam steps its
+    # state would depend on the signs of near-zero gradients, i.e. on FP32 rounding
+    net_at_init = copy.deepcopy(net)
     opt = torch.optim.Adam(net.parameters(), lr=1e-4, capturable=True)
 
     solver = mk()  # built once: a KS plan uploads its pairing (a host sync) when first used
@@ -646,7 +650,7 @@ def bench_diff(args, dev, world, which):
     times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop),
                  gfwd=ms(t_gfwd))
     extra = dict(clocks=clk.summary(), h2d=0, d2h=4, launches=None)
-    extra["checks"] = diff_checks(which, net, cfg, dev)
+    extra["checks"] = diff_checks(which, net_at_init, cfg, dev)
     if which == "burgers_diff":  # the fused corrector rollout against the FP32 FMA peak
         from inc_b200.roofline import burgers_cnn_flops_per_cell_step
         fpc = burgers_cnn_flops_per_cell_step(cfg["scheme"])
@@ -732,12 +736,12 @@ def diff_checks(which, net, cfg, dev, rows=4, fwd_steps=10, grad_steps=8, direct
 
     def loss64(u):
         return float((loop64(u, grad_steps) * wgt).sum())
-    errs = []
+    errs_u, errs = [], []
     with torch.no_grad():
         for _ in range(directions):  # in u0
             d = rng.standard_normal(u0_np.shape)
             fd = (loss64(u0_np + h * d) - loss64(u0_np - h * d)) / (2 * h)
-            errs.append(abs(float((g_u * d).sum()) - fd) / max(abs(fd), 1e-12))
+            errs_u.append(abs(float((g_u * d).sum()) - fd) / max(abs(fd), 1e-12))
         for _ in range(directions):  # in the parameters
             ds = [rng.standard_normal(tuple(q.shape)) for q in params64]
             base = [q.detach().clone() for q in params64]
@@ -753,7 +757,9 @@ def diff_checks(which, net, cfg, dev, rows=4, fwd_steps=10, grad_steps=8, direct
             errs.append(abs(an - fd) / max(abs(fd), 1e-12))
     return {"rows": rows, "forward_steps": fwd_steps, "forward_rel_l2_vs_fp64": fwd_err,
             "grad_steps": grad_steps, "fd_h": h, "fd_directions": {"u0": directions, "params": directions},
-            "grad_max_rel_err_vs_fp64_fd": max(errs),
+            "grad_max_rel_err_vs_fp64_fd": max(errs_u + errs),
+            "grad_max_rel_err_u0": max(errs_u), "grad_max_rel_err_params": max(errs),
+            "network": "the seeded network before the timed training steps",
             "reference": "the same corrected loop in FP64 on the host: torch corrector in float64, oracle step"}
 
 
@@ -908,8 +914,8 @@ def main():
 
 def profile_small(dev, which="ks", rows=1024, tpp=32):
     """Small cases for ncu captures: the KS fused rollout (rows x 256, 64 steps, `tpp` threads
-    per row pair) and its backward, the ragged Burgers batch (rows of n in {64..512}, 20 steps)
-    or the 32x128 Burgers rollout."""
+    per row pair) and its backward, the ragged Burgers batch (rows of n in {64..512}, 20 steps),
+    the 32x128 Burgers rollout, the fused CNN rollout, or one FNO spectral layer (512 x 64 x 512)."""
     import torch
     from types import SimpleNamespace
     if which == "burgers_ragged":
@@ -936,6 +942,20 @@ def profile_small(dev, which="ks", rows=1024, tpp=32):
         for _ in range(2):
             f, c = burgers_cnn_rollout(net, solver, u0, 32, ckpt_every=8)
             (f.square().mean() + c.square().mean()).backward()
+        torch.cuda.synchronize()
+        return
+    if which == "spectral_conv":  # one FNO layer sum, forward and backward, at the KS FNO's shape
+        from inc_b200.correctors import spectral_conv1d
+        B, W, N, M = 512, 64, 512, 16
+        g = torch.Generator(device=dev).manual_seed(0)
+        x = torch.randn(B, W, N, device=dev, generator=g, requires_grad=True)
+        add = torch.randn(B, W, N, device=dev, generator=g, requires_grad=True)
+        w_re = (torch.rand(W, W, M, device=dev, generator=g) / (W * W)).requires_grad_(True)
+        w_im = (torch.rand(W, W, M, device=dev, generator=g) / (W * W)).requires_grad_(True)
+        bias = torch.randn(W, device=dev, generator=g, requires_grad=True)
+        gy = torch.randn(B, W, N, device=dev, generator=g)
+        for _ in range(2):
+            spectral_conv1d(x, w_re, w_im, M, bias=bias, addend=add).backward(gy)
         torch.cuda.synchronize()
         return
     if which == "burgers_plain":

@@ -1,6 +1,5 @@
 """Corrector networks s(u) for the hybrid rollouts (torch modules).
 
-The corrector stays in torch; the solver step around it is the CUDA path.
 Two architectures from the benchmark configurations:
 
 * ``PeriodicCNN1D`` - 4 circular Conv1d layers (32 channels, kernel 5) with
@@ -11,12 +10,21 @@ Two architectures from the benchmark configurations:
   layers, project with two linear layers.  ``forward(u, L)`` takes the
   per-trajectory domain size like the reference's FNO corrector
   (models/models_1d/fno.py:39-105) does.
+
+On CUDA tensors the FNO's spectral convolution runs as one kernel per call
+(``inc_spectral_conv1d``: the row-pair FFTs, the mode mixing and the inverse
+FFTs of one trajectory in one CTA) with a hand-written adjoint; the other
+layers are torch (cuBLAS matmuls, cuDNN convolutions).  Shapes the kernel does
+not cover, and CPU tensors, take the torch FFT path.  The CNN runs inside the
+Burgers solver kernel when ``simulate_rollout`` can fuse it (``fused.py``).
 """
 from __future__ import annotations
 
 import torch
 import torch.nn as nn
 import torch.nn.functional as F
+
+from . import _native as nat
 
 
 class PeriodicCNN1D(nn.Module):
@@ -36,6 +44,111 @@ class PeriodicCNN1D(nn.Module):
         return x.squeeze(1)
 
 
+SPECTRAL_CONV_N = (16, 32, 64, 128, 256, 512)
+
+
+def spectral_conv1d_torch(x, w_re, w_im, modes: int):
+    """SpectralConv1d.forward with torch FFTs (models/models_1d/fno.py:26-37):
+    rfft, the lowest `modes` modes times complex [cin][cout][modes] weights,
+    irfft back to x's length."""
+    n = x.shape[-1]
+    xf = torch.fft.rfft(x)
+    m = min(modes, xf.shape[-1])
+    w = torch.complex(w_re[..., :m], w_im[..., :m])
+    out = torch.zeros(x.shape[0], w.shape[1], xf.shape[-1], dtype=xf.dtype, device=x.device)
+    out[..., :m] = torch.einsum("bim,iom->bom", xf[..., :m], w)
+    return torch.fft.irfft(out, n=n)
+
+
+def spectral_conv_supported(x, w_re, w_im, modes: int) -> bool:
+    """True when ``inc_spectral_conv1d`` computes this call: FP32 CUDA tensors,
+    x [B, W, n] with n a power of two in [16, 512], square weights of even width
+    <= 128, 1 <= modes <= min(32, n / 2)."""
+    if not (isinstance(x, torch.Tensor) and x.is_cuda and x.dim() == 3 and x.dtype == torch.float32):
+        return False
+    B, W, n = x.shape
+    return (w_re.dtype == torch.float32 and w_im.dtype == torch.float32 and w_re.is_cuda
+            and tuple(w_re.shape[:2]) == (W, W) and w_im.shape == w_re.shape and W % 2 == 0 and W <= 128
+            and n in SPECTRAL_CONV_N and 1 <= modes <= min(32, n // 2, w_re.shape[-1]) and B > 0)
+
+
+def _spectral_work(B: int, W: int, modes: int, device):
+    """Scratch of inc_spectral_conv1d: the mixed modes and the mode-major weights."""
+    return torch.empty(2 * modes * W * (B + W), device=device, dtype=torch.float32)
+
+
+class SpectralConv1dFn(torch.autograd.Function):
+    """``inc_spectral_conv1d`` forward (with the optional bias and addend of the
+    layer sum); ``inc_spectral_conv1d_bwd`` for the input gradient.  The weight
+    gradient is sum_b dL/dout[b][o][k] conj(rfft(x)[b][c][k]) as one complex
+    batched matmul over the modes; the bias gradient, sum over b and n of dL/dy,
+    is n times the real part of the backward's DC coefficient summed over b."""
+
+    @staticmethod
+    def forward(ctx, x, w_re, w_im, bias, addend, modes: int):
+        x = x.contiguous()
+        wr = w_re[..., :modes].contiguous()
+        wi = w_im[..., :modes].contiguous()
+        B, W, n = x.shape
+        if addend is not None:
+            addend = addend.contiguous()
+        y = torch.empty_like(x)
+        need_w = ctx.needs_input_grad[1] or ctx.needs_input_grad[2]
+        xm = torch.empty(B, W, modes, 2, device=x.device, dtype=torch.float32)  # rfft(x) modes
+        work = _spectral_work(B, W, modes, x.device)
+        rc = nat.lib().inc_spectral_conv1d(x.data_ptr(), wr.data_ptr(), wi.data_ptr(), nat.ptr(bias),
+                                           nat.ptr(addend), y.data_ptr(), xm.data_ptr(), work.data_ptr(),
+                                           B, W, n, modes, nat.stream_of(x.device))
+        nat.check(rc, "inc_spectral_conv1d")
+        ctx.save_for_backward(wr, wi, xm if need_w else None)
+        ctx.modes, ctx.full_modes = modes, w_re.shape[-1]
+        ctx.has_bias, ctx.has_addend = bias is not None, addend is not None
+        return y
+
+    @staticmethod
+    def backward(ctx, gy):
+        wr, wi, xm = ctx.saved_tensors
+        gy = gy.contiguous()
+        B, W, n = gy.shape
+        m = ctx.modes
+        need_w = ctx.needs_input_grad[1] or ctx.needs_input_grad[2]
+        need_b = ctx.has_bias and ctx.needs_input_grad[3]
+        gx = torch.empty_like(gy)
+        gm = torch.empty(B, W, m, 2, device=gy.device, dtype=torch.float32)  # dL/dF modes
+        work = _spectral_work(B, W, m, gy.device)
+        rc = nat.lib().inc_spectral_conv1d_bwd(gy.data_ptr(), wr.data_ptr(), wi.data_ptr(), gx.data_ptr(),
+                                               gm.data_ptr(), work.data_ptr(), B, W, n, m,
+                                               nat.stream_of(gy.device))
+        nat.check(rc, "inc_spectral_conv1d_bwd")
+        gw_re = gw_im = g_bias = None
+        if need_w:
+            gw = torch.einsum("bok,bck->cok", torch.view_as_complex(gm), torch.view_as_complex(xm).conj())
+            gw_re = gw.real.new_zeros(W, W, ctx.full_modes)
+            gw_im = torch.zeros_like(gw_re)
+            gw_re[..., :m] = gw.real
+            gw_im[..., :m] = gw.imag
+        if need_b:
+            g_bias = gm[:, :, 0, 0].sum(0) * n
+        g_add = gy if (ctx.has_addend and ctx.needs_input_grad[4]) else None
+        return (gx if ctx.needs_input_grad[0] else None), gw_re, gw_im, g_bias, g_add, None
+
+
+def spectral_conv1d(x, w_re, w_im, modes: int, bias=None, addend=None):
+    """SpectralConv1d.forward, plus bias[:, None] and addend where given (the FNO
+    layer's sum with its 1x1 convolution): the CUDA kernel where it applies,
+    else torch FFTs."""
+    m = min(modes, x.shape[-1] // 2 + 1)
+    if spectral_conv_supported(x, w_re, w_im, m) and (bias is None or (bias.is_cuda and bias.dtype == torch.float32 and bias.shape == x.shape[1:2])) \
+            and (addend is None or (addend.shape == x.shape and addend.dtype == torch.float32 and addend.is_cuda)):
+        return SpectralConv1dFn.apply(x, w_re, w_im, bias, addend, m)
+    y = spectral_conv1d_torch(x, w_re, w_im, modes)
+    if bias is not None:
+        y = y + bias[:, None]
+    if addend is not None:
+        y = y + addend
+    return y
+
+
 class SpectralConv1d(nn.Module):
     """Multiply the lowest `modes` rFFT modes by learned complex in x out matrices."""
 
@@ -47,20 +160,23 @@ class SpectralConv1d(nn.Module):
         self.w_im = nn.Parameter(scale * torch.rand(cin, cout, modes))
 
     def forward(self, x):
-        n = x.shape[-1]
-        xf = torch.fft.rfft(x)
-        m = min(self.modes, xf.shape[-1])
-        w = torch.complex(self.w_re[..., :m], self.w_im[..., :m])
-        out = torch.zeros(x.shape[0], w.shape[1], xf.shape[-1], dtype=xf.dtype, device=x.device)
-        out[..., :m] = torch.einsum("bim,iom->bom", xf[..., :m], w)
-        return torch.fft.irfft(out, n=n)
+        return spectral_conv1d(x, self.w_re, self.w_im, self.modes)
 
 
-def _pointwise(conv: nn.Conv1d, x):
-    """A kernel-size-1 Conv1d as a channel matmul (same parameters and result):
-    cuDNN's FP32 weight gradient for 1x1 convolutions is a slow direct kernel,
-    while the matmul's runs on cuBLAS."""
-    return torch.matmul(conv.weight[:, :, 0], x) + conv.bias[:, None]
+def _channel_mm(w, x):
+    """w [out, in] applied to every trajectory of x [B, in, n] -> [B, out, n] as
+    one batched matmul.  (torch.matmul of a 2-D by a 3-D operand folds the batch
+    into the columns, which transposes x and the result through copies, and
+    makes the weight gradient one GEMM with K = B * n and a tiny output tile;
+    the batched form needs neither.)  The FNO's kernel-size-1 Conv1d layers run
+    as this product too (same parameters and result): cuDNN's FP32 weight
+    gradient for 1x1 convolutions is a slow direct kernel."""
+    return torch.bmm(w.expand(x.shape[0], -1, -1), x)
+
+
+def _channel_linear(lin: nn.Linear, x):
+    """nn.Linear over the channel axis of x [B, in, n] -> [B, out, n]."""
+    return _channel_mm(lin.weight, x) + lin.bias[:, None]
 
 
 class FNO1D(nn.Module):
@@ -81,10 +197,16 @@ class FNO1D(nn.Module):
             grid = L.reshape(B, 1).to(u.dtype) * base
         else:
             grid = float(L) * base.expand(B, n)
-        x = self.lift(torch.stack([u, grid], dim=-1)).permute(0, 2, 1)
+        # The hidden state stays [B, width, n] (contiguous) from the lift to the
+        # projection: the Linear layers act on the channel axis as channel matmuls
+        # (same parameters, same result), so no permuted view reaches an
+        # elementwise kernel or a gradient.
+        x = _channel_linear(self.lift, torch.stack([u, grid], dim=1))
         for i, (sc, pw) in enumerate(zip(self.spectral, self.pointwise)):
-            x = sc(x) + _pointwise(pw, x)
+            # sc(x) + pw(x) with pw's bias and product added in the spectral kernel's epilogue
+            x = spectral_conv1d(x, sc.w_re, sc.w_im, sc.modes, bias=pw.bias,
+                                addend=_channel_mm(pw.weight[:, :, 0], x))
             if i + 1 < len(self.spectral):
                 x = F.gelu(x)
-        x = F.gelu(self.proj1(x.permute(0, 2, 1)))
-        return self.proj2(x).squeeze(-1)
+        x = F.gelu(_channel_linear(self.proj1, x))
+        return _channel_linear(self.proj2, x).squeeze(1)

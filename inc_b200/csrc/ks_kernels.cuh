@@ -340,6 +340,47 @@ INC_DEV void load_lane_twiddles(Twiddles<P, T>& tw, const float2* table, int t) 
     }
 }
 
+// The same lane twiddles computed in FP64 on the device (kernels without a plan).
+template <int P, int T>
+INC_DEV void compute_lane_twiddles(Twiddles<P, T>& tw, int t) {
+    static_assert(twiddles_in_registers<P, T>(), "shapes with lane twiddles in registers");
+    constexpr int N = P * T;
+    int i = 0;
+#pragma unroll
+    for (int ns = P; ns < N; ns *= pass_radix(P, T, ns)) {
+        const int R = pass_radix(P, T, ns), Q = P / R;
+#pragma unroll
+        for (int q = 0; q < Q; ++q)
+#pragma unroll
+            for (int r = 1; r < R; ++r) {
+                const int k = (t + T * q) % ns;
+                double sn, cs;
+                sincospi(-2.0 * (double)(r * k) / (double)(ns * R), &sn, &cs);
+                tw.reg[i++] = make_float2((float)cs, (float)sn);
+            }
+    }
+}
+
+// The later passes' twiddle table (entry pi*N + (q*R + r)*T + t =
+// exp(-2 pi i r k / (NS R)), k = (t + T q) % NS) computed in FP64 by the block
+// into shared memory, for kernels without a plan whose shape does not keep
+// the lane twiddles in registers.  The caller synchronises before use.
+template <int P, int T>
+INC_DEV void fill_twiddle_table(float2* table) {
+    constexpr int N = P * T;
+    int pi = 0;
+    for (int ns = P; ns < N; ns *= pass_radix(P, T, ns), ++pi) {
+        const int R = pass_radix(P, T, ns), Q = P / R;
+        for (int i = threadIdx.x; i < Q * R * T; i += blockDim.x) {
+            const int t = i % T, r = (i / T) % R, q = i / (T * R);
+            const int k = (t + T * q) % ns;
+            double sn, cs;
+            sincospi(-2.0 * (double)(r * k) / (double)(ns * R), &sn, &cs);
+            table[pi * N + i] = make_float2((float)cs, (float)sn);
+        }
+    }
+}
+
 template <int P, int T, int NS>
 INC_DEV void fft_later(float2 (&v)[P], const Buf<P, T>& buf, const Twiddles<P, T>& tw, int t) {
     constexpr int N = P * T;

@@ -9,26 +9,6 @@ namespace inc {
 namespace ks {
 
 template <int P, int T>
-INC_DEV void compute_lane_twiddles(Twiddles<P, T>& tw, int t) {
-    static_assert(twiddles_in_registers<P, T>(), "spectrum shapes keep twiddles in registers");
-    constexpr int N = P * T;
-    int i = 0;
-#pragma unroll
-    for (int ns = P; ns < N; ns *= pass_radix(P, T, ns)) {
-        const int R = pass_radix(P, T, ns), Q = P / R;
-#pragma unroll
-        for (int q = 0; q < Q; ++q)
-#pragma unroll
-            for (int r = 1; r < R; ++r) {
-                const int k = (t + T * q) % ns;
-                double sn, cs;
-                sincospi(-2.0 * (double)(r * k) / (double)(ns * R), &sn, &cs);
-                tw.reg[i++] = make_float2((float)cs, (float)sn);
-            }
-    }
-}
-
-template <int P, int T>
 __global__ void __launch_bounds__(128) k_spectrum(const float* __restrict__ v, float* __restrict__ out, int rows) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;

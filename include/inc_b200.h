@@ -252,6 +252,33 @@ int inc_ks_rollout_bwd(const inc_ks_plan* plan, const float* ckpts, const float*
  * which the reference runs on the CPU after a rollout.                        */
 int inc_energy_spectrum(const float* u, float* out, int32_t rows, int32_t n, void* stream);
 
+/* ---- corrector: FNO spectral convolution ----------------------------------- */
+/* y[b][o] = irfft(sum_c rfft(x[b][c])[k] * (w_re + i w_im)[c][o][k] for
+ * k < modes, zero above), n points, plus bias[o] and addend[b][o][n] where
+ * those are not NULL.  Replaces SpectralConv1d.forward
+ * (models/models_1d/fno.py:26-37: rfft, compl_mul1d einsum, irfft) for
+ * in_channels == out_channels == width, and with bias and addend the sum of
+ * an FNO layer's two branches (fno.py:86-88: conv(x) + w(x), the 1x1
+ * convolution's bias and product passed in).  x, y, addend [batch][width][n];
+ * w_re, w_im [width][width][modes]; bias [width].  x_modes receives
+ * rfft(x)[..., :modes] as complex pairs [batch][width][modes][2] (the weight
+ * gradient's input); work is scratch of 2 * modes * width * (batch + width)
+ * floats, 16-byte aligned.  n a power of two in [16, 512]; width even,
+ * <= 128; 1 <= modes <= min(32, n/2).  Returns INC_E_UNSUPPORTED outside
+ * those.                                                                     */
+int inc_spectral_conv1d(const float* x, const float* w_re, const float* w_im, const float* bias,
+                        const float* addend, float* y, float* x_modes, float* work, int32_t batch,
+                        int32_t width, int32_t n, int32_t modes, void* stream);
+/* Adjoint w.r.t. x: g_x = d<g_y, y>/dx (what autograd gives through
+ * SpectralConv1d.forward).  g_modes receives the gradient of the mixed modes
+ * out_ft[..., :modes] [batch][width][modes][2] (irfft's adjoint: 2/n
+ * rfft(g_y), 1/n at k = 0 with the imaginary part dropped); the weight
+ * gradient is then sum_b g_modes[b][o][k] * conj(x_modes[b][c][k]), and the
+ * bias gradient n * sum_b Re g_modes[b][o][0].  work as for the forward.     */
+int inc_spectral_conv1d_bwd(const float* g_y, const float* w_re, const float* w_im, float* g_x,
+                            float* g_modes, float* work, int32_t batch, int32_t width, int32_t n,
+                            int32_t modes, void* stream);
+
 /* ---- measurement utility ------------------------------------------------ */
 /* FP32 FMA throughput probe used by bench.py for the roofline denominator:
  * `blocks` x 256 threads, each 128 * iters FMAs (2 flops each) in 8

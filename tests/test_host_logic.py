@@ -154,3 +154,14 @@ def test_cnn_weight_packing_layout():
         raise AssertionError("expected ValueError")
     except ValueError:
         pass
+
+
+def test_spectral_conv_dispatch_on_cpu():
+    """CPU tensors never reach inc_spectral_conv1d; the layer is the torch FFT formulation there."""
+    import torch
+    from inc_b200.correctors import SpectralConv1d, spectral_conv1d_torch, spectral_conv_supported
+    torch.manual_seed(0)
+    layer = SpectralConv1d(8, 8, 4)
+    x = torch.randn(3, 8, 32)
+    assert not spectral_conv_supported(x, layer.w_re, layer.w_im, 4)
+    torch.testing.assert_close(layer(x), spectral_conv1d_torch(x, layer.w_re, layer.w_im, 4), rtol=0, atol=0)
