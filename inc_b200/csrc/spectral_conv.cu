@@ -316,17 +316,23 @@ void sc_allow_smem(K kernel, size_t smem) {
     if (smem > 48 * 1024) cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
 }
 
-// Grid of the streaming kernels: every SM's resident blocks, at most one block
-// per SC_BLOCK / T pairs.
+// Resident blocks of a streaming kernel on the whole device (SM count times
+// blocks per SM), queried once per kernel instance: the smem size is fixed per
+// instance and the devices of a process are alike.
 template <typename K>
-int sc_grid(K kernel, size_t smem, int npairs, int G) {
+int sc_resident(K kernel, size_t smem) {
     int dev = 0, sms = 148, per_sm = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, SC_BLOCK, smem);
+    return sms * (per_sm > 0 ? per_sm : 1);
+}
+
+// Grid of the streaming kernels: every SM's resident blocks, at most one block
+// per SC_BLOCK / T pairs.
+inline int sc_grid(int resident, int npairs, int G) {
     const int want = (npairs + G - 1) / G;
-    const int cap = sms * (per_sm > 0 ? per_sm : 1);
-    return want < cap ? want : cap;
+    return want < resident ? want : resident;
 }
 
 template <int P, int T, bool BWD>
@@ -338,7 +344,10 @@ int run_spectral_conv(const float* in, float* out, const float* w_re, const floa
     const size_t fsm = sc_fft_smem<P, T>();
     sc_allow_smem(k_sc_modes<P, T, BWD>, fsm);
     sc_allow_smem(k_sc_inverse<P, T>, fsm);
-    const int g1 = sc_grid(k_sc_modes<P, T, BWD>, fsm, npairs, G);
+    // (after the smem opt-in, which the occupancy query depends on)
+    static const int res1 = sc_resident(k_sc_modes<P, T, BWD>, fsm);
+    static const int res3 = sc_resident(k_sc_inverse<P, T>, fsm);
+    const int g1 = sc_grid(res1, npairs, G);
     k_sc_modes<P, T, BWD><<<g1, SC_BLOCK, fsm, st>>>(in, modes, npairs, M);
     float2* wt = mixed + (int64_t)batch * W * M;
     k_sc_weights<BWD><<<(W * W * M + SC_BLOCK - 1) / SC_BLOCK, SC_BLOCK, 0, st>>>(w_re, w_im, wt, W, M);
@@ -346,7 +355,7 @@ int run_spectral_conv(const float* in, float* out, const float* w_re, const floa
     sc_allow_smem(k_sc_mix<BWD>, msm);
     const dim3 g2(M, (batch + MIX_TB - 1) / MIX_TB);
     k_sc_mix<BWD><<<g2, SC_BLOCK, msm, st>>>(modes, wt, mixed, batch, W, M, 1.f / (float)N);
-    const int g3 = sc_grid(k_sc_inverse<P, T>, fsm, npairs, G);
+    const int g3 = sc_grid(res3, npairs, G);
     k_sc_inverse<P, T><<<g3, SC_BLOCK, fsm, st>>>(mixed, out, BWD ? nullptr : bias, BWD ? nullptr : addend, npairs,
                                                   W, M);
     return check_launch("spectral_conv");
