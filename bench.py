@@ -646,11 +646,29 @@ def bench_diff(args, dev, world, which):
     graph.replay()
     torch.cuda.synchronize()
     t_graph = event_time(graph.replay, args.steps)
+    # end to end through the public API: every step's u0 and target come from pinned host
+    # memory, the loss goes back to pinned host memory; the eager step (simulate_rollout,
+    # backward, Adam)
+    u0_host = u0.detach().cpu().pin_memory()
+    tgt_host = target.detach().cpu().pin_memory()
+    loss_host = torch.empty((), dtype=torch.float32).pin_memory()
+
+    def e2e_step():
+        u0.copy_(u0_host, non_blocking=True)
+        target.copy_(tgt_host, non_blocking=True)
+        loss_host.copy_(train_step(8).detach(), non_blocking=True)
+
+    e2e_step()
+    torch.cuda.synchronize()
+    t_e2e = event_time(e2e_step, args.steps)
+    launches = count_own_launches(lambda: train_step(8)) * args.steps
     ms = lambda t: sum(t) / len(t)  # noqa: E731
-    times = dict(fused=ms(t_graph), e2e=ms(t_ck), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop),
+    times = dict(fused=ms(t_graph), e2e=ms(t_e2e), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop),
                  gfwd=ms(t_gfwd))
-    extra = dict(clocks=clk.summary(), h2d=0, d2h=4, launches=None)
+    extra = dict(clocks=clk.summary(), h2d=(u0.numel() + target.numel()) * 4, d2h=4, launches=launches)
     extra["checks"] = diff_checks(which, net_at_init, cfg, dev)
+    if which == "ks_diff":  # the FNO's spectral convolution layer against the HBM peak
+        extra["roofline"] = spectral_layer_roofline(dev, B, N)
     if which == "burgers_diff":  # the fused corrector rollout against the FP32 FMA peak
         from inc_b200.roofline import burgers_cnn_flops_per_cell_step
         fpc = burgers_cnn_flops_per_cell_step(cfg["scheme"])
@@ -658,11 +676,77 @@ def bench_diff(args, dev, world, which):
         peak = fp32_peak_tflops(dev)
         extra["fused_inference_roofline"] = {
             "kernel": "inc_burgers_cnn_rollout (k_cnn_rollout<256>)", "bound": "fp32", "achieved": achieved,
-            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "flops_per_cell_step": fpc,
+            "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "flops_per_cell_step": fpc,
             "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run"}
     cfg = dict(name=which, B=B, N=N, steps=steps, scheme=cfg["scheme"],
                corrector=("PeriodicCNN1D(4x32ch,k5,GELU)" if which == "burgers_diff" else "FNO1D(4 layers,w64,16 modes)"))
     return cfg, cells, times, extra
+
+
+def count_own_launches(fn):
+    """Kernels of libinc_b200 that one call of fn launches (torch profiler, outside any timed region)."""
+    import torch
+    from torch.profiler import ProfilerActivity, profile
+    torch.cuda.synchronize()
+    with profile(activities=[ProfilerActivity.CUDA]) as prof:
+        fn()
+        torch.cuda.synchronize()
+    return sum(1 for e in prof.events()
+               if e.device_type.name == "CUDA" and (e.name.startswith("void inc::") or e.name.startswith("inc::")))
+
+
+def hbm_peak_gbs():
+    """(HBM GB/s, source): the driver-measured copy bandwidth when MEASURED_PEAKS.json holds it, else the
+    pool's earlier measurement."""
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            v = float(json.load(f)["hbm_gbs"])
+        return v, "measured (MEASURED_PEAKS.json hbm_gbs)"
+    except (OSError, KeyError, ValueError, TypeError):
+        return 6650.0, "fallback (6.65 TB/s, an earlier copy-bandwidth measurement on this pool)"
+
+
+def spectral_layer_roofline(dev, B, N, W=64, M=16):
+    """One FNO layer's spectral(x) + bias + 1x1 branch (inc_spectral_conv1d) at the workload's shape,
+    timed alone, against the HBM peak.  Algorithmic bytes: x, addend and y (12 B per point), the rfft
+    modes and the mixed modes each written and read (32 B per mode), the weights read, relaid and
+    read (24 B per weight entry).  Inputs exceed L2 (192 MB of activations); the calls are replayed from
+    a CUDA graph so that the time is the device's."""
+    import torch
+    from inc_b200.correctors import spectral_conv1d
+    g = torch.Generator(device=dev).manual_seed(0)
+    x = torch.randn(B, W, N, device=dev, generator=g)
+    add = torch.randn(B, W, N, device=dev, generator=g)
+    wr = torch.rand(W, W, M, device=dev, generator=g) / (W * W)
+    wi = torch.rand(W, W, M, device=dev, generator=g) / (W * W)
+    bias = torch.randn(W, device=dev, generator=g)
+    reps = 10  # layer calls per graph replay: device time without the host's per-call work
+    with torch.no_grad():
+        side = torch.cuda.Stream(dev)
+        side.wait_stream(torch.cuda.current_stream(dev))
+        with torch.cuda.stream(side):
+            for _ in range(3):
+                spectral_conv1d(x, wr, wi, M, bias=bias, addend=add)
+        torch.cuda.current_stream(dev).wait_stream(side)
+        graph = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(graph):
+            for _ in range(reps):
+                spectral_conv1d(x, wr, wi, M, bias=bias, addend=add)
+        graph.replay()
+        torch.cuda.synchronize()
+        t = event_time(graph.replay, 10)
+    ms = sum(t) / len(t) / reps
+    nbytes = 12 * B * W * N + 32 * B * W * M + 24 * W * W * M
+    achieved = nbytes / (ms * 1e-3) / 1e9
+    peak, src = hbm_peak_gbs()
+    # ncu dram__bytes_read.sum + dram__bytes_write.sum of the four kernels at this shape
+    # (profiles/fno_spectral_conv_b512_w64_n512_full.md); outputs still in L2 at the end of a
+    # launch are not counted there
+    traffic = 167.8e6 if (B, N, W, M) == (512, 512, 64, 16) else None
+    return {"kernel": "FNO spectral conv layer forward: k_sc_modes, k_sc_weights, k_sc_mix, k_sc_inverse",
+            "bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": traffic, "bytes_per_launch": nbytes, "ms_per_launch": ms, "peak_source": src}
 
 
 def diff_checks(which, net, cfg, dev, rows=4, fwd_steps=10, grad_steps=8, directions=4, h=1e-6):
@@ -845,9 +929,14 @@ def main():
                           "forward_graphed_loop": tot / (times["gfwd"] * 1e-3)},
                 "forward_only_is": ("fused corrector + solver kernel (inc_burgers_cnn_rollout)"
                                     if cfg["name"] == "burgers_diff" else "corrector in torch, solver step launches"),
+                "e2e": {"value": tot / (times["e2e"] * 1e-3), "unit": "cell-steps/s",
+                        "h2d_bytes_per_step": extra["h2d"], "d2h_bytes_per_step": extra["d2h"],
+                        "api": "eager training step: simulate_rollout, loss.backward(), Adam"},
+                "roofline": extra.get("roofline") or extra.get("fused_inference_roofline"),
                 "fused_inference_roofline": extra.get("fused_inference_roofline"),
                 "checks": extra.get("checks"),
-                "clocks": extra["clocks"]}), flush=True)
+                "clocks": extra["clocks"],
+                "gpu_launches": extra["launches"]}), flush=True)
         if world > 1:
             torch.distributed.barrier()
             torch.distributed.destroy_process_group()
