@@ -558,14 +558,18 @@ def bench_diff(args, dev, world, which):
     from inc_b200.correctors import FNO1D, PeriodicCNN1D
     from inc_b200.rollout import simulate_rollout
     from inc_b200.solvers import BurgersSolverTorch, KSSolverTorch
+    from inc_b200.sharding import allreduce_mean_
     from inc_b200.workloads import burgers_diff_config, ks_diff_config
 
+    # data-parallel over ranks: every rank trains the same seeded network on its own seeded
+    # trajectories and the gradients are averaged every step (one all-reduce)
+    rank = torch.distributed.get_rank() if world > 1 else 0
     torch.manual_seed(0)
     # FP32 throughout, the corrector included (cuDNN would otherwise run its convolutions in TF32)
     torch.backends.cudnn.allow_tf32 = False
     torch.backends.cuda.matmul.allow_tf32 = False
     if which == "burgers_diff":
-        cfg = burgers_diff_config()
+        cfg = burgers_diff_config(seed=3 + 1000 * rank)
         B, N, steps = cfg["B"], cfg["N"], cfg["steps"]
         mk = lambda: BurgersSolverTorch(SimpleNamespace(  # noqa: E731
             resolution=N, dt=cfg["dt"], x=None, adaptive_CFL=None, L=cfg["L"], nu=cfg["nu"], device=dev,
@@ -573,7 +577,7 @@ def bench_diff(args, dev, world, which):
         net = PeriodicCNN1D(channels=32, kernel=5, layers=4).to(dev)
         L = None
     else:
-        cfg = ks_diff_config()
+        cfg = ks_diff_config(seed=4 + 1000 * rank)
         B, N, steps = cfg["B"], cfg["N"], cfg["steps"]
         L = torch.full((B,), cfg["L"], device=dev)
         mk = lambda: KSSolverTorch(SimpleNamespace(  # noqa: E731
@@ -598,6 +602,8 @@ def bench_diff(args, dev, world, which):
         res, _ = simulate_rollout(net, solver, u0, steps, "INC", L, checkpoint_every=ckpt)
         loss = torch.mean((res - target) ** 2)
         loss.backward()
+        if world > 1:
+            allreduce_mean_([p.grad for p in net.parameters()])
         opt.step()
         opt.zero_grad(set_to_none=False)
         return loss
@@ -680,6 +686,8 @@ def bench_diff(args, dev, world, which):
             "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run"}
     cfg = dict(name=which, B=B, N=N, steps=steps, scheme=cfg["scheme"],
                corrector=("PeriodicCNN1D(4x32ch,k5,GELU)" if which == "burgers_diff" else "FNO1D(4 layers,w64,16 modes)"))
+    del graph, graphed  # a CUDA graph holding NCCL calls must be released before the process group
+    torch.cuda.synchronize()
     return cfg, cells, times, extra
 
 
@@ -921,7 +929,10 @@ def main():
                 "dtype": "f32", "data": "synthetic (seeded)",
                 "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "unroll": cfg["steps"],
                            "scheme": cfg["scheme"], "corrector": cfg["corrector"], "checkpoint_every": 8,
-                           "value_is": "whole training step (rollout, loss, backward, Adam) in one CUDA graph"},
+                           "value_is": "whole training step (rollout, loss, backward, Adam) in one CUDA graph",
+                           "parallelism": (f"data-parallel over {world} GPUs: per-rank trajectories, corrector "
+                                           "gradients averaged by one all-reduce per step" if world > 1
+                                           else "single GPU")},
                 "eager": {"train_step_ckpt8": tot / (times["ckpt"] * 1e-3),
                           "train_step_no_ckpt": tot / (times["plain"] * 1e-3),
                           "forward_only": tot / (times["fwd"] * 1e-3),

@@ -1,11 +1,14 @@
 """Sharding of independent trajectories over ranks (one process per GPU).
 
 Trajectories never exchange data, so a batch splits by rows with no collective
-on the data path.  ``partition_rows`` balances rows by their work (n * steps for
-a ragged batch) with a deterministic longest-first greedy assignment, so every
-rank computes the same partition without communication.  ``gather_rows`` and
-``max_over_ranks`` are the only collectives: assembling results (optional) and
-the max-over-ranks of device times for benchmarking.
+on the solver's data path.  ``partition_rows`` balances rows by their work
+(n * steps for a ragged batch) with a deterministic longest-first greedy
+assignment, so every rank computes the same partition without communication.
+``gather_rows`` and ``max_over_ranks`` assemble results (optional) and take the
+max over ranks of device times for benchmarking.  Data-parallel training of a
+corrector has one real exchange per step: ``allreduce_mean_`` averages the
+network's gradients over the ranks (what DDP does), one all-reduce of one flat
+bucket.
 """
 from __future__ import annotations
 
@@ -61,3 +64,24 @@ def max_over_ranks(value: float, device=None, group=None) -> float:
     t = torch.tensor([float(value)], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX, group=group)
     return float(t.item())
+
+
+def allreduce_mean_(tensors, group=None) -> None:
+    """Average `tensors` (e.g. parameter gradients; None entries skipped) in place over the
+    ranks of `group`: the values are packed into one flat bucket, summed by one all-reduce and
+    divided by the world size.  Every rank must call it with tensors of the same shapes."""
+    import torch.distributed as dist
+    ts = [t for t in tensors if t is not None]
+    if not ts or not dist.is_available() or not dist.is_initialized():
+        return
+    world = dist.get_world_size(group)
+    if world == 1:
+        return
+    flat = torch.cat([t.reshape(-1) for t in ts])
+    dist.all_reduce(flat, group=group)
+    flat.div_(world)
+    off = 0
+    for t in ts:
+        n = t.numel()
+        t.copy_(flat[off:off + n].view_as(t))
+        off += n

@@ -16,6 +16,11 @@ def _free_port():
         return s.getsockname()[1]
 
 
+def _shard(rank):
+    g = torch.Generator().manual_seed(100 + rank)
+    return torch.randn(3, 16, generator=g, dtype=torch.float64)
+
+
 def _rank_main(rank, world, port, out_dir):
     import torch.distributed as dist
     from inc_b200.sharding import gather_rows, max_over_ranks, partition_rows
@@ -30,7 +35,15 @@ def _rank_main(rank, world, port, out_dir):
     local = torch.tensor([[float(i), float(cfg["n"][i])] for i in mine], dtype=torch.float64)
     full = gather_rows(local, parts, rank, world)
     t = max_over_ranks(1.0 + rank)
-    torch.save({"full": full, "t": t, "parts": parts}, os.path.join(out_dir, f"rank{rank}.pt"))
+    # data-parallel corrector gradients: each rank's mean loss over its own shard, averaged
+    from inc_b200.correctors import PeriodicCNN1D
+    from inc_b200.sharding import allreduce_mean_
+    torch.manual_seed(0)
+    net = PeriodicCNN1D(channels=4).double()
+    net(_shard(rank)).square().mean().backward()
+    allreduce_mean_([p.grad for p in net.parameters()] + [None])
+    grads = [p.grad.clone() for p in net.parameters()]
+    torch.save({"full": full, "t": t, "parts": parts, "grads": grads}, os.path.join(out_dir, f"rank{rank}.pt"))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -49,6 +62,14 @@ def test_sharding_gloo_world2(tmp_path):
     assert sorted(p[0] + p[1]) == list(range(37)) and res[1]["parts"] == p
     loads = [sum(int(cfg["n"][i]) for i in q) for q in p]
     assert max(loads) - min(loads) <= 512                      # within one largest row
+    # averaged shard gradients == the gradient of the mean loss over the whole batch
+    from inc_b200.correctors import PeriodicCNN1D
+    torch.manual_seed(0)
+    net = PeriodicCNN1D(channels=4).double()
+    net(torch.cat([_shard(r) for r in range(world)])).square().mean().backward()
+    for r in res:
+        for g, p in zip(r["grads"], net.parameters()):
+            torch.testing.assert_close(g, p.grad, rtol=1e-12, atol=1e-14)
 
 
 def test_partition_properties():
