@@ -11,12 +11,13 @@ Two architectures from the benchmark configurations:
   per-trajectory domain size like the reference's FNO corrector
   (models/models_1d/fno.py:39-105) does.
 
-On CUDA tensors the FNO's spectral convolution runs as one kernel per call
-(``inc_spectral_conv1d``: the row-pair FFTs, the mode mixing and the inverse
-FFTs of one trajectory in one CTA) with a hand-written adjoint; the other
-layers are torch (cuBLAS matmuls, cuDNN convolutions).  Shapes the kernel does
-not cover, and CPU tensors, take the torch FFT path.  The CNN runs inside the
-Burgers solver kernel when ``simulate_rollout`` can fuse it (``fused.py``).
+On CUDA tensors each FNO layer's ``spectral(x) + W x + b`` runs through
+``inc_spectral_conv1d`` with a hand-written adjoint.  Its kernels are streaming
+row-pair FFTs to the kept modes, the mode mixing, and streaming inverse FFTs that
+add the 1x1 branch and its bias.  The other layers are batched matmuls (cuBLAS)
+on the [B, width, n] state.  Shapes the kernels do not cover, and CPU tensors,
+take torch's FFTs.  The CNN runs inside the Burgers solver kernel when
+``simulate_rollout`` can fuse it (``fused.py``).
 """
 from __future__ import annotations
 
