@@ -48,9 +48,14 @@ def _check(B, W, n, modes, seed=0):
     return errs
 
 
-@pytest.mark.parametrize("n", SPECTRAL_CONV_N)
-def test_every_row_length(n):
-    _check(3, 8, n, min(16, n // 2))
+_LANES = {16: 4, 32: 8, 64: 16, 128: 32, 256: 32, 512: 32}  # lanes per row pair of each n's transform
+_N_MODES = sorted({(n, m) for n in SPECTRAL_CONV_N for m in (1, _LANES[n], min(16, n // 2), min(32, n // 2))})
+
+
+@pytest.mark.parametrize("n,modes", _N_MODES)
+def test_every_row_length_and_split_path(n, modes):
+    # modes <= lanes: the two rows' coefficients split by one exchange; above: the full mirror split
+    _check(3, 8, n, modes, seed=n + modes)
 
 
 @pytest.mark.parametrize("W,modes", [(2, 1), (6, 5), (64, 16), (128, 32), (64, 32)])
