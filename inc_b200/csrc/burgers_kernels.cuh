@@ -542,7 +542,22 @@ template <int CPT, int TPR>
 struct WideSmem {
     float row[2][CPT * TPR];
     float wmax[2][TPR / 32];
+    float flux[2][TPR];  // each thread's last right-interface flux sum, read by its right neighbour
 };
+
+// h+ + h- at the right interface (i + 1/2) of each of the CPT cells of a window
+// (the same operations as in weno_rhs).
+template <int CPT>
+INC_DEV void weno_right_fluxes(const float (&w)[CPT + 6], float alpha, float (&hs)[CPT]) {
+    const float ha = 0.5f * alpha;
+    float fp[CPT + 6], fm[CPT + 6];
+#pragma unroll
+    for (int k = 1; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c)
+        hs[c] = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
+                weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+}
 
 template <int CPT, int TPR>
 INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, float nu, float inv_dx, float inv_dx2,
@@ -564,7 +579,21 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
         float alpha = 0.f;
 #pragma unroll
         for (int i = 0; i < TPR / 32; ++i) alpha = fmaxf(alpha, sh.wmax[parity][i]);
-        weno_rhs<CPT>(w, alpha, nu * inv_dx2, inv_dx, r);
+        // Only the right interfaces: the first cell's left interface is the previous
+        // thread's last right interface (same row values, same operations), read
+        // back after one barrier instead of reconstructed twice.
+        float hs[CPT];
+        weno_right_fluxes<CPT>(w, alpha, hs);
+        sh.flux[parity][g] = hs[CPT - 1];
+        __syncthreads();
+        float prev = sh.flux[parity][(g + TPR - 1) % TPR];
+        const float nu_dx2 = nu * inv_dx2;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
+            r[c] = fmaf(inv_dx, prev - hs[c], nu_dx2 * lap);
+            prev = hs[c];
+        }
     } else {
         fdm_rhs<CPT>(w, nu * inv_dx2, inv_2dx, r);
     }
@@ -617,7 +646,7 @@ INC_DEV void store_cells(float* __restrict__ p, const float (&r)[CPT]) {
 
 // One step (steps == 1 && frames == nullptr) or a fused rollout, one row per CTA.
 template <int CPT, int TPR>
-__global__ void __launch_bounds__(TPR) k_rollout_wide(Args a, int single_step) {
+__global__ void __launch_bounds__(TPR, 1) k_rollout_wide(Args a, int single_step) {
     __shared__ WideSmem<CPT, TPR> sh;
     const int row = blockIdx.x, g = threadIdx.x;
     Ctx<CPT> cx;
