@@ -185,25 +185,24 @@ INC_DEV void halo_window(const float (&u)[CPT], float (&w)[CPT + 6], int left, i
     w[CPT + 5] = shfl<TPR>(u[2], right);
 }
 
-// r[c] for the CPT cells of a window w (3 halo cells each side):
-// -(Dminus f+ + Dminus f-)/dx + nu D2 u, with f+- reconstructed at i+1/2
-// (solver_1d.py:129-146; the dense D2 matmul is the 3-point stencil).
+// h+ + h- at the right interface (i + 1/2) of each of the CPT cells of a window
+// w (3 halo cells each side), f+- reconstructed at i+1/2 (solver_1d.py:129-142).
+// The right-hand side r[c] = -(Dminus f+ + Dminus f-)/dx + nu D2 u (:129-146; the
+// dense D2 matmul is the 3-point stencil) also needs the first cell's left
+// interface: the previous thread's last right interface, computed there from the
+// same row values by the same operations, so the callers hand it over (a shuffle,
+// or a shared slot) instead of reconstructing it again.  The r loop stays inline
+// at each caller: as a separate function it made the fused CNN kernel 13% slower.
 template <int CPT>
-INC_DEV void weno_rhs(const float (&w)[CPT + 6], float alpha, float nu_dx2, float inv_dx, float (&r)[CPT]) {
+INC_DEV void weno_right_fluxes(const float (&w)[CPT + 6], float alpha, float (&hs)[CPT]) {
     const float ha = 0.5f * alpha;
     float fp[CPT + 6], fm[CPT + 6];
 #pragma unroll
-    for (int k = 0; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
-    // hs = h+ + h- at i+1/2; the difference of the two sums is the flux difference
-    float hs_prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]) + weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
+    for (int k = 1; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) {
-        const float hs = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
-                         weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
-        const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
-        r[c] = fmaf(inv_dx, hs_prev - hs, nu_dx2 * lap);
-        hs_prev = hs;
-    }
+    for (int c = 0; c < CPT; ++c)
+        hs[c] = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
+                weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
 }
 
 // central-difference convection (calc_nonlinear_FDM, solver_1d.py:125-127) + diffusion
@@ -227,7 +226,28 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
 #pragma unroll
         for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
         const float alpha = group_max_nonneg<TPR>(m);  // per-row max |u|, solver_1d.py:133
-        weno_rhs<CPT>(w, alpha, nu * inv_dx2, inv_dx, r);
+        float hs[CPT];
+        weno_right_fluxes<CPT>(w, alpha, hs);
+        float left_flux;
+        if constexpr (CPT <= 8) {
+            left_flux = shfl<TPR>(hs[CPT - 1], left);
+        } else {
+            // at 16 cells per lane the handover saves 1/17 of the reconstructions, and the
+            // backward kernels (at the register limit) run slower with it: reconstruct
+            const float ha = 0.5f * alpha;
+            float fp[6], fm[6];
+#pragma unroll
+            for (int k = 0; k < 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
+            left_flux = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]) + weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
+        }
+        float prev = left_flux;
+        const float nu_dx2 = nu * inv_dx2;
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) {
+            const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
+            r[c] = fmaf(inv_dx, prev - hs[c], nu_dx2 * lap);
+            prev = hs[c];
+        }
     } else {
         fdm_rhs<CPT>(w, nu * inv_dx2, inv_2dx, r);
     }
@@ -545,19 +565,6 @@ struct WideSmem {
     float flux[2][TPR];  // each thread's last right-interface flux sum, read by its right neighbour
 };
 
-// h+ + h- at the right interface (i + 1/2) of each of the CPT cells of a window
-// (the same operations as in weno_rhs).
-template <int CPT>
-INC_DEV void weno_right_fluxes(const float (&w)[CPT + 6], float alpha, float (&hs)[CPT]) {
-    const float ha = 0.5f * alpha;
-    float fp[CPT + 6], fm[CPT + 6];
-#pragma unroll
-    for (int k = 1; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
-#pragma unroll
-    for (int c = 0; c < CPT; ++c)
-        hs[c] = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
-                weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
-}
 
 template <int CPT, int TPR>
 INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, float nu, float inv_dx, float inv_dx2,
@@ -579,9 +586,7 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
         float alpha = 0.f;
 #pragma unroll
         for (int i = 0; i < TPR / 32; ++i) alpha = fmaxf(alpha, sh.wmax[parity][i]);
-        // Only the right interfaces: the first cell's left interface is the previous
-        // thread's last right interface (same row values, same operations), read
-        // back after one barrier instead of reconstructed twice.
+        // the first cell's left interface from the previous thread, after one barrier
         float hs[CPT];
         weno_right_fluxes<CPT>(w, alpha, hs);
         sh.flux[parity][g] = hs[CPT - 1];
