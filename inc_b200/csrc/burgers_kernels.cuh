@@ -226,27 +226,35 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
 #pragma unroll
         for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
         const float alpha = group_max_nonneg<TPR>(m);  // per-row max |u|, solver_1d.py:133
-        float hs[CPT];
-        weno_right_fluxes<CPT>(w, alpha, hs);
-        float left_flux;
-        if constexpr (CPT <= 8) {
-            left_flux = shfl<TPR>(hs[CPT - 1], left);
-        } else {
-            // at 16 cells per lane the handover saves 1/17 of the reconstructions, and the
-            // backward kernels (at the register limit) run slower with it: reconstruct
-            const float ha = 0.5f * alpha;
-            float fp[6], fm[6];
-#pragma unroll
-            for (int k = 0; k < 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
-            left_flux = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]) + weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
-        }
-        float prev = left_flux;
         const float nu_dx2 = nu * inv_dx2;
+        if constexpr (CPT <= 8) {
+            float hs[CPT];
+            weno_right_fluxes<CPT>(w, alpha, hs);
+            float prev = shfl<TPR>(hs[CPT - 1], left);
 #pragma unroll
-        for (int c = 0; c < CPT; ++c) {
-            const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
-            r[c] = fmaf(inv_dx, prev - hs[c], nu_dx2 * lap);
-            prev = hs[c];
+            for (int c = 0; c < CPT; ++c) {
+                const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
+                r[c] = fmaf(inv_dx, prev - hs[c], nu_dx2 * lap);
+                prev = hs[c];
+            }
+        } else {
+            // At 16 cells per lane the handover saves 1/17 of the reconstructions; the
+            // left interface is reconstructed here and the fluxes are consumed as they
+            // are made (two live values, for the register-bound backward and adaptive
+            // kernels).
+            const float ha = 0.5f * alpha;
+            float fp[CPT + 6], fm[CPT + 6];
+#pragma unroll
+            for (int k = 0; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
+            float prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]) + weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
+#pragma unroll
+            for (int c = 0; c < CPT; ++c) {
+                const float hs = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
+                                 weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+                const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
+                r[c] = fmaf(inv_dx, prev - hs, nu_dx2 * lap);
+                prev = hs;
+            }
         }
     } else {
         fdm_rhs<CPT>(w, nu * inv_dx2, inv_2dx, r);
