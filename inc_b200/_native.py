@@ -76,6 +76,8 @@ SIGNATURES = {
                                       C.c_int32, _vp]),
     "inc_spectral_conv1d_bwd": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32,
                                           _vp]),
+    "inc_bias_gelu": (C.c_int, [_vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, _vp]),
+    "inc_bias_gelu_bwd": (C.c_int, [_vp, _vp, _vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32, _vp]),
     "inc_burgers_rollout_grad_noalloc": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, C.c_int32,
                                                    C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
     "inc_burgers_cnn_rollout": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, C.c_int32, _vp, _vp,

@@ -14,8 +14,9 @@ Two architectures from the benchmark configurations:
 On CUDA tensors each FNO layer's ``spectral(x) + W x + b`` runs through
 ``inc_spectral_conv1d`` with a hand-written adjoint.  Its kernels are streaming
 row-pair FFTs to the kept modes, the mode mixing, and streaming inverse FFTs that
-add the 1x1 branch and its bias.  The other layers are batched matmuls (cuBLAS)
-on the [B, width, n] state.  Shapes the kernels do not cover, and CPU tensors,
+add the 1x1 branch and its bias.  The projection's bias and GELU are one kernel
+(``inc_bias_gelu``).  The other layers are batched matmuls (cuBLAS) on the
+[B, width, n] state.  Shapes the kernels do not cover, and CPU tensors,
 take torch's FFTs.  The CNN runs inside the Burgers solver kernel when
 ``simulate_rollout`` can fuse it (``fused.py``).
 """
@@ -139,8 +140,9 @@ def spectral_conv1d(x, w_re, w_im, modes: int, bias=None, addend=None):
     layer's sum with its 1x1 convolution): the CUDA kernel where it applies,
     else torch FFTs."""
     m = min(modes, x.shape[-1] // 2 + 1)
-    if spectral_conv_supported(x, w_re, w_im, m) and (bias is None or (bias.is_cuda and bias.dtype == torch.float32 and bias.shape == x.shape[1:2])) \
-            and (addend is None or (addend.shape == x.shape and addend.dtype == torch.float32 and addend.is_cuda)):
+    bias_ok = bias is None or (bias.is_cuda and bias.dtype == torch.float32 and bias.shape == x.shape[1:2])
+    addend_ok = addend is None or (addend.is_cuda and addend.dtype == torch.float32 and addend.shape == x.shape)
+    if spectral_conv_supported(x, w_re, w_im, m) and bias_ok and addend_ok:
         return SpectralConv1dFn.apply(x, w_re, w_im, bias, addend, m)
     y = spectral_conv1d_torch(x, w_re, w_im, modes)
     if bias is not None:
@@ -173,6 +175,43 @@ def _channel_mm(w, x):
     as this product too (same parameters and result): cuDNN's FP32 weight
     gradient for 1x1 convolutions is a slow direct kernel."""
     return torch.bmm(w.expand(x.shape[0], -1, -1), x)
+
+
+class BiasGeluFn(torch.autograd.Function):
+    """gelu(h + bias[:, None]) for h [B, C, n] on CUDA: ``inc_bias_gelu`` (one pass), and
+    ``inc_bias_gelu_bwd`` (gelu' and the per-row sums that give the bias gradient)."""
+
+    @staticmethod
+    def forward(ctx, h, bias):
+        h = h.contiguous()
+        B, C, n = h.shape
+        y = torch.empty_like(h)
+        rc = nat.lib().inc_bias_gelu(h.data_ptr(), bias.data_ptr(), y.data_ptr(), B * C, n, C,
+                                     nat.stream_of(h.device))
+        nat.check(rc, "inc_bias_gelu")
+        ctx.save_for_backward(h, bias)
+        return y
+
+    @staticmethod
+    def backward(ctx, gy):
+        h, bias = ctx.saved_tensors
+        gy = gy.contiguous()
+        B, C, n = h.shape
+        gh = torch.empty_like(h)
+        sums = torch.empty(B * C, device=h.device, dtype=torch.float32)
+        rc = nat.lib().inc_bias_gelu_bwd(gy.data_ptr(), h.data_ptr(), bias.data_ptr(), gh.data_ptr(),
+                                         sums.data_ptr(), B * C, n, C, nat.stream_of(h.device))
+        nat.check(rc, "inc_bias_gelu_bwd")
+        return gh, sums.view(B, C).sum(0)
+
+
+def bias_gelu(h, bias):
+    """F.gelu(h + bias[:, None]) for h [B, C, n]: one CUDA kernel where it applies."""
+    if (h.is_cuda and h.dim() == 3 and h.dtype == torch.float32 and h.shape[-1] % 4 == 0
+            and isinstance(bias, torch.Tensor) and bias.is_cuda and bias.dtype == torch.float32
+            and tuple(bias.shape) == (h.shape[1],)):
+        return BiasGeluFn.apply(h, bias)
+    return F.gelu(h + bias[:, None])
 
 
 def _channel_linear(lin: nn.Linear, x):
@@ -209,5 +248,5 @@ class FNO1D(nn.Module):
                                 addend=_channel_mm(pw.weight[:, :, 0], x))
             if i + 1 < len(self.spectral):
                 x = F.gelu(x)
-        x = F.gelu(_channel_linear(self.proj1, x))
+        x = bias_gelu(_channel_mm(self.proj1.weight, x), self.proj1.bias)
         return _channel_linear(self.proj2, x).squeeze(1)

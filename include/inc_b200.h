@@ -279,6 +279,19 @@ int inc_spectral_conv1d_bwd(const float* g_y, const float* w_re, const float* w_
                             float* g_modes, float* work, int32_t batch, int32_t width, int32_t n,
                             int32_t modes, void* stream);
 
+/* y = gelu(h + bias[r % channels]) for every row r of [rows][n] activations
+ * (exact erf GELU, torch.nn.functional.gelu): the FNO projection's bias and
+ * activation (models/models_1d/fno.py:101-102, fc1 then F.gelu) in one pass
+ * over the channel-major [batch][channels][n] layout.  n a positive multiple
+ * of 4, rows a multiple of channels; 16-byte aligned arrays.               */
+int inc_bias_gelu(const float* h, const float* bias, float* y, int32_t rows, int32_t n,
+                  int32_t channels, void* stream);
+/* Its backward: g_h = g_y * gelu'(h + bias[r % channels]), and row_sums[r]
+ * = sum over the row of g_h (the bias gradient is their sum over the rows of
+ * each channel).                                                             */
+int inc_bias_gelu_bwd(const float* g_y, const float* h, const float* bias, float* g_h,
+                      float* row_sums, int32_t rows, int32_t n, int32_t channels, void* stream);
+
 /* ---- measurement utility ------------------------------------------------ */
 /* FP32 FMA throughput probe used by bench.py for the roofline denominator:
  * `blocks` x 256 threads, each 128 * iters FMAs (2 flops each) in 8

@@ -10,8 +10,8 @@ import pytest
 import torch
 
 from inc_b200 import _native as nat
-from inc_b200.correctors import (FNO1D, SPECTRAL_CONV_N, SpectralConv1d, spectral_conv1d, spectral_conv1d_torch,
-                                 spectral_conv_supported)
+from inc_b200.correctors import (FNO1D, SPECTRAL_CONV_N, SpectralConv1d, bias_gelu, spectral_conv1d,
+                                 spectral_conv1d_torch, spectral_conv_supported)
 
 pytestmark = pytest.mark.gpu
 TOL = 1e-5  # max abs error over max abs FP64 value
@@ -162,3 +162,32 @@ def test_fno_corrector_matches_fp64():
     for (name, p), (_, pr) in zip(net.named_parameters(), ref_net.named_parameters()):
         assert _rel(p.grad, pr.grad) < 1e-4, name
     assert isinstance(net.spectral[0], SpectralConv1d)
+
+
+@pytest.mark.parametrize("B,C,n", [(3, 128, 512), (2, 8, 16), (1, 5, 36)])
+def test_bias_gelu_matches_fp64(B, C, n):
+    """The FNO projection's gelu(h + b) (inc_bias_gelu and its backward) against torch in FP64."""
+    g = torch.Generator().manual_seed(B * C + n)
+    h = 3 * torch.randn(B, C, n, generator=g, dtype=torch.float64)
+    b = torch.randn(C, generator=g, dtype=torch.float64)
+    gy = torch.randn(B, C, n, generator=g, dtype=torch.float64)
+    hr, br = h.clone().requires_grad_(True), b.clone().requires_grad_(True)
+    yr = torch.nn.functional.gelu(hr + br[:, None])
+    yr.backward(gy)
+    hc, bc = h.float().cuda().requires_grad_(True), b.float().cuda().requires_grad_(True)
+    y = bias_gelu(hc, bc)
+    assert "BiasGeluFn" in type(y.grad_fn).__name__
+    y.backward(gy.float().cuda())
+    assert _rel(y, yr.detach()) < TOL
+    assert _rel(hc.grad, hr.grad) < TOL
+    assert _rel(bc.grad, br.grad) < TOL
+
+
+def test_bias_gelu_c_abi_rejects_bad_shapes():
+    lib = nat.lib()
+    h = torch.zeros(2, 4, 18, device="cuda")
+    b = torch.zeros(4, device="cuda")
+    s = nat.stream_of(h.device)
+    assert lib.inc_bias_gelu(h.data_ptr(), b.data_ptr(), h.data_ptr(), 8, 18, 4, s) != 0   # n not a multiple of 4
+    assert lib.inc_bias_gelu(h.data_ptr(), b.data_ptr(), h.data_ptr(), 8, 16, 3, s) != 0   # rows % channels
+    assert "bias_gelu" in nat.last_error()
