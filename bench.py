@@ -512,7 +512,7 @@ def bench_burgers_batched(args, dev, world):
     cfg = burgers_batched_config()
     rb = RaggedBurgers(cfg["u0"], cfg["nu"], cfg["dt"], cfg["dx"], scheme=cfg["scheme"], device=dev)
     grid, tune_ms = autotune.tune_ragged(rb)  # outside the timed region
-    cfg["layout"] = {"grid_blocks": grid, "warps_per_block": 4, "autotune_ms_per_20_steps": tune_ms}
+    cfg["layout"] = {"grid_blocks": grid, "warps_per_block": 4, "autotune_ms_per_100_steps": tune_ms}
     steps = cfg["steps"]
     cells = rb.total * steps
     out = torch.empty_like(rb.u0)

@@ -158,14 +158,19 @@ def tune_ks(n, rows, scheme="ETRK2", device="cuda", steps=50, L=64.0, dt=0.25):
     return best, times
 
 
-def tune_ragged(rb, steps=20):
-    """Time the persistent ragged launch at a few grid sizes; keep the fastest on `rb`."""
+def tune_ragged(rb, steps=100, margin=0.02):
+    """Time the persistent ragged launch at a few grid sizes and keep the fastest on `rb`.
+    The default grid (sized to the work) is kept unless another one is faster by more
+    than `margin`: launches of a few hundred microseconds differ by about that much from
+    run to run, and a pick made on that noise does not carry over to long rollouts."""
     sms = torch.cuda.get_device_properties(rb.device).multi_processor_count
+    default = rb.default_grid()
     times = {}
-    for g in sorted({rb.default_grid(), 2 * sms, 3 * sms, 4 * sms}):
+    for g in sorted({default, 2 * sms, 3 * sms, 4 * sms}):
         rb.grid_blocks = g
         times[g] = _time(lambda: rb.rollout(steps))
-    rb.grid_blocks = min(times, key=times.get)
+    best = min(times, key=times.get)
+    rb.grid_blocks = best if times[best] < (1.0 - margin) * times[default] else default
     return rb.grid_blocks, times
 
 
