@@ -185,32 +185,26 @@ __global__ void __launch_bounds__(256) k_cnn_rollout_bwd(Args a, const float* __
         for (int k = 0; k < KW; ++k) { g2[c][k] = 0.f; g3[c][k] = 0.f; }
 #pragma unroll
     for (int k = 0; k < KW; ++k) { g1[k] = 0.f; g4[k] = 0.f; }
-    // warp 0: the solver in its warp layout (8 cells per lane)
-    const int left = (lane + 31) & 31, right = (lane + 1) & 31;
-    Ctx<8> cx;
-    make_ctx<8, 32>(a, row, lane, true, cx);
+    // The solver, one cell per thread (the wide-row layout): all eight warps run the
+    // segment replay and the step adjoints.  Its shared scratch is S.x, which holds
+    // no activations while the solver runs.
+    WideAdjSmem<BN>& SW = *reinterpret_cast<WideAdjSmem<BN>*>(&S.x[0][0]);
+    Ctx<1> cx;
+    make_ctx<1, BN>(a, row, t, true, cx);
     cx.has_s = true;
-    float gu[8];
-    const int64_t rbase = (int64_t)row * BN + 8 * lane;
-    if (w == 0) {
-        if (a.g_final) load_row_chunk<8>(gu, a.g_final + rbase, true);
-        else {
-#pragma unroll
-            for (int c = 0; c < 8; ++c) gu[c] = 0.f;
-        }
-    }
+    int parity = 0;
+    const int64_t cell = (int64_t)row * BN + t;
+    float gu = a.g_final ? __ldg(a.g_final + cell) : 0.f;
     for (int sidx = nseg - 1; sidx >= 0; --sidx) {
         const int k0 = sidx * K;
         const int len = min(K, a.steps - k0);
-        if (w == 0) {  // replay the segment's states from its checkpoint
-            float u[8];
-            load_row_chunk<8>(u, a.ckpts + ((int64_t)row * nseg + sidx) * BN + 8 * lane, true);
+        {  // replay the segment's states from its checkpoint
+            float u[1] = {__ldg(a.ckpts + ((int64_t)row * nseg + sidx) * BN + t)};
             for (int j = 0; j < len; ++j) {
-#pragma unroll
-                for (int c = 0; c < 8; ++c) seg[j][8 * lane + c] = u[c];
+                seg[j][t] = u[0];
                 if (j + 1 < len) {
-                    load_row_chunk<8>(cx.s, corr + ((int64_t)row * a.steps + k0 + j) * BN + 8 * lane, true);
-                    advance<8, 32>(a, cx, u, cx.t + (k0 + j) * cx.dt, left, right);
+                    cx.s[0] = __ldg(corr + ((int64_t)row * a.steps + k0 + j) * BN + t);
+                    advance_wide<1, BN>(a, cx, u, cx.t + (k0 + j) * cx.dt, SW.fw, parity, t);
                 }
             }
         }
@@ -230,30 +224,18 @@ __global__ void __launch_bounds__(256) k_cnn_rollout_bwd(Args a, const float* __
             __syncthreads();
             conv_mid<BN, false>(S.w + OFF_W3, S.w + OFF_B3, S.x, S.z[2], w, lane);
             __syncthreads();
-            // ---- the solver step's adjoint (warp 0): u_bar through S and s_bar; meanwhile
-            // warps 1-7 form layer 4's input gelu(z3)
-            if (w != 0) gelu_rows(S.x, S.z[2], 32, 224);
-            if (w == 0) {
-                const int64_t at = ((int64_t)row * a.steps + k) * BN + 8 * lane;
-                if (a.g_frames) {
-                    float gf[8];
-                    load_row_chunk<8>(gf, a.g_frames + at, true);
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) gu[c] += gf[c];
-                }
-                float u[8], gs[8];
-#pragma unroll
-                for (int c = 0; c < 8; ++c) { u[c] = seg[j][8 * lane + c]; gs[c] = 0.f; }
-                load_row_chunk<8>(cx.s, corr + at, true);
-                advance_bwd<8, 32>(a, cx, u, gu, gs, cx.t + k * cx.dt, lane, left, right);
-                if (g_corr) {
-                    float gc[8];
-                    load_row_chunk<8>(gc, g_corr + at, true);
-#pragma unroll
-                    for (int c = 0; c < 8; ++c) gs[c] += gc[c];
-                }
-                put_row_warp(S.d, gs, lane);
+            // ---- the solver step's adjoint, all threads: u_bar through S and s_bar
+            {
+                const int64_t at = ((int64_t)row * a.steps + k) * BN + t;
+                if (a.g_frames) gu += __ldg(a.g_frames + at);
+                float gs = 0.f;
+                cx.s[0] = __ldg(corr + at);
+                advance_bwd_wide<BN>(a, cx, seg[j][t], gu, gs, cx.t + k * cx.dt, SW, parity, t);
+                if (g_corr) gs += __ldg(g_corr + at);
+                put_cell<BN>(S.d, t, gs);
             }
+            __syncthreads();
+            gelu_rows(S.x, S.z[2]);  // layer 4's input gelu(z3), after the solver's use of S.x
             __syncthreads();
             // ---- layer 4 (32 -> 1, no activation): dW4, db4, then dz3 in place of z3
             wgrad_part(g4, S.d, S.x[lane], w);
@@ -328,37 +310,60 @@ __global__ void __launch_bounds__(256) k_cnn_rollout_bwd(Args a, const float* __
                 S.d[apad(t + 2)] = du;
             }
             __syncthreads();
-            if (w == 0) {
-#pragma unroll
-                for (int c = 0; c < 8; ++c) gu[c] += S.d[apad(8 * lane + c + 2)];
-            }
+            gu += S.d[apad(t + 2)];
             // the next step's first writes (S.u) are ordered after these reads by its first barrier
         }
         __syncthreads();  // segment states are rewritten by the next replay
     }
-    if (w == 0) store_row_chunk<8>(a.g_u + rbase, gu, true);
-    // ---- weight gradients: per-thread sums -> shared -> this row's slot of work
+    a.g_u[cell] = gu;
+    // ---- weight gradients: per-thread sums -> shared -> this row's slot of work.
+    // W2, W3: one slot per thread.  W1, W4 and the biases: one partial per warp,
+    // summed over the warps in a fixed order (the result does not depend on timing).
     float* acc = &S.z[0][0][0];
+    constexpr int NP = 2 * KW + 4;
+    float* part = &S.z[2][0][0];  // [8 warps][32 lanes][NP], past acc's W_FLOATS
     __syncthreads();
     for (int i = t; i < W_FLOATS; i += blockDim.x) acc[i] = 0.f;
+    {
+        float* p = part + (w * 32 + lane) * NP;
+#pragma unroll
+        for (int k = 0; k < KW; ++k) {
+            p[k] = g1[k];
+            p[KW + k] = g4[k];
+        }
+        p[2 * KW] = gb1;
+        p[2 * KW + 1] = gb2;
+        p[2 * KW + 2] = gb3;
+        p[2 * KW + 3] = gb4;
+    }
     __syncthreads();
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
         for (int k = 0; k < KW; ++k) {
             const int co = 4 * w + c;
-            atomicAdd(acc + OFF_W2 + (lane * C + co) * KW + k, g2[c][k]);
-            atomicAdd(acc + OFF_W3 + (lane * C + co) * KW + k, g3[c][k]);
+            acc[OFF_W2 + (lane * C + co) * KW + k] = g2[c][k];
+            acc[OFF_W3 + (lane * C + co) * KW + k] = g3[c][k];
+        }
+    if (w == 0) {
+        float s[NP];
+#pragma unroll
+        for (int i = 0; i < NP; ++i) s[i] = 0.f;
+        for (int q = 0; q < 8; ++q) {
+            const float* p = part + (q * 32 + lane) * NP;
+#pragma unroll
+            for (int i = 0; i < NP; ++i) s[i] += p[i];
         }
 #pragma unroll
-    for (int k = 0; k < KW; ++k) {
-        atomicAdd(acc + OFF_W1 + lane * KW + k, g1[k]);
-        atomicAdd(acc + OFF_W4 + lane * KW + k, g4[k]);
+        for (int k = 0; k < KW; ++k) {
+            acc[OFF_W1 + lane * KW + k] = s[k];
+            acc[OFF_W4 + lane * KW + k] = s[KW + k];
+        }
+        acc[OFF_B1 + lane] = s[2 * KW];
+        acc[OFF_B2 + lane] = s[2 * KW + 1];
+        acc[OFF_B3 + lane] = s[2 * KW + 2];
+        if (lane == 0) acc[OFF_B4] = s[2 * KW + 3];  // each warp's gb4 is the same on all its lanes
     }
-    atomicAdd(acc + OFF_B1 + lane, gb1);
-    atomicAdd(acc + OFF_B2 + lane, gb2);
-    atomicAdd(acc + OFF_B3 + lane, gb3);
-    if (lane == 0) atomicAdd(acc + OFF_B4, gb4);
     __syncthreads();
     for (int i = t; i < W_FLOATS; i += blockDim.x) work[(int64_t)row * W_FLOATS + i] = acc[i];
 }

@@ -646,6 +646,122 @@ INC_DEV void advance_wide(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], fl
     }
 }
 
+// ---- wide-row adjoint (one cell per thread, TPR threads per row) -----------------
+// Shared scratch: the forward's row buffers (stage replays) and the adjoint's
+// rows, contributions and per-warp reductions.
+template <int TPR>
+struct WideAdjSmem {
+    WideSmem<1, TPR> fw;
+    float urow[TPR];   // u of the stage being differentiated
+    float vrow[TPR];   // the adjoint vector v
+    float ub[6][TPR];  // ub[e][i]: cell i's contribution to cell i - 2 + e
+    float wmax[TPR / 32];
+    int warg[TPR / 32];
+    float wsum[TPR / 32];
+};
+
+// out = J(u)^T v at this thread's cell: rhs_vjp for one cell per thread, the
+// halos, the row max |u| with its first argmax (alpha's gradient) and the
+// neighbours' contributions through shared memory (two block barriers).
+template <int TPR>
+INC_DEV void rhs_vjp_wide(const Args& a, const Ctx<1>& cx, float u, float v, float& out, WideAdjSmem<TPR>& sh,
+                          int g) {
+    constexpr int N = TPR, NW = TPR / 32;
+    const int lane = g & 31, warp = g >> 5;
+    sh.urow[g] = u;
+    sh.vrow[g] = v;
+    const bool weno = a.conv == INC_CONV_WENO;
+    if (weno) {  // as the forward's fmaxf: a NaN cell is passed over
+        const float au = fabsf(u);
+        float m = au > 0.f ? au : 0.f;
+        int mi = g;
+        group_argmax_nonneg<32>(m, mi);
+        if (lane == 0) {
+            sh.wmax[warp] = m;
+            sh.warg[warp] = mi;
+        }
+    }
+    __syncthreads();
+    float w[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) w[k] = sh.urow[(g - 3 + k + N) & (N - 1)];
+    const float v_r = sh.vrow[(g + 1) & (N - 1)], v_l = sh.vrow[(g + N - 1) & (N - 1)];
+    float alpha = 0.f;
+    int am = 0;
+    if (weno) {
+        alpha = sh.wmax[0];
+        am = sh.warg[0];
+#pragma unroll
+        for (int i = 1; i < NW; ++i)
+            if (sh.wmax[i] > alpha) {
+                alpha = sh.wmax[i];
+                am = sh.warg[i];
+            }
+        float fp[7], fm[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) flux_split(w[k], 0.5f * alpha, fp[k], fm[k]);
+        float accp[6], accm[6];  // index e <-> cell g - 2 + e
+#pragma unroll
+        for (int e = 0; e < 6; ++e) { accp[e] = 0.f; accm[e] = 0.f; }
+        // hp at g + 1/2 enters R[g] with -1/dx and R[g+1] with +1/dx (same for hm)
+        const float hb = (v_r - v) * a.inv_dx;
+        weno5_vjp<false>(fp[1], fp[2], fp[3], fp[4], fp[5], hb, accp[0], accp[1], accp[2], accp[3], accp[4]);
+        weno5_vjp<true>(fm[2], fm[3], fm[4], fm[5], fm[6], hb, accm[1], accm[2], accm[3], accm[4], accm[5]);
+        float abar = 0.f;
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+            const float uj = w[e + 1];
+            sh.ub[e][g] = accp[e] * (0.5f * (uj + alpha)) + accm[e] * (0.5f * (uj - alpha));
+            abar += 0.5f * uj * (accp[e] - accm[e]);
+        }
+        abar = group_sum<32>(abar);
+        if (lane == 0) sh.wsum[warp] = abar;
+    }
+    __syncthreads();
+    if (weno) {
+        out = sh.ub[0][(g + 2) & (N - 1)] + sh.ub[1][(g + 1) & (N - 1)] + sh.ub[2][g] +
+              sh.ub[3][(g + N - 1) & (N - 1)] + sh.ub[4][(g + N - 2) & (N - 1)] + sh.ub[5][(g + N - 3) & (N - 1)];
+        if (g == am) {  // alpha = |u[argmax]|: d|u|/du = sign(u) (torch.abs backward, 0 at 0)
+            float abar = 0.f;
+#pragma unroll
+            for (int i = 0; i < NW; ++i) abar += sh.wsum[i];
+            const float sg = u > 0.f ? 1.f : (u < 0.f ? -1.f : 0.f);
+            out = fmaf(abar, sg, out);
+        }
+    } else {  // R_i = -u_i (u_{i+1} - u_{i-1}) / (2 dx)
+        out = -v * ((w[4] - w[2]) * a.inv_2dx) - v_l * w[2] * a.inv_2dx + v_r * w[4] * a.inv_2dx;
+    }
+    out += cx.nu * ((v_l - 2.f * v + v_r) * a.inv_dx2);
+    if (a.src == INC_SRC_LINEAR) out = fmaf(cx.beta, v, out);
+}
+
+// advance_bwd for one cell per thread: the stage inputs replayed with the wide
+// forward, then the stages' adjoints in reverse (see advance_bwd).
+template <int TPR>
+INC_DEV void advance_bwd_wide(const Args& a, const Ctx<1>& cx, float u, float& gu, float& gs, float t,
+                              WideAdjSmem<TPR>& sh, int& parity, int g) {
+    const float dt = cx.dt;
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
+    float x[1] = {u}, r[1];
+    float u1 = u, u2 = u;
+    for (int k = 0; k + 1 < stages; ++k) {  // replay u_1, u_2
+        full_rhs_wide<1, TPR>(a, cx, x, r, t + rk3_c(k) * dt, sh.fw, parity, g);
+        x[0] = rk3_a(k) * u + rk3_b(k) * (x[0] + dt * r[0]);
+        if (k == 0) u1 = x[0];
+        else u2 = x[0];
+    }
+    float acc = 0.f;
+    for (int k = stages - 1; k >= 0; --k) {
+        float rv;
+        rhs_vjp_wide<TPR>(a, cx, k == 2 ? u2 : (k == 1 ? u1 : u), gu, rv, sh, g);
+        const float ka = rk3_a(k), kb = rk3_b(k);
+        gs += kb * dt * gu;
+        acc += ka * gu;
+        gu = kb * (gu + dt * rv);
+    }
+    gu += acc;
+}
+
 template <int CPT>
 INC_DEV void load_cells(float (&r)[CPT], const float* __restrict__ p) {
 #pragma unroll

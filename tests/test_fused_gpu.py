@@ -290,3 +290,25 @@ def test_fused_rejects_unsupported(cuda):
     with torch.no_grad():
         f, c = simulate_rollout(small, solver, u, 3, "INC")  # falls back to the per-step loop
     assert f.shape == (2, 3, 64) and c.shape == (2, 3, 64)
+
+
+def test_fused_training_gradients_are_deterministic(cuda):
+    """Two runs of the fused backward give bit-identical gradients: every weight-gradient
+    sum (across the warps of a row, then across rows) is taken in a fixed order."""
+    from inc_b200.fused import burgers_cnn_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    N, B, steps = 256, 7, 9
+    p = _params(N, B=B, seed=11)
+    u0_np = _u0(B, N, seed=12)
+
+    def run():
+        net = _net(5).float().to(cuda)
+        solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+        u0 = torch.tensor(u0_np, dtype=torch.float32, device=cuda, requires_grad=True)
+        f, c = burgers_cnn_rollout(net, solver, u0, steps, ckpt_every=4)
+        (f.square().sum() + c.square().sum()).backward()
+        return [u0.grad.clone()] + [q.grad.clone() for q in net.parameters()]
+
+    a, b = run(), run()
+    for x, y in zip(a, b):
+        assert torch.equal(x, y)
