@@ -5,17 +5,18 @@
 // Forward per step k: s_k = CNN(u_k), u_{k+1} = S(u_k, s_k), frame k = u_{k+1}.
 // Backward, one CTA (256 threads) per row, segments of ckpt_every steps in
 // reverse order:
-//   * replay: warp 0 re-runs the solver from the segment's checkpoint with the
-//     forward's saved corrections s_k, keeping every u_k in shared memory;
+//   * replay: all threads re-run the solver from the segment's checkpoint (one
+//     cell per thread, the wide forward) with the forward's saved corrections
+//     s_k, keeping every u_k in shared memory;
 //   * per step k (last first): u_bar += dL/dframe_k; the CNN's pre-activations
-//     z1..z3 at u_k are recomputed into shared memory; warp 0 runs the solver
-//     step's adjoint (advance_bwd, the kernels' SSP-RK3/Euler VJP), giving
-//     u_bar through S and s_bar = dL/ds_k (+ dL/dcorrection_k); then the
-//     network's backward layer by layer: weight gradients (kept in registers for
-//     the whole launch) and input adjoints, GELU' applied in place over z;
-//     finally u_bar += dCNN/du^T s_bar.
-// Weight gradients go to a per-row slot of `work` (each thread's sums added in
-// shared memory first), and a second kernel adds the rows in a fixed order.
+//     z1..z3 at u_k are recomputed into shared memory; all threads run the
+//     solver step's adjoint (advance_bwd_wide, the SSP-RK3/Euler VJP one cell
+//     per thread), giving u_bar through S and s_bar = dL/ds_k
+//     (+ dL/dcorrection_k); then the network's backward layer by layer: weight
+//     gradients (kept in registers for the whole launch) and input adjoints,
+//     GELU' applied in place over z; finally u_bar += dCNN/du^T s_bar.
+// Weight gradients go to a per-row slot of `work` (the warps' partials summed in
+// a fixed order), and a second kernel adds the rows in a fixed order.
 //
 // Thread maps (256 threads = 8 warps, N = 256 cells):
 //   convolution tiles: warp w = channel group (4 channels), lane = 8 cells;
@@ -151,17 +152,6 @@ INC_DEV void wgrad_part(float (&acc)[KW], const float* dr, const float* ar, int 
             acc[k] = fmaf(d.x, win[2 * i + k], acc[k]);
             acc[k] = fmaf(d.y, win[2 * i + 1 + k], acc[k]);
         }
-    }
-}
-
-// warp 0's cells in the solver's layout: lane holds cells 8 lane .. 8 lane + 7
-INC_DEV void put_row_warp(float* row, const float (&v)[8], int lane) {
-#pragma unroll
-    for (int c = 0; c < 8; ++c) {
-        const int x = 8 * lane + c;
-        row[apad(x + 2)] = v[c];
-        if (x < 2) row[apad(BN + 2 + x)] = v[c];
-        if (x >= BN - 2) row[apad(x - BN + 2)] = v[c];
     }
 }
 
