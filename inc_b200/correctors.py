@@ -207,7 +207,7 @@ class BiasGeluFn(torch.autograd.Function):
 
 def bias_gelu(h, bias):
     """F.gelu(h + bias[:, None]) for h [B, C, n]: one CUDA kernel where it applies."""
-    if (h.is_cuda and h.dim() == 3 and h.dtype == torch.float32 and h.shape[-1] % 4 == 0
+    if (h.is_cuda and h.dim() == 3 and h.dtype == torch.float32 and h.shape[-1] % 4 == 0 and h.shape[0] > 0
             and isinstance(bias, torch.Tensor) and bias.is_cuda and bias.dtype == torch.float32
             and tuple(bias.shape) == (h.shape[1],)):
         return BiasGeluFn.apply(h, bias)

@@ -35,8 +35,21 @@ int dispatch(Kind kind, const Args& a, int cpt, cudaStream_t st) {
     const int n = a.n;
     const bool fwd = kind == Kind::Step || kind == Kind::Rollout;
     // Small batches: spread each row over a whole CTA (1-2 cells per lane).
-    if (cpt == 0 && fwd && a.rows <= 148 && n >= 64) cpt = n >= 256 ? 2 : 1;
-    if ((cpt == 1 || cpt == 2) && !fwd) cpt = 0;  // the adjoints use the warp layouts
+    const bool small = a.rows <= 148 && n >= 64;
+    if (cpt == 0 && fwd && small) cpt = n >= 256 ? 2 : 1;
+    if (!fwd && (cpt == 1 || cpt == 2 || (cpt == 0 && small))) {
+        // the adjoints' wide layout has one cell per thread; where it does not
+        // apply (n, or a segment too large for shared memory) the warp layouts do
+        const int K = kind == Kind::StepBwd ? 1 : a.ckpt_every;
+        const size_t seg = (size_t)K * n * sizeof(float);
+        if (is_pow2(n) && n >= 64 && n <= 512 && K >= 1) {
+#define INC_BW(T) \
+            if (n == T && seg + bwd_wide_static_smem<T>() <= 227 * 1024) return launch_bwd_wide<T>(kind, a, st);
+            INC_BURGERS_BWD_WIDE_SHAPES(INC_BW)
+#undef INC_BW
+        }
+        cpt = 0;
+    }
     if (cpt == 1 || cpt == 2) {
         if (!is_pow2(n) || n < 64 || n / cpt > 512) {
             set_error("burgers: cells_per_thread=%d needs n a power of two with 64 <= n/%d <= 512", cpt, cpt);

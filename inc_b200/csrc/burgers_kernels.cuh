@@ -796,6 +796,45 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_wide(Args a, int single_step
     if (a.out) store_cells<CPT>(a.out + base, u);
 }
 
+// Backward of a fused rollout (or of one step: ckpts = u, one one-step segment,
+// g_final = dL/du_new), one row per CTA and one cell per thread.  Each segment
+// is replayed from its checkpoint with the wide forward, every state going to
+// this thread's slot of `seg` ([step][cell], written and read by the same
+// thread), and then differentiated step by step, last first, by
+// advance_bwd_wide.  For small batches, where the warp layout's serial cells
+// per lane set the latency of every step.
+template <int TPR>
+__global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
+    __shared__ WideAdjSmem<TPR> sh;
+    extern __shared__ float seg[];
+    const int row = blockIdx.x, g = threadIdx.x;
+    Ctx<1> cx;
+    make_ctx<1, TPR>(a, row, g, true, cx);
+    if (cx.has_s) cx.s[0] = __ldg(a.s + (int64_t)row * TPR + g);
+    const int K = a.ckpt_every;
+    const int nseg = (a.steps + K - 1) / K;
+    const int64_t base = (int64_t)row * TPR + g;
+    float gu = a.g_final ? __ldg(a.g_final + base) : 0.f;
+    float gs = 0.f;
+    int parity = 0;
+    for (int sidx = nseg - 1; sidx >= 0; --sidx) {
+        const int k0 = sidx * K;
+        const int len = min(K, a.steps - k0);
+        float u[1] = {__ldg(a.ckpts + ((int64_t)row * nseg + sidx) * TPR + g)};
+        for (int j = 0; j < len; ++j) {
+            seg[j * TPR + g] = u[0];
+            if (j + 1 < len) advance_wide<1, TPR>(a, cx, u, cx.t + (k0 + j) * cx.dt, sh.fw, parity, g);
+        }
+        for (int j = len - 1; j >= 0; --j) {
+            const int k = k0 + j;
+            if (a.g_frames) gu += __ldg(a.g_frames + ((int64_t)row * a.steps + k) * TPR + g);
+            advance_bwd_wide<TPR>(a, cx, seg[j * TPR + g], gu, gs, cx.t + k * cx.dt, sh, parity, g);
+        }
+    }
+    a.g_u[base] = gu;
+    if (a.g_s) a.g_s[base] = gs;
+}
+
 // weno_reconstruction(f, direction) as a standalone op (solver_1d.py:4-42).
 template <int CPT, int TPR>
 __global__ void __launch_bounds__(256) k_weno(const float* __restrict__ f, float* __restrict__ out, int rows,
@@ -866,6 +905,33 @@ int launch_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
 }
 
 #define INC_BURGERS_WIDE_SHAPES(X) X(1, 64) X(1, 128) X(1, 256) X(1, 512) X(2, 64) X(2, 128) X(2, 256)
+
+// Wide-row backward launchers (one cell per thread), instantiated in burgers_bwd_wide.cu.
+// The dynamic shared memory holds one segment's states: ckpt_every * n floats.
+template <int TPR>
+int launch_bwd_wide(Kind kind, const Args& a, cudaStream_t st);
+
+template <int TPR>
+constexpr size_t bwd_wide_static_smem() { return sizeof(WideAdjSmem<TPR>); }
+
+template <int TPR>
+int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
+    Args b = a;
+    if (kind == Kind::StepBwd) {  // one step = a one-step rollout from the checkpoint u
+        b.ckpts = const_cast<float*>(a.u);
+        b.steps = 1;
+        b.ckpt_every = 1;
+        b.g_final = a.g_out;
+        b.g_frames = nullptr;
+    }
+    const size_t smem = (size_t)b.ckpt_every * TPR * sizeof(float);
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_rollout_bwd_wide<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    k_rollout_bwd_wide<TPR><<<b.rows, TPR, smem, st>>>(b);
+    return check_launch("burgers_bwd_wide");
+}
+
+#define INC_BURGERS_BWD_WIDE_SHAPES(X) X(64) X(128) X(256) X(512)
 
 template <int CPT, int TPR>
 int launch_weno(const float* f, float* out, int rows, int n, int dir, cudaStream_t st, int block);

@@ -45,7 +45,7 @@ def cnn_supported(model, solver, u) -> bool:
             and _cnn_shape_ok(model)
             and isinstance(solver, BurgersSolverTorch) and solver.adaptive_CFL is None
             and isinstance(u, torch.Tensor) and u.is_cuda and u.dtype == torch.float32 and u.dim() == 2
-            and u.shape[1] in CNN_N and u.shape[1] == solver.resolution)
+            and u.shape[0] > 0 and u.shape[1] in CNN_N and u.shape[1] == solver.resolution)
 
 
 def pack_cnn_weights(model, device=None) -> torch.Tensor:

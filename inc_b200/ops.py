@@ -18,6 +18,8 @@ def weno_reconstruction(f: torch.Tensor, direction: str = "left") -> torch.Tenso
         raise ValueError("f must be a [rows, n] float32 CUDA tensor")
     f = f.contiguous()
     out = torch.empty_like(f)
+    if f.shape[0] == 0:  # no rows: nothing to launch
+        return out
     with torch.cuda.device(f.device):
         rc = nat.lib().inc_weno_reconstruct(f.data_ptr(), out.data_ptr(), f.shape[0], f.shape[1],
                                             0 if direction == "left" else 1, nat.stream_of(f.device))

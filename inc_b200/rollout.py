@@ -73,13 +73,17 @@ def burgers_rollout(solver: BurgersSolverTorch, u0, steps, s=None, ckpt_every=8)
     Differentiable w.r.t. u0 and s.  Advances ``solver.t`` by steps * dt."""
     if solver.adaptive_CFL is not None:
         raise ValueError("fused rollouts use a fixed dt; adaptive_CFL solvers step one call at a time")
+    _check_state(u0, solver.resolution)
     u0 = u0.contiguous()
-    launch = solver.launch_for(u0)
+    launch = solver.launch_for(u0) if u0.shape[0] else None
     s = _contig(s)
     if s is not None:
         _check_state(s, solver.resolution, "s")
     want = torch.is_grad_enabled() and (u0.requires_grad or (s is not None and s.requires_grad))
-    frames = BurgersRolloutFn.apply(u0, s, launch, int(steps), int(ckpt_every), want)
+    if u0.shape[0] == 0:  # an empty batch: nothing to launch
+        frames = u0.unsqueeze(1).expand(0, int(steps), u0.shape[1]).clone()
+    else:
+        frames = BurgersRolloutFn.apply(u0, s, launch, int(steps), int(ckpt_every), want)
     solver.t += steps * solver.dt
     return frames
 
@@ -88,10 +92,12 @@ def ks_rollout(solver: KSSolverTorch, u0, steps, domain_size, s=None, ckpt_every
     """Frames [B, steps, N] of `steps` KS step() calls in one launch (s held constant)."""
     _check_state(u0, solver.resolution)
     u0 = u0.contiguous()
-    plan = solver.plan_for(u0, domain_size)
     s = _contig(s)
     if s is not None:
         _check_state(s, solver.resolution, "s")
+    if u0.shape[0] == 0:  # an empty batch: nothing to launch
+        return u0.unsqueeze(1).expand(0, int(steps), u0.shape[1]).clone()
+    plan = solver.plan_for(u0, domain_size)
     want = torch.is_grad_enabled() and (u0.requires_grad or (s is not None and s.requires_grad))
     return KSRolloutFn.apply(u0, s, plan, int(steps), int(ckpt_every), want)
 

@@ -286,7 +286,11 @@ class BurgersSolverTorch:
         """Advance by dt (forward Euler, or SSP-RK3 when configured); solver_1d.py:181-195."""
         if self.adaptive_CFL is not None:
             return self.step_adaptive(u)
+        _check_state(u, self.resolution)
         u = u.contiguous()
+        if u.shape[0] == 0:  # an empty batch: nothing to launch
+            self.t += self.dt
+            return u.clone()
         launch = self.launch_for(u)
         s = _contig(self.correction_s)
         if s is not None:
@@ -463,6 +467,8 @@ class KSSolverTorch:
     def _step(self, u, domain_size, scheme):
         _check_state(u, self.resolution)
         u = u.contiguous()
+        if u.shape[0] == 0:  # an empty batch: nothing to launch
+            return u.clone()
         plan = self.plan_for(u, domain_size, scheme)
         s, cu = _contig(self.correction_s), _contig(self.correction_u)
         if s is not None:

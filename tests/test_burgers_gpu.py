@@ -196,6 +196,55 @@ def test_rollout_backward_matches_stepwise(cuda, scheme):
         assert rel_l2(x2.cpu().numpy(), x1.cpu().numpy()) < 1e-6
 
 
+_WARP_CPT = {64: 4, 128: 4, 256: 8, 512: 16}
+
+
+@pytest.mark.parametrize("n", [64, 128, 256, 512])
+@pytest.mark.parametrize("scheme", ["euler", "ssprk3"])
+@pytest.mark.parametrize("conv,eq", [("WENO", "viscosity"), ("WENO", "linear"), ("FDM", "learning")])
+def test_wide_adjoint_matches_warp_adjoint(cuda, n, scheme, conv, eq):
+    """The one-cell-per-thread adjoint (small batches) against the warp-layout
+    adjoint: a step's VJP and a checkpointed rollout's gradient w.r.t. u0 and
+    s, with per-row nu, the linear or forcing source and per-row time."""
+    from inc_b200.rollout import burgers_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    B, L, J = 5, 2 * math.pi, 2
+    g = torch.Generator().manual_seed(n + len(eq))
+    rnd = lambda *shape: torch.rand(*shape, generator=g).to(cuda)  # noqa: E731
+    u0 = torch.tensor(_rand_u0(B, n, n), dtype=torch.float32, device=cuda)
+    s0 = 0.05 * (rnd(B, n) - 0.5)
+    t0 = rnd(B, 1)
+
+    def solver(cpt):
+        sp = SimpleNamespace(resolution=n, dt=0.2 / n, x=torch.arange(n, device=cuda) * (L / n),
+                             adaptive_CFL=None, L=L, nu=0.005 + 0.02 * rnd(B, 1), device=cuda,
+                             convection_term=conv, equation_type=eq, batch_size=B, beta=rnd(B, 1) - 0.5, J=J,
+                             A=0.3 * rnd(B, J), omega=rnd(B, J), phi=6 * rnd(B, J),
+                             l=torch.randint(1, 4, (B, J), generator=g).float().to(cuda),
+                             time_scheme=scheme, cells_per_thread=cpt)
+        return sp
+
+    g_state = g.get_state()
+    out = []
+    for cpt in (1, _WARP_CPT[n]):
+        g.set_state(g_state)  # the same random parameters for both layouts
+        slv = BurgersSolverTorch(solver(cpt))
+        slv.t = t0.clone()
+        u = u0.clone().requires_grad_(True)
+        s = s0.clone().requires_grad_(True)
+        slv.correction_s = s
+        w = torch.sin(torch.arange(n, device=cuda) * 0.3)
+        step_g = torch.autograd.grad((slv.step(u) * w).sum(), (u, s))
+        slv.t = t0.clone()
+        fr = burgers_rollout(slv, u, 11, s=s, ckpt_every=4)
+        wf = torch.cos(torch.arange(11 * n, device=cuda).reshape(11, n) * 0.01)
+        roll_g = torch.autograd.grad((fr * wf).sum(), (u, s))
+        out.append(step_g + roll_g)
+    for a, b in zip(*out):
+        assert torch.isfinite(a).all()
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 2e-5
+
+
 def test_fd_check_fp64_oracle(cuda):
     """GPU adjoint vs FP64 central differences (h=1e-6) of the oracle, 3 SSP-RK3 steps."""
     from inc_b200.solvers import BurgersSolverTorch
