@@ -41,7 +41,7 @@ int dispatch(Kind kind, const Args& a, int cpt, cudaStream_t st) {
         // the adjoints' wide layout has one cell per thread; where it does not
         // apply (n, or a segment too large for shared memory) the warp layouts do
         const int K = kind == Kind::StepBwd ? 1 : a.ckpt_every;
-        const size_t seg = (size_t)K * n * sizeof(float);
+        const size_t seg = (size_t)3 * K * n * sizeof(float);
         if (is_pow2(n) && n >= 64 && n <= 512 && K >= 1) {
 #define INC_BW(T) \
             if (n == T && seg + bwd_wide_static_smem<T>() <= 227 * 1024) return launch_bwd_wide<T>(kind, a, st);

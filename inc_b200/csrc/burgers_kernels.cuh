@@ -735,8 +735,27 @@ INC_DEV void rhs_vjp_wide(const Args& a, const Ctx<1>& cx, float u, float v, flo
     if (a.src == INC_SRC_LINEAR) out = fmaf(cx.beta, v, out);
 }
 
+// The stages' adjoints in reverse (see advance_bwd) for one cell per thread,
+// given the step's stage inputs u, u1, u2 (u1, u2 unused for Euler).
+template <int TPR>
+INC_DEV void stages_bwd_wide(const Args& a, const Ctx<1>& cx, float u, float u1, float u2, float& gu, float& gs,
+                             WideAdjSmem<TPR>& sh, int g) {
+    const float dt = cx.dt;
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
+    float acc = 0.f;
+    for (int k = stages - 1; k >= 0; --k) {
+        float rv;
+        rhs_vjp_wide<TPR>(a, cx, k == 2 ? u2 : (k == 1 ? u1 : u), gu, rv, sh, g);
+        const float ka = rk3_a(k), kb = rk3_b(k);
+        gs += kb * dt * gu;
+        acc += ka * gu;
+        gu = kb * (gu + dt * rv);
+    }
+    gu += acc;
+}
+
 // advance_bwd for one cell per thread: the stage inputs replayed with the wide
-// forward, then the stages' adjoints in reverse (see advance_bwd).
+// forward, then the stages' adjoints in reverse.
 template <int TPR>
 INC_DEV void advance_bwd_wide(const Args& a, const Ctx<1>& cx, float u, float& gu, float& gs, float t,
                               WideAdjSmem<TPR>& sh, int& parity, int g) {
@@ -750,16 +769,7 @@ INC_DEV void advance_bwd_wide(const Args& a, const Ctx<1>& cx, float u, float& g
         if (k == 0) u1 = x[0];
         else u2 = x[0];
     }
-    float acc = 0.f;
-    for (int k = stages - 1; k >= 0; --k) {
-        float rv;
-        rhs_vjp_wide<TPR>(a, cx, k == 2 ? u2 : (k == 1 ? u1 : u), gu, rv, sh, g);
-        const float ka = rk3_a(k), kb = rk3_b(k);
-        gs += kb * dt * gu;
-        acc += ka * gu;
-        gu = kb * (gu + dt * rv);
-    }
-    gu += acc;
+    stages_bwd_wide<TPR>(a, cx, u, u1, u2, gu, gs, sh, g);
 }
 
 template <int CPT>
@@ -798,11 +808,12 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_wide(Args a, int single_step
 
 // Backward of a fused rollout (or of one step: ckpts = u, one one-step segment,
 // g_final = dL/du_new), one row per CTA and one cell per thread.  Each segment
-// is replayed from its checkpoint with the wide forward, every state going to
-// this thread's slot of `seg` ([step][cell], written and read by the same
-// thread), and then differentiated step by step, last first, by
-// advance_bwd_wide.  For small batches, where the warp layout's serial cells
-// per lane set the latency of every step.
+// is replayed from its checkpoint with the wide forward, the three stage inputs
+// of every step going to this thread's slots of `seg` ([step][stage][cell],
+// written and read by the same thread; the segment's last step runs only the
+// stages that give its stage inputs), and then differentiated step by step,
+// last first.  For small batches, where the warp layout's serial cells per lane
+// set the latency of every step.
 template <int TPR>
 __global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
     __shared__ WideAdjSmem<TPR> sh;
@@ -813,6 +824,8 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
     if (cx.has_s) cx.s[0] = __ldg(a.s + (int64_t)row * TPR + g);
     const int K = a.ckpt_every;
     const int nseg = (a.steps + K - 1) / K;
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
+    const float dt = cx.dt;
     const int64_t base = (int64_t)row * TPR + g;
     float gu = a.g_final ? __ldg(a.g_final + base) : 0.f;
     float gs = 0.f;
@@ -820,15 +833,23 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
     for (int sidx = nseg - 1; sidx >= 0; --sidx) {
         const int k0 = sidx * K;
         const int len = min(K, a.steps - k0);
-        float u[1] = {__ldg(a.ckpts + ((int64_t)row * nseg + sidx) * TPR + g)};
+        float x[1] = {__ldg(a.ckpts + ((int64_t)row * nseg + sidx) * TPR + g)}, r[1];
         for (int j = 0; j < len; ++j) {
-            seg[j * TPR + g] = u[0];
-            if (j + 1 < len) advance_wide<1, TPR>(a, cx, u, cx.t + (k0 + j) * cx.dt, sh.fw, parity, g);
+            const float t = cx.t + (k0 + j) * dt;
+            const float u0 = x[0];
+            seg[3 * j * TPR + g] = u0;
+            const int run = j + 1 < len ? stages : stages - 1;
+            for (int k = 0; k < run; ++k) {  // as advance_wide
+                full_rhs_wide<1, TPR>(a, cx, x, r, t + rk3_c(k) * dt, sh.fw, parity, g);
+                x[0] = stages == 1 ? x[0] + dt * r[0] : rk3_a(k) * u0 + rk3_b(k) * (x[0] + dt * r[0]);
+                if (k + 1 < stages) seg[(3 * j + 1 + k) * TPR + g] = x[0];
+            }
         }
         for (int j = len - 1; j >= 0; --j) {
             const int k = k0 + j;
             if (a.g_frames) gu += __ldg(a.g_frames + ((int64_t)row * a.steps + k) * TPR + g);
-            advance_bwd_wide<TPR>(a, cx, seg[j * TPR + g], gu, gs, cx.t + k * cx.dt, sh, parity, g);
+            stages_bwd_wide<TPR>(a, cx, seg[3 * j * TPR + g], seg[(3 * j + 1) * TPR + g],
+                                 seg[(3 * j + 2) * TPR + g], gu, gs, sh, g);
         }
     }
     a.g_u[base] = gu;
@@ -907,7 +928,7 @@ int launch_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
 #define INC_BURGERS_WIDE_SHAPES(X) X(1, 64) X(1, 128) X(1, 256) X(1, 512) X(2, 64) X(2, 128) X(2, 256)
 
 // Wide-row backward launchers (one cell per thread), instantiated in burgers_bwd_wide.cu.
-// The dynamic shared memory holds one segment's states: ckpt_every * n floats.
+// The dynamic shared memory holds one segment's stage inputs: 3 * ckpt_every * n floats.
 template <int TPR>
 int launch_bwd_wide(Kind kind, const Args& a, cudaStream_t st);
 
@@ -924,7 +945,7 @@ int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
         b.g_final = a.g_out;
         b.g_frames = nullptr;
     }
-    const size_t smem = (size_t)b.ckpt_every * TPR * sizeof(float);
+    const size_t smem = (size_t)3 * b.ckpt_every * TPR * sizeof(float);
     if (smem > 48 * 1024)
         cudaFuncSetAttribute(k_rollout_bwd_wide<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_rollout_bwd_wide<TPR><<<b.rows, TPR, smem, st>>>(b);
