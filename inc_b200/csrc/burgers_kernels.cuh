@@ -946,7 +946,7 @@ int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
         b.g_frames = nullptr;
     }
     const size_t smem = (size_t)3 * b.ckpt_every * TPR * sizeof(float);
-    if (smem > 48 * 1024)
+    if (smem + bwd_wide_static_smem<TPR>() > 48 * 1024)  // the 48 KB default covers static + dynamic
         cudaFuncSetAttribute(k_rollout_bwd_wide<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_rollout_bwd_wide<TPR><<<b.rows, TPR, smem, st>>>(b);
     return check_launch("burgers_bwd_wide");
