@@ -827,13 +827,19 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
     const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
     const float dt = cx.dt;
     const int64_t base = (int64_t)row * TPR + g;
+    // global loads are issued one step (g_frames) or one segment (ckpts) ahead
+    const float* gfr = a.g_frames ? a.g_frames + (int64_t)row * a.steps * TPR + g : nullptr;
+    const float* ckr = a.ckpts + (int64_t)row * nseg * TPR + g;
     float gu = a.g_final ? __ldg(a.g_final + base) : 0.f;
+    float gf = gfr ? __ldg(gfr + (int64_t)(a.steps - 1) * TPR) : 0.f;
+    float ck = __ldg(ckr + (int64_t)(nseg - 1) * TPR);
     float gs = 0.f;
     int parity = 0;
     for (int sidx = nseg - 1; sidx >= 0; --sidx) {
         const int k0 = sidx * K;
         const int len = min(K, a.steps - k0);
-        float x[1] = {__ldg(a.ckpts + ((int64_t)row * nseg + sidx) * TPR + g)}, r[1];
+        float x[1] = {ck}, r[1];
+        if (sidx > 0) ck = __ldg(ckr + (int64_t)(sidx - 1) * TPR);
         for (int j = 0; j < len; ++j) {
             const float t = cx.t + (k0 + j) * dt;
             const float u0 = x[0];
@@ -847,7 +853,10 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
         }
         for (int j = len - 1; j >= 0; --j) {
             const int k = k0 + j;
-            if (a.g_frames) gu += __ldg(a.g_frames + ((int64_t)row * a.steps + k) * TPR + g);
+            if (gfr) {
+                gu += gf;
+                if (k > 0) gf = __ldg(gfr + (int64_t)(k - 1) * TPR);
+            }
             stages_bwd_wide<TPR>(a, cx, seg[3 * j * TPR + g], seg[(3 * j + 1) * TPR + g],
                                  seg[(3 * j + 2) * TPR + g], gu, gs, sh, g);
         }
