@@ -52,7 +52,8 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--profile", nargs="?", const="ks", default=None,
-                    choices=["ks", "burgers_ragged", "burgers_plain", "ks_bwd", "burgers_cnn", "spectral_conv"],
+                    choices=["ks", "burgers_ragged", "burgers_plain", "burgers_plain_bwd", "ks_bwd", "burgers_cnn",
+                             "spectral_conv"],
                     help="a small case of one kernel for ncu (no JSON)")
     ap.add_argument("--profile-rows", type=int, default=1024, help="rows of the KS profile case")
     ap.add_argument("--tpp", type=int, default=None,
@@ -1056,6 +1057,20 @@ def profile_small(dev, which="ks", rows=1024, tpp=32):
         gy = torch.randn(B, W, N, device=dev, generator=g)
         for _ in range(2):
             spectral_conv1d(x, w_re, w_im, M, bias=bias, addend=add).backward(gy)
+        torch.cuda.synchronize()
+        return
+    if which == "burgers_plain_bwd":  # the same rollout differentiated (checkpoints every 8 steps)
+        from inc_b200.rollout import burgers_rollout
+        from inc_b200.solvers import BurgersSolverTorch
+        from inc_b200.workloads import burgers_plain_config
+        cfg = burgers_plain_config()
+        sp = SimpleNamespace(resolution=cfg["N"], dt=cfg["dt"], x=None, adaptive_CFL=None, L=cfg["L"], nu=cfg["nu"],
+                             device=dev, convection_term="WENO", equation_type="viscosity", batch_size=cfg["B"],
+                             time_scheme="ssprk3", cells_per_thread=1)
+        u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=dev)
+        for _ in range(2):
+            u = u0.clone().requires_grad_(True)
+            burgers_rollout(BurgersSolverTorch(sp), u, cfg["steps"], ckpt_every=8).square().mean().backward()
         torch.cuda.synchronize()
         return
     if which == "burgers_plain":
