@@ -241,14 +241,45 @@ extern "C" int inc_ks_rollout(const inc_ks_plan* p, const float* u0, const float
     return dispatch(Kind::Rollout, p, a, as_stream(stream));
 }
 
-extern "C" int inc_ks_rollout_bwd(const inc_ks_plan* p, const float* ckpts, const float* s, int32_t steps,
-                                  int32_t ckpt_every, const float* g_frames, const float* g_final, float* g_u0,
-                                  float* g_s, void* stream) {
+extern "C" int64_t inc_ks_rollout_bwd_work_size(const inc_ks_plan* p, int32_t ckpt_every) {
+    if (!p || p->npairs <= 0 || ckpt_every <= 0) return -1;
+    const int n = p->n;
+    const int T = p->threads_per_pair ? p->threads_per_pair : default_tpp(n);
+    if (!valid_shape(n, T)) return -1;
+    // one [ckpt_every][3][n] float2 slot per launched group (the launch's grid x groups per block)
+    const int gpb = pick_block(Kind::RolloutBwd, p->npairs, T, n, ckpt_every) / T;
+    const int64_t groups = (int64_t)((p->npairs + gpb - 1) / gpb) * gpb;
+    return groups * 3 * ckpt_every * n * (int64_t)sizeof(float2);
+}
+
+static int ks_rollout_bwd(const inc_ks_plan* p, const float* ckpts, const float* s, int32_t steps,
+                          int32_t ckpt_every, const float* g_frames, const float* g_final, float* g_u0, float* g_s,
+                          void* work, void* stream) {
     Args a;
     int rc = fill_args(p, a);
     if (rc) return rc;
     if (!ok_ptr(ckpts) || !ok_ptr(g_u0) || steps <= 0 || ckpt_every <= 0) { set_error("ks_rollout_bwd: bad arguments"); return INC_E_INVALID; }
     a.s = s; a.steps = steps; a.ckpt_every = ckpt_every; a.ckpts = const_cast<float*>(ckpts);
     a.g_frames = g_frames; a.g_final = g_final; a.g_u = g_u0; a.g_s = g_s;
+    a.stage = static_cast<float2*>(work);
     return dispatch(Kind::RolloutBwd, p, a, as_stream(stream));
+}
+
+extern "C" int inc_ks_rollout_bwd(const inc_ks_plan* p, const float* ckpts, const float* s, int32_t steps,
+                                  int32_t ckpt_every, const float* g_frames, const float* g_final, float* g_u0,
+                                  float* g_s, void* stream) {
+    return ks_rollout_bwd(p, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s, nullptr, stream);
+}
+
+extern "C" int inc_ks_rollout_bwd_ws(const inc_ks_plan* p, const float* ckpts, const float* s, int32_t steps,
+                                     int32_t ckpt_every, const float* g_frames, const float* g_final, float* g_u0,
+                                     float* g_s, void* work, int64_t work_bytes, void* stream) {
+    const int64_t need = inc_ks_rollout_bwd_work_size(p, ckpt_every);
+    if (need < 0) { set_error("ks_rollout_bwd_ws: bad plan or ckpt_every"); return INC_E_INVALID; }
+    if (!work || work_bytes < need || (reinterpret_cast<uintptr_t>(work) & 15u) != 0) {
+        set_error("ks_rollout_bwd_ws: work needs %lld bytes, 16-byte aligned (got %lld)", (long long)need,
+                  (long long)work_bytes);
+        return INC_E_INVALID;
+    }
+    return ks_rollout_bwd(p, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s, work, stream);
 }

@@ -535,6 +535,7 @@ struct Args {
     const float* dR;      // [rows] pi / L
     const float* coef;    // [rows][3][nhp]: exp(L dt), phi1, phi2
     const float2* tw;     // [N] FFT twiddles (layout of fft())
+    float2* stage;        // rollout backward scratch: per launched group [ckpt_every][3][N] (or null)
     int rows, n, npairs, scheme, split, dealias, steps, ckpt_every, nhp;
     float invN;
 };
@@ -754,10 +755,14 @@ INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
 
 // seg (optional): shared memory receiving the state at the start of every step,
 // in lane layout [step][m][t] (the backward replay).  ckpt_on: store checkpoints.
+// stg (optional, the backward replay): receives the physical states after a
+// step's first three half-substeps (ETRK2: xi1, x1, xi2; ETD1: x1 after the
+// first), in lane layout [step][3][m][t]; tail_skip half-substeps are left out
+// at the end (the last step's states are needed, its result is not).
 template <int P, int T>
 INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, const Buf<P, T>& buf,
                              const Twiddles<P, T>& tw, bool frames_on, int nseg, bool ckpt_on = true,
-                             float2* seg = nullptr) {
+                             float2* seg = nullptr, float2* stg = nullptr, int tail_skip = 0) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
@@ -794,7 +799,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
     int h = 0, step = 0, ck_left = 0, ck_idx = 0;
     bool stage2 = false;
 #pragma unroll 1
-    for (int it = steps * per_step; it > 0; --it) {
+    for (int it = steps * per_step - tail_skip; it > 0; --it) {
         if (h == 0) {
             if (ckpt_on && a.ckpts) {
                 if (ck_left == 0) {
@@ -834,6 +839,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
         fft_fwd<P, T>(v, buf, tw, t);
 #pragma unroll
         for (int m = 0; m < P; ++m) x[m] = cswap(v[m]);
+        if (stg && h < per_step - 1) st_put<P, T>(stg + (step * 3 + h) * N, x, t);
         if (rk2) stage2 = !stage2;
         if (++h == per_step) {
             if (frames_on) store_pair_strided<P, T>(a.frames, x, c, N, frame_stride, (int64_t)step * N);
@@ -904,20 +910,24 @@ INC_DEV void pair_mul2(float2 (&v)[P], const float2 (&x)[P], float s) {
 // the adjoint units  w2 = IFFT(d phi2 G) -> G -= FFT(2 xi w2)/N  and
 // Sacc += phi1 G, w1 = IFFT(d phi1 G) -> G = E G + FFT(2 x (w2 - w1))/N
 // (ETD1: the second unit alone with w2 = 0).
-template <int P, int T>
+//
+// STG: stg holds the step's states xi1, x1, xi2 (ETD1: x1) kept by the segment
+// replay in lane layout [3][m][t]; the replay units and FFT(x0) are skipped.
+template <int P, int T, bool STG = false>
 INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>& cc, const float2 (&SS)[P],
                               float2 (&G)[P], float2 (&Sacc)[P], const float* gframe, int64_t gf_row_stride,
-                              int64_t gf_off, const float2* x0s, float2* st, const Buf<P, T>& buf, const Twiddles<P, T>& tw) {
+                              int64_t gf_off, const float2* x0s, float2* st, const Buf<P, T>& buf, const Twiddles<P, T>& tw,
+                              const float2* stg = nullptr) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
-    float2* x1s = st;
-    float2* xi1s = st + N;
-    float2* xi2s = st + 2 * N;
+    const float2* x1s = STG ? stg + (rk2 ? N : 0) : st;
+    const float2* xi1s = STG ? stg : st + N;
+    const float2* xi2s = STG ? stg + 2 * N : st + 2 * N;
     float2* w2s = st + 3 * N;
     float2 X[P];
 #pragma unroll 1
-    for (int k = gframe ? 0 : 1; k < 2; ++k) {
+    for (int k = gframe ? 0 : 1; k < (STG ? 1 : 2); ++k) {
         float2 v[P];
         if (k == 0) load_pair_strided<P, T>(v, gframe, c, N, gf_row_stride, gf_off);
         else st_get<P, T>(v, x0s, t);
@@ -933,8 +943,8 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
     const int nrec = rk2 ? 3 : 1;
     const int nunits = nrec + (rk2 ? 4 : 2);
 #pragma unroll 1
-    for (int k = 0; k < nunits; ++k) {
-        const bool rec = k < nrec;
+    for (int k = STG ? nrec : 0; k < nunits; ++k) {
+        const bool rec = !STG && k < nrec;
         const int j = k - nrec;                        // adjoint unit
         const bool unit_w2 = rk2 && !rec && !(j & 1);  // w2 unit (ETRK2 only)
         const bool sub1 = rk2 ? j < 2 : j < 1;         // second substep first
@@ -1005,7 +1015,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
         if (rec) {
 #pragma unroll
             for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
-            st_put<P, T>(rk2 ? (k == 0 ? xi1s : (k == 1 ? x1s : xi2s)) : x1s, v, t);
+            st_put<P, T>(rk2 ? (k == 0 ? st + N : (k == 1 ? st : st + 2 * N)) : st, v, t);
         } else {
             if (a.split) to_split<P, T>(v, t, buf.a);
             if (unit_w2) {
@@ -1100,7 +1110,7 @@ __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
 
 // Backward of the fused rollout: each ckpt_every-step segment is replayed from
 // its checkpoint (states kept in shared memory), then differentiated step by step.
-template <int P, int T>
+template <int P, int T, bool STG>
 __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
@@ -1121,19 +1131,25 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
 #pragma unroll
     for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
     const int nseg = (a.steps + K - 1) / K;
+    // STG: this group's scratch for the replayed substep states (every launched group has one)
+    float2* stg = STG ? a.stage + (size_t)pair * 3 * K * N : nullptr;
     for (int sidx = nseg - 1; sidx >= 0; --sidx) {
         const int k0 = sidx * K;
         const int len = min(K, a.steps - k0);
         {
             float2 x[P];
             load_pair_strided<P, T>(x, a.ckpts, c, N, (int64_t)nseg * N, (int64_t)sidx * N);
-            forward_program<P, T>(a, c, x, len - 1, buf, tw, false, nseg, false, seg);
-            st_put<P, T>(seg + (len - 1) * N, x, t);
+            if (STG) {  // every step's start state and its substep states, the last step's result left out
+                forward_program<P, T>(a, c, x, len, buf, tw, false, nseg, false, seg, stg, 1);
+            } else {
+                forward_program<P, T>(a, c, x, len - 1, buf, tw, false, nseg, false, seg);
+                st_put<P, T>(seg + (len - 1) * N, x, t);
+            }
         }
         for (int j = len - 1; j >= 0; --j) {
             const int k = k0 + j;
-            step_bwd_program<P, T>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N,
-                                   seg + j * N, st, buf, tw);
+            step_bwd_program<P, T, STG>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N,
+                                        seg + j * N, st, buf, tw, STG ? stg + (size_t)j * 3 * N : nullptr);
         }
     }
     adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
@@ -1181,7 +1197,8 @@ int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     const int grid = (a.npairs + gpb - 1) / gpb;
     const size_t smem = smem_bytes<P, T>(kind, block, a.ckpt_every);
     if (kind == Kind::StepBwd) return launch_with_smem(k_step_bwd<P, T>, grid, block, smem, st, a);
-    return launch_with_smem(k_rollout_bwd<P, T>, grid, block, smem, st, a);
+    if (a.stage) return launch_with_smem(k_rollout_bwd<P, T, true>, grid, block, smem, st, a);
+    return launch_with_smem(k_rollout_bwd<P, T, false>, grid, block, smem, st, a);
 }
 
 

@@ -360,12 +360,31 @@ class KSPlan:
                                           nat.ptr(u_final), ckpt_every, nat.ptr(ckpts), nat.stream_of(self.device))
         nat.check(rc, "inc_ks_rollout")
 
-    def rollout_bwd(self, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s):
+    def rollout_bwd(self, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s, work=None):
+        """The rollout's VJP.  ``work`` (default: allocated here) is the device
+        scratch of ``rollout_bwd_work_size(ckpt_every)`` bytes in which the
+        segment replay keeps the substep states; ``work=False`` rebuilds them
+        per step instead (fewer bytes, more transforms)."""
         with torch.cuda.device(self.device):
-            rc = nat.lib().inc_ks_rollout_bwd(C.byref(self.c), ckpts.data_ptr(), nat.ptr(s), steps, ckpt_every,
-                                              nat.ptr(g_frames), nat.ptr(g_final), g_u0.data_ptr(), nat.ptr(g_s),
-                                              nat.stream_of(self.device))
+            if work is False:
+                rc = nat.lib().inc_ks_rollout_bwd(C.byref(self.c), ckpts.data_ptr(), nat.ptr(s), steps, ckpt_every,
+                                                  nat.ptr(g_frames), nat.ptr(g_final), g_u0.data_ptr(), nat.ptr(g_s),
+                                                  nat.stream_of(self.device))
+            else:
+                if work is None:
+                    work = torch.empty(self.rollout_bwd_work_size(ckpt_every), dtype=torch.uint8, device=self.device)
+                rc = nat.lib().inc_ks_rollout_bwd_ws(C.byref(self.c), ckpts.data_ptr(), nat.ptr(s), steps,
+                                                     ckpt_every, nat.ptr(g_frames), nat.ptr(g_final),
+                                                     g_u0.data_ptr(), nat.ptr(g_s), work.data_ptr(), work.numel(),
+                                                     nat.stream_of(self.device))
         nat.check(rc, "inc_ks_rollout_bwd")
+
+    def rollout_bwd_work_size(self, ckpt_every):
+        """Bytes of device scratch rollout_bwd uses for this plan and ckpt_every."""
+        n = int(nat.lib().inc_ks_rollout_bwd_work_size(C.byref(self.c), int(ckpt_every)))
+        if n < 0:
+            raise ValueError(f"ckpt_every must be positive (got {ckpt_every})")
+        return n
 
 
 class KSStepFn(torch.autograd.Function):

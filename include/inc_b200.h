@@ -244,6 +244,16 @@ int inc_ks_rollout(const inc_ks_plan* plan, const float* u0, const float* s,
 int inc_ks_rollout_bwd(const inc_ks_plan* plan, const float* ckpts, const float* s,
                        int32_t steps, int32_t ckpt_every, const float* g_frames,
                        const float* g_final, float* g_u0, float* g_s, void* stream);
+/* inc_ks_rollout_bwd with a caller-owned device scratch of
+ * inc_ks_rollout_bwd_work_size(plan, ckpt_every) bytes (16-byte aligned; -1 for
+ * a bad plan or ckpt_every).  The segment replay keeps every step's substep
+ * states there, so the adjoint does not rebuild them: 17 instead of 24 row-pair
+ * transforms per step() (ETRK2).  Same results to rounding.                    */
+int64_t inc_ks_rollout_bwd_work_size(const inc_ks_plan* plan, int32_t ckpt_every);
+int inc_ks_rollout_bwd_ws(const inc_ks_plan* plan, const float* ckpts, const float* s,
+                          int32_t steps, int32_t ckpt_every, const float* g_frames,
+                          const float* g_final, float* g_u0, float* g_s, void* work,
+                          int64_t work_bytes, void* stream);
 
 /* ---- analysis -------------------------------------------------------------- */
 /* Energy spectrum of each of `rows` real rows of length n (a power of two in

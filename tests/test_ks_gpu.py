@@ -183,6 +183,39 @@ def test_rollout_backward_matches_stepwise(cuda, mixed):
         assert rel_l2(x2.cpu().numpy(), x1.cpu().numpy()) < 1e-6
 
 
+@pytest.mark.parametrize("N,tpp", [(16, 4), (64, 16), (128, 32), (256, 32), (256, 64), (512, 32)])
+@pytest.mark.parametrize("scheme", ["ETRK2", "ETD1"])
+def test_rollout_backward_scratch_matches_rebuild(cuda, N, tpp, scheme):
+    """The rollout backward that keeps the segment replay's substep states in
+    device scratch against the one that rebuilds them per step: odd batch (a
+    lone row), a short last segment, frame and final-state adjoints."""
+    B, steps, K = 7, 11, 4
+    dt = 0.2 if scheme == "ETRK2" else 0.05
+    Ls = [40.0 + 9 * i for i in range(B)]
+    solver = _solver(N, dt, scheme, Ls, tpp=tpp)
+    u0 = torch.tensor(_u0(B, N, Ls, 5), dtype=torch.float32, device=cuda)
+    g = torch.Generator(device=cuda).manual_seed(N + tpp)
+    s = 0.01 * torch.randn(B, N, device=cuda, generator=g)
+    ds = torch.tensor(Ls, device=cuda)
+    plan = solver.plan_for(u0, ds)
+    frames = torch.empty(B, steps, N, device=cuda)
+    ck = torch.empty(B, (steps + K - 1) // K, N, device=cuda)
+    plan.rollout(u0, s, steps, frames, None, K, ck)
+    gf = torch.randn(B, steps, N, device=cuda, generator=g)
+    gfin = torch.randn(B, N, device=cuda, generator=g)
+    out = []
+    for work in (None, False):
+        gu, gs = torch.empty_like(u0), torch.empty_like(u0)
+        plan.rollout_bwd(ck, s, steps, K, gf, gfin, gu, gs, work=work)
+        out.append((gu, gs))
+    for a, b in zip(*out):
+        assert torch.isfinite(a).all()
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-5
+    small = torch.empty(plan.rollout_bwd_work_size(K) - 16, dtype=torch.uint8, device=cuda)
+    with pytest.raises((ValueError, RuntimeError)):
+        plan.rollout_bwd(ck, s, steps, K, gf, gfin, gu, gs, work=small)
+
+
 def test_fd_check_fp64_oracle(cuda):
     N, B, dt, steps = 64, 3, 0.25, 2
     Ls = [64.0, 64.0, 50.0]
