@@ -67,3 +67,22 @@ def test_struct_layouts():
     assert C.sizeof(nat.BurgersDesc) == 8 * 4 + 4 * 4 + 5 * 8
     assert C.sizeof(nat.KSPlan) == 8 * 4 + 8 + 8
     assert C.sizeof(nat.BurgersRaggedDesc) == 4 * 4 + 6 * 8
+
+
+def test_ks_rollout_bwd_work_size_needs_no_gpu(lib):
+    """The KS backward's scratch size: one [ckpt_every][3][n] complex slot per
+    launched row-pair group, computed on the host from the plan's shape."""
+    from inc_b200 import _native as nat
+    p = nat.KSPlan()
+    p.rows, p.n, p.npairs, p.threads_per_pair = 1024, 256, 512, 32
+    # 512 pairs of 32 lanes launch one group per 32-thread block: 512 groups
+    assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 8) == 512 * 3 * 8 * 256 * 8
+    assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 0) == -1
+    p.threads_per_pair = 64  # a pair spans two warps, one group per block
+    assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 4) == 512 * 3 * 4 * 256 * 8
+    p.npairs = 0  # not initialised
+    assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 8) == -1
+    # the scratch entry point rejects a missing or short scratch before any CUDA call
+    p.npairs = 512
+    assert lib.inc_ks_rollout_bwd_ws(C.byref(p), None, None, 1, 8, None, None, None, None, None, 0,
+                                     None) == nat.INC_E_INVALID
