@@ -949,6 +949,11 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
         const bool unit_w2 = rk2 && !rec && !(j & 1);  // w2 unit (ETRK2 only)
         const bool sub1 = rk2 ? j < 2 : j < 1;         // second substep first
         float2 v[P];
+        // STG: the adjoint unit's state is loaded from scratch before its first
+        // transform, so the load overlaps the transform
+        float2 u[P];
+        if (STG)
+            st_get<P, T>(u, unit_w2 ? (sub1 ? xi2s : xi1s) : (sub1 ? x1s : x0s), t);
         // ---- operand of the first transform
         if (rec) {
             st_get<P, T>(v, k == 0 ? x0s : (k == 1 ? xi1s : x1s), t);
@@ -990,15 +995,14 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
 #pragma unroll
             for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
         } else {
-            float2 u[P];
 #pragma unroll
             for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);  // w2 or w1
             if (unit_w2) {
                 st_put<P, T>(w2s, v, t);
-                st_get<P, T>(u, sub1 ? xi2s : xi1s, t);
+                if (!STG) st_get<P, T>(u, sub1 ? xi2s : xi1s, t);
                 pair_mul2<P, T>(v, u, 2.f);
             } else {
-                st_get<P, T>(u, sub1 ? x1s : x0s, t);
+                if (!STG) st_get<P, T>(u, sub1 ? x1s : x0s, t);
                 if (rk2) {
                     float2 w2[P];
                     st_get<P, T>(w2, w2s, t);
