@@ -559,7 +559,7 @@ def bench_diff(args, dev, world, which):
     from inc_b200.correctors import FNO1D, PeriodicCNN1D
     from inc_b200.rollout import simulate_rollout
     from inc_b200.solvers import BurgersSolverTorch, KSSolverTorch
-    from inc_b200.sharding import allreduce_mean_
+    from inc_b200.sharding import average_gradients_
     from inc_b200.workloads import burgers_diff_config, ks_diff_config
 
     # data-parallel over ranks: every rank trains the same seeded network on its own seeded
@@ -604,7 +604,7 @@ def bench_diff(args, dev, world, which):
         loss = torch.mean((res - target) ** 2)
         loss.backward()
         if world > 1:
-            allreduce_mean_([p.grad for p in net.parameters()])
+            average_gradients_(net.parameters(), local_rows=B)
         opt.step()
         opt.zero_grad(set_to_none=False)
         return loss

@@ -28,10 +28,13 @@ constexpr int kMaxDevices = 64;
 float* g_area_ptr[kMaxDevices] = {};
 std::mutex g_area_mu;
 
-// Device address of g_ckpt_area on the current device, looked up once per
-// device.  In host code the array's name is only a host-side stand-in, so the
-// kernels must be given this address.
-int area_on_current_device(float** out) {
+// Device address of g_ckpt_area in the current context.  In host code the
+// array's name is only a host-side stand-in, so the kernels must be given this
+// address.  It is looked up again on every call whose stream is not capturing
+// (the context may have been reset, or be another one than last time, and the
+// module then lives at another address); a call on a capturing stream uses the
+// address the last uncapturing call on this device found.
+int area_on_current_device(cudaStream_t st, float** out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) {
@@ -42,8 +45,13 @@ int area_on_current_device(float** out) {
         inc::set_error("rollout_grad_noalloc: device %d out of range", dev);
         return INC_E_UNSUPPORTED;
     }
+    cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) {
+        cudaGetLastError();  // e.g. the legacy stream while another stream captures
+        cap = cudaStreamCaptureStatusActive;
+    }
     std::lock_guard<std::mutex> lock(g_area_mu);
-    if (!g_area_ptr[dev]) {
+    if (cap == cudaStreamCaptureStatusNone) {
         float* p = nullptr;
         e = cudaGetSymbolAddress(reinterpret_cast<void**>(&p), g_ckpt_area);
         if (e != cudaSuccess || p == nullptr) {
@@ -51,6 +59,9 @@ int area_on_current_device(float** out) {
             return INC_E_LAUNCH;
         }
         g_area_ptr[dev] = p;
+    } else if (!g_area_ptr[dev]) {
+        inc::set_error("rollout_grad_noalloc: the first call on device %d must come before stream capture", dev);
+        return INC_E_INVALID;
     }
     *out = g_area_ptr[dev];
     return INC_OK;
@@ -80,10 +91,10 @@ extern "C" int inc_burgers_rollout_grad_noalloc(const inc_burgers_desc* d, const
                   (long long)need, INC_NOALLOC_CKPT_FLOATS);
         return INC_E_INVALID;
     }
-    float* area = nullptr;
-    rc = area_on_current_device(&area);
-    if (rc) return rc;
     cudaStream_t st = as_stream(stream);
+    float* area = nullptr;
+    rc = area_on_current_device(st, &area);
+    if (rc) return rc;
     // forward: frames / final state for the caller, checkpoints into the area
     a.u = u0; a.s = s; a.t_rows = t_rows; a.t0 = (float)t0; a.steps = steps; a.frames = frames; a.out = u_final;
     a.ckpt_every = ckpt_every; a.ckpts = area;

@@ -170,9 +170,12 @@ int inc_burgers_ragged_rollout(const inc_burgers_ragged_desc* d,
  * nothing: the caller passes only inputs (u0, s, t, g_frames, g_final) and
  * outputs (frames and u_final may be NULL; g_u0 required, g_s may be NULL).
  * Limit: rows * ceil(steps / ckpt_every) * n <= INC_NOALLOC_CKPT_FLOATS, else
- * INC_E_INVALID.  The first call on a device looks the array's device address
- * up once (cudaGetSymbolAddress), so make that first call before any stream
- * capture on that device.  All calls share the one array, which keeps
+ * INC_E_INVALID.  A call looks the array's device address up in the current
+ * context (cudaGetSymbolAddress) unless its stream is capturing; a capturing
+ * call reuses the address the last call on that device found, so make the
+ * first call on a device, and the first one after a context reset
+ * (cudaDeviceReset) or a switch to another context, before any stream capture
+ * there.  All calls share the one array, which keeps
  * the last call's checkpoints; each call writes every checkpoint before it
  * reads it, so nothing needs clearing, but calls that overlap on the GPU (on
  * different streams) race on it.  No counterpart in the reference.          */

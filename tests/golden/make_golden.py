@@ -1,9 +1,10 @@
 """Generate golden vectors by running the reference's own 1D solvers in FP64.
 
-Run from the repository root in a container where the reference tree is
-mounted (default ``/root/reference``; override with ``INC_REFERENCE``):
+Run from the repository root with the path of a checkout of the reference
+(``--reference PATH``, or the ``INC_REFERENCE`` environment variable; there is
+no default):
 
-    python tests/golden/make_golden.py
+    python tests/golden/make_golden.py --reference PATH
 
 It imports ``solvers/solver_1d.py`` from the reference (never copied), runs it
 with ``torch.set_default_dtype(torch.float64)`` on seeded inputs, and writes
@@ -27,60 +28,67 @@ from types import SimpleNamespace
 import numpy as np
 import torch
 
-REF = os.environ.get("INC_REFERENCE", "/root/reference")
+REF = None  # the reference checkout, set by main()
 OUT = os.path.dirname(os.path.abspath(__file__))
+BurgersSolverTorch = KSSolverTorch = weno_reconstruction = _FixedBurgers = None
 
 
-def _import_reference():
+def _import_reference(ref):
+    """Import the reference's solvers/solver_1d.py from the checkout at `ref` and
+    bind the module-level names the generators use."""
+    global REF, BurgersSolverTorch, KSSolverTorch, weno_reconstruction, _FixedBurgers
+    REF = os.path.abspath(ref)
+    if not os.path.isfile(os.path.join(REF, "solvers", "solver_1d.py")):
+        raise SystemExit(f"{REF} is not a checkout of the reference (no solvers/solver_1d.py)")
     if REF not in sys.path:
         sys.path.insert(0, REF)
     from solvers.solver_1d import BurgersSolverTorch, KSSolverTorch, weno_reconstruction
-    return BurgersSolverTorch, KSSolverTorch, weno_reconstruction
+    _FixedBurgers = _fixed_burgers(BurgersSolverTorch)
 
 
-BurgersSolverTorch, KSSolverTorch, weno_reconstruction = _import_reference()
+def _fixed_burgers(base):
+    class _FixedBurgers(base):
+        """Reference solver with the ``_apply_corrections`` call fixed."""
 
+        def rhs_at(self, u, t):
+            saved = self.t
+            self.t = t
+            source = self._compute_source(u)
+            self.t = saved
+            source = self._apply_corrections(source)
+            return self.calc_nonlinear(u) + self.calc_linear(u) + source
 
-class _FixedBurgers(BurgersSolverTorch):
-    """Reference solver with the ``_apply_corrections`` call fixed."""
+        def step(self, u):
+            if self.adaptive_CFL is not None:
+                return self.step_adaptive(u)
+            u_new = u + self.dt * self.rhs_at(u, self.t)
+            self.t += self.dt
+            return u_new
 
-    def rhs_at(self, u, t):
-        saved = self.t
-        self.t = t
-        source = self._compute_source(u)
-        self.t = saved
-        source = self._apply_corrections(source)
-        return self.calc_nonlinear(u) + self.calc_linear(u) + source
+        def step_rk3(self, u):
+            dt, t = self.dt, self.t
+            u1 = u + dt * self.rhs_at(u, t)
+            u2 = 0.75 * u + 0.25 * (u1 + dt * self.rhs_at(u1, t + dt))
+            u3 = (1.0 / 3.0) * u + (2.0 / 3.0) * (u2 + dt * self.rhs_at(u2, t + 0.5 * dt))
+            self.t = t + dt
+            return u3
 
-    def step(self, u):
-        if self.adaptive_CFL is not None:
-            return self.step_adaptive(u)
-        u_new = u + self.dt * self.rhs_at(u, self.t)
-        self.t += self.dt
-        return u_new
+        def step_adaptive(self, u):
+            target, substeps = self.dt, 0
+            while target > 0:
+                max_u = torch.max(torch.abs(u))
+                allowed = self.adaptive_CFL * self.dx / max_u.item() if max_u.item() > 0 else target
+                dt_local = min(target, allowed)
+                u = u + dt_local * self.rhs_at(u, self.t)
+                self.t += dt_local
+                target -= dt_local
+                if int(math.ceil(target / dt_local)) > 1000:
+                    break
+                substeps += 1
+            self.substeps = substeps
+            return u
 
-    def step_rk3(self, u):
-        dt, t = self.dt, self.t
-        u1 = u + dt * self.rhs_at(u, t)
-        u2 = 0.75 * u + 0.25 * (u1 + dt * self.rhs_at(u1, t + dt))
-        u3 = (1.0 / 3.0) * u + (2.0 / 3.0) * (u2 + dt * self.rhs_at(u2, t + 0.5 * dt))
-        self.t = t + dt
-        return u3
-
-    def step_adaptive(self, u):
-        target, substeps = self.dt, 0
-        while target > 0:
-            max_u = torch.max(torch.abs(u))
-            allowed = self.adaptive_CFL * self.dx / max_u.item() if max_u.item() > 0 else target
-            dt_local = min(target, allowed)
-            u = u + dt_local * self.rhs_at(u, self.t)
-            self.t += dt_local
-            target -= dt_local
-            if int(math.ceil(target / dt_local)) > 1000:
-                break
-            substeps += 1
-        self.substeps = substeps
-        return u
+    return _FixedBurgers
 
 
 def burgers_params(rng, B, N, *, eq="viscosity", conv="WENO", nu_rows=False, J=3,
@@ -407,11 +415,24 @@ def make_analysis_and_data():
     np.savez_compressed(os.path.join(OUT, "analysis_data_golden.npz"), **out)
 
 
-if __name__ == "__main__":
+def main():
+    import argparse
+    gens = {"burgers": make_burgers, "ks": make_ks, "hybrid": make_hybrid, "analysis_data": make_analysis_and_data}
+    ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
+    ap.add_argument("--reference", default=os.environ.get("INC_REFERENCE"),
+                    help="checkout of the reference (default: $INC_REFERENCE; required)")
+    ap.add_argument("--only", nargs="+", choices=sorted(gens), default=sorted(gens),
+                    help="golden files to (re)generate (default: all)")
+    args = ap.parse_args()
+    if not args.reference:
+        ap.error("the reference checkout is required: --reference PATH or INC_REFERENCE=PATH")
+    _import_reference(args.reference)
     torch.set_default_dtype(torch.float64)
-    make_burgers()
-    make_ks()
-    make_hybrid()
-    make_analysis_and_data()
-    for f in ("burgers_golden.npz", "ks_golden.npz", "hybrid_golden.npz", "analysis_data_golden.npz"):
+    for name in args.only:
+        gens[name]()
+        f = f"{name}_golden.npz"
         print(f, os.path.getsize(os.path.join(OUT, f)), "bytes")
+
+
+if __name__ == "__main__":
+    main()

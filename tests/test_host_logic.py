@@ -18,7 +18,7 @@ def _free_port():
 
 def _shard(rank):
     g = torch.Generator().manual_seed(100 + rank)
-    return torch.randn(3, 16, generator=g, dtype=torch.float64)
+    return torch.randn(3 + 2 * rank, 16, generator=g, dtype=torch.float64)  # unequal shards: 3 and 5 rows
 
 
 def _rank_main(rank, world, port, out_dir):
@@ -37,13 +37,24 @@ def _rank_main(rank, world, port, out_dir):
     t = max_over_ranks(1.0 + rank)
     # data-parallel corrector gradients: each rank's mean loss over its own shard, averaged
     from inc_b200.correctors import PeriodicCNN1D
-    from inc_b200.sharding import allreduce_mean_
+    from inc_b200.sharding import allreduce_mean_, average_gradients_
     torch.manual_seed(0)
     net = PeriodicCNN1D(channels=4).double()
-    net(_shard(rank)).square().mean().backward()
-    allreduce_mean_([p.grad for p in net.parameters()] + [None])
+    x = _shard(rank)
+    net(x).square().mean().backward()
+    if rank == 1:  # a parameter that took no part in this rank's loss has no gradient here
+        net.convs[0].bias.grad = None
+    average_gradients_(net.parameters(), local_rows=x.shape[0])
     grads = [p.grad.clone() for p in net.parameters()]
-    torch.save({"full": full, "t": t, "parts": parts, "grads": grads}, os.path.join(out_dir, f"rank{rank}.pt"))
+    try:
+        allreduce_mean_([grads[0], None])
+        none_rejected = False
+    except ValueError:
+        none_rejected = True
+    pair = [torch.full((2,), float(rank + 1), dtype=torch.float64)]
+    allreduce_mean_(pair)
+    torch.save({"full": full, "t": t, "parts": parts, "grads": grads, "none_rejected": none_rejected,
+                "pair": pair[0], "bias_grad0": net.convs[0].bias.grad is not None}, os.path.join(out_dir, f"rank{rank}.pt"))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -62,14 +73,22 @@ def test_sharding_gloo_world2(tmp_path):
     assert sorted(p[0] + p[1]) == list(range(37)) and res[1]["parts"] == p
     loads = [sum(int(cfg["n"][i]) for i in q) for q in p]
     assert max(loads) - min(loads) <= 512                      # within one largest row
-    # averaged shard gradients == the gradient of the mean loss over the whole batch
+    # row-weighted shard gradients == the gradient of the mean loss over the whole batch,
+    # also where one rank had no gradient for a parameter: that rank's share counts as zero
     from inc_b200.correctors import PeriodicCNN1D
     torch.manual_seed(0)
     net = PeriodicCNN1D(channels=4).double()
     net(torch.cat([_shard(r) for r in range(world)])).square().mean().backward()
+    torch.manual_seed(0)
+    net0 = PeriodicCNN1D(channels=4).double()
+    net0(_shard(0)).square().mean().backward()
+    rows0, rows = _shard(0).shape[0], sum(_shard(r).shape[0] for r in range(world))
     for r in res:
-        for g, p in zip(r["grads"], net.parameters()):
-            torch.testing.assert_close(g, p.grad, rtol=1e-12, atol=1e-14)
+        assert r["none_rejected"] and r["bias_grad0"]
+        assert torch.equal(r["pair"], torch.full((2,), 1.5, dtype=torch.float64))
+        for i, (g, p) in enumerate(zip(r["grads"], net.parameters())):
+            want = p.grad if i != 1 else net0.convs[0].bias.grad * rows0 / rows
+            torch.testing.assert_close(g, want, rtol=1e-12, atol=1e-14)
 
 
 def test_partition_properties():

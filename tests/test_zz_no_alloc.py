@@ -70,9 +70,11 @@ def test_noalloc_matches_allocating_entry_points_twice(cuda):
     from inc_b200 import _native as nat
     lib = nat.lib()
     stream = nat.stream_of(cuda)
-    # two different problems in a row: the second call reuses the area the first filled
+    # different problems in a row: each call reuses the area the previous one filled.  At most
+    # 148 rows take the one-row-per-CTA kernels, more rows the warp-per-row ones.
     for call, (rows, n, steps, k, scheme, seed) in enumerate([(64, 256, 40, 8, "ssprk3", 1),
-                                                               (37, 128, 29, 5, "euler", 2)]):
+                                                               (37, 128, 29, 5, "euler", 2),
+                                                               (300, 256, 16, 8, "ssprk3", 3)]):
         d = _desc(nat, rows, n, 0.004, 0.01, scheme)
         u0, s, gf, gl = _inputs(rows, n, steps, seed, cuda)
         fr_a, gu_a, gs_a = _allocating(lib, nat, d, u0, s, gf, gl, steps, k, stream)
