@@ -2,7 +2,7 @@
 """Benchmark of the INC 1D hybrid time-stepper on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload ks_plain|burgers_plain|burgers_batched]
+                    [--workload ks_plain|burgers_plain|burgers_batched|burgers_diff|ks_diff]
 
 Metric: cell-steps/s (one grid point advanced by one reference step()).
 Default workload: the plain KS configuration - 1024 trajectories, N=256,
@@ -20,7 +20,16 @@ Printed (rank 0, one JSON line):
   roofline   - the fused kernel's FP32 throughput against an FMA-loop peak
                measured in this run;
   cpu_baseline - the FP32 numpy port of the reference (oracle/) on the host
-               cores, on a bounded sample.
+               cores, on a bounded sample;
+  error      - the timed launch's own frames against the FP64 oracle on the
+               same inputs (relative L2 at 1, 10 and 20 step() calls);
+  configs    - (default run) the other four configurations, each measured
+               the same way with fewer timed repeats: Burgers plain (32 x 128,
+               200 SSP-RK3 steps), the ragged batch (4096 rows, 500 steps),
+               and the two differentiable training steps (Burgers 256 x 256
+               with the CNN corrector, KS 512 x 512 with the FNO corrector),
+               each with its fused-over-per-step ratios, roofline, e2e and
+               error against FP64.
 Multi-GPU (torchrun): every rank runs the full workload on its own GPU (weak
 scaling, trajectories are independent, no data-path collective).
 """
@@ -50,6 +59,9 @@ def parse_args():
     ap.add_argument("--workload", choices=["ks_plain", "burgers_plain", "burgers_batched", "burgers_diff", "ks_diff"],
                     default="ks_plain")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true",
+                    help="the default workload only (no compact blocks of the other configurations)")
+    ap.add_argument("--extra-steps", type=int, default=3, help="timed repeats of each compact block")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--profile", nargs="?", const="ks", default=None,
                     choices=["ks", "burgers_ragged", "burgers_plain", "burgers_plain_bwd", "ks_bwd", "burgers_cnn",
@@ -200,6 +212,59 @@ def event_time(fn, iters, flush=None):
     return times
 
 
+def ks_error_vs_fp64(frames, cfg, horizons=(1, 10, 20)):
+    """Relative L2 error of a KS launch's frames (all rows) against the FP64 oracle
+    (oracle/ks.py) run on the same seeded inputs, at the given step() counts.  The
+    chaotic dynamics amplify rounding, so the 1e-5 bar holds to a horizon of 20."""
+    import numpy as np
+    from oracle import ks as oks
+    H = max(horizons)
+    got = frames[:, :H].double().cpu().numpy()
+    B, N, L, dt = cfg["B"], cfg["N"], cfg["L"], cfg["dt"]
+    coeffs = oks.coefficients_fp64([L] * B, N, dt, cfg["scheme"], np.float64)
+    ref, out = np.asarray(cfg["u0"], dtype=np.float64), {}
+    for k in range(1, H + 1):
+        ref = oks.step(ref, [L] * B, dt, cfg["scheme"], cfg["s"], None, coeffs)
+        if k in horizons:
+            out[str(k)] = float(np.linalg.norm(got[:, k - 1] - ref) / np.linalg.norm(ref))
+    return {"rel_l2_at_step": out, "rows": B, "tol": 1e-5,
+            "vs": "FP64 oracle (oracle/ks.py) on the same seeded inputs, frames of the timed launch"}
+
+
+def burgers_error_vs_fp64(frames, cfg):
+    """Relative L2 error over all rows and frames of a Burgers rollout against the FP64 oracle."""
+    import numpy as np
+    from oracle import burgers as ob
+    p = ob.BurgersParams(resolution=cfg["N"], L=cfg["L"], dt=cfg["dt"], nu=cfg["nu"])
+    ref = ob.rollout(np.asarray(cfg["u0"], dtype=np.float64), p, cfg["steps"], cfg["scheme"])
+    got = frames.double().cpu().numpy()
+    return {"rel_l2_all_frames": float(np.linalg.norm(got - ref) / np.linalg.norm(ref)), "rows": cfg["B"],
+            "steps": cfg["steps"], "tol": 1e-5,
+            "vs": "FP64 oracle (oracle/burgers.py) on the same seeded inputs, frames of the timed launch"}
+
+
+def ragged_error_vs_fp64(final_rows, cfg, sample=64, seed=7):
+    """Relative L2 error of the ragged launch's final states on a seeded subset of rows against
+    the FP64 oracle (rows of one width advanced together, per-row nu and dt)."""
+    import numpy as np
+    from oracle import burgers as ob
+    ns = np.asarray(cfg["n"])
+    sub = sorted(np.random.default_rng(seed).choice(cfg["rows"], sample, replace=False).tolist())
+    num = den = 0.0
+    for n in sorted(set(ns[sub].tolist())):
+        idx = [r for r in sub if ns[r] == n]
+        u = np.stack([cfg["u0"][r] for r in idx]).astype(np.float64)
+        p = ob.BurgersParams(resolution=int(n), L=2 * np.pi, dt=0.0, nu=cfg["nu"][idx][:, None])
+        dt = cfg["dt"][idx][:, None]
+        for _ in range(cfg["steps"]):
+            u, _ = ob.step_ssprk3(u, p, 0.0, None, dt)
+        got = np.stack([final_rows[r] for r in idx]).astype(np.float64)
+        num += float(np.sum((got - u) ** 2))
+        den += float(np.sum(u ** 2))
+    return {"rel_l2_final": (num / den) ** 0.5, "rows": sample, "steps": cfg["steps"], "tol": 1e-5,
+            "vs": f"FP64 oracle (oracle/burgers.py) on {sample} seeded rows of the timed launch's final state"}
+
+
 def fp32_peak_tflops(device):
     """FP32 FMA throughput of this GPU, measured with inc_bench_fma."""
     import torch
@@ -270,6 +335,7 @@ def bench_ks(args, dev, world):
     if world > 1:
         torch.distributed.barrier()
     ms_fused = sum(t_fused) / len(t_fused)
+    error = ks_error_vs_fp64(frames, cfg)  # the timed launch's own frames, outside the timed region
 
     # --- the same rollout with the opt-in 2/3-rule truncation (the reference's "3/2 padding"
     # is a physical-space no-op, so the headline runs without it, as the reference does)
@@ -385,6 +451,7 @@ def bench_ks(args, dev, world):
                         "note": "flops this kernel executes: two rows per complex FFT, FFT(s) once per launch"},
         plain_hbm_gbs=plain_bytes_per_cell_step(True) * B * N / (plain_ms_step * 1e-3) / 1e9,
         clocks=clk.summary(), h2d=2 * B * N * 4, d2h=B * N * 4, launches=args.steps, traffic=extra_traffic,
+        error=error,
     )
     return cfg, cells, times, extra
 
@@ -427,6 +494,8 @@ def bench_burgers_plain(args, dev, world):
     torch.cuda.synchronize()
     with ClockSampler(dev.index) as clk:
         t_fused = event_time(fused, args.steps, flush)
+    torch.cuda.synchronize()
+    error = burgers_error_vs_fp64(frames, cfg)  # the timed launch's own frames
     bufs = [torch.empty(B, N, device=dev) for _ in range(2)]
 
     def plain():
@@ -451,6 +520,20 @@ def bench_burgers_plain(args, dev, world):
     graph.replay()
     torch.cuda.synchronize()
     t_graph = event_time(graph.replay, max(2, args.steps // 2), flush)
+    # the same per-step loop through the drop-in class (BurgersSolverTorch.step, as the reference's
+    # simulate_rollout calls it): the host cost of the public per-step API beside the raw launches
+    api = BurgersSolverTorch(sp)
+
+    def api_loop():
+        api.t = 0.0
+        u = u0
+        for k in range(steps):
+            u = api.step(u)
+            frames[:, k] = u
+
+    with torch.no_grad():
+        api_loop()
+        t_api = event_time(api_loop, max(2, args.steps // 2), flush)
     K = 8
     ckpts = torch.empty(B, (steps + K - 1) // K, N, device=dev)
     g_frames = torch.randn(B, steps, N, device=dev)
@@ -495,10 +578,11 @@ def bench_burgers_plain(args, dev, world):
     achieved = flops_cell * cells / (ms_fused * 1e-3) / 1e12
     plain_ms_step = sum(t_plain) / len(t_plain) / steps
     times = dict(fused=ms_fused, plain=sum(t_plain) / len(t_plain), graph=sum(t_graph) / len(t_graph),
-                 fused_fb=sum(t_ffb) / len(t_ffb), plain_fb=sum(t_pfb) / len(t_pfb), e2e=sum(t_e2e) / len(t_e2e))
+                 fused_fb=sum(t_ffb) / len(t_ffb), plain_fb=sum(t_pfb) / len(t_pfb), e2e=sum(t_e2e) / len(t_e2e),
+                 api=sum(t_api) / len(t_api))
     extra = dict(flops_per_cell_step=flops_cell, peak=peak, achieved=achieved,
                  plain_hbm_gbs=plain_bytes_per_cell_step(False) * B * N / (plain_ms_step * 1e-3) / 1e9,
-                 clocks=clk.summary(), h2d=B * N * 4, d2h=B * N * 4, launches=args.steps)
+                 clocks=clk.summary(), h2d=B * N * 4, d2h=B * N * 4, launches=args.steps, error=error)
     return cfg, cells, times, extra
 
 
@@ -518,6 +602,11 @@ def bench_burgers_batched(args, dev, world):
     cells = rb.total * steps
     out = torch.empty_like(rb.u0)
 
+    flush_buf = torch.empty(256 * 2 ** 20 // 4, device=dev)  # 256 MB > 126 MB L2
+
+    def flush():
+        flush_buf.fill_(1.0)
+
     def run():
         rb.rollout(steps, out=out)
 
@@ -525,7 +614,33 @@ def bench_burgers_batched(args, dev, world):
         run()
     torch.cuda.synchronize()
     with ClockSampler(dev.index) as clk:
-        t = event_time(run, args.steps)
+        t = event_time(run, args.steps, flush)
+    torch.cuda.synchronize()
+    error = ragged_error_vs_fp64(rb.unpack(out.cpu().numpy()), cfg)  # the timed launch's final state
+    # the same kernel one launch per step (the persistent launch with steps = 1), eager and graphed
+    bufs = [torch.empty_like(rb.u0) for _ in range(2)]
+
+    def plain():
+        u = rb.u0
+        for k in range(steps):
+            rb.rollout(1, u0=u, out=bufs[k & 1])
+            u = bufs[k & 1]
+
+    plain()
+    torch.cuda.synchronize()
+    t_plain = event_time(plain, max(2, args.steps // 2), flush)
+    graph = torch.cuda.CUDAGraph()
+    side = torch.cuda.Stream(dev)
+    side.wait_stream(torch.cuda.current_stream(dev))
+    with torch.cuda.stream(side):
+        plain()
+    torch.cuda.current_stream(dev).wait_stream(side)
+    with torch.cuda.graph(graph):
+        plain()
+    graph.replay()
+    torch.cuda.synchronize()
+    t_graph = event_time(graph.replay, max(2, args.steps // 2), flush)
+    del graph
     u0_h = rb.u0.cpu().pin_memory()
     out_h = torch.empty_like(u0_h).pin_memory()
 
@@ -536,13 +651,14 @@ def bench_burgers_batched(args, dev, world):
 
     for _ in range(args.warmup):
         e2e()
-    t_e2e = event_time(e2e, args.steps)
+    t_e2e = event_time(e2e, args.steps, flush)
     peak = fp32_peak_tflops(dev)
     ms = sum(t) / len(t)
     flops_cell = BURGERS_FLOPS[cfg["scheme"]]
-    times = dict(fused=ms, e2e=sum(t_e2e) / len(t_e2e))
+    times = dict(fused=ms, e2e=sum(t_e2e) / len(t_e2e), plain=sum(t_plain) / len(t_plain),
+                 graph=sum(t_graph) / len(t_graph))
     extra = dict(flops_per_cell_step=flops_cell, peak=peak, achieved=flops_cell * cells / (ms * 1e-3) / 1e12,
-                 clocks=clk.summary(), h2d=rb.total * 4, d2h=rb.total * 4, launches=args.steps)
+                 clocks=clk.summary(), h2d=rb.total * 4, d2h=rb.total * 4, launches=args.steps, error=error)
     cfg = dict(name="burgers_batched", B=cfg["rows"], N="64..512", steps=steps, scheme=cfg["scheme"],
                layout=cfg["layout"])
     return cfg, cells, times, extra
@@ -624,17 +740,35 @@ def bench_diff(args, dev, world, which):
                 solver.correction_s = net(u) if L is None else net(u, L)
                 u = solver.step(u) if L is None else solver.step(u, L)
 
+    def train_loop():  # the reference's training loop: one corrector call and one step() per step, autograd
+        if which == "burgers_diff":
+            solver.t = 0.0
+        u, frames = u0, []
+        for _ in range(steps):
+            solver.correction_s = net(u) if L is None else net(u, L)
+            u = solver.step(u) if L is None else solver.step(u, L)
+            frames.append(u)
+        loss = torch.mean((torch.stack(frames, 1) - target) ** 2)
+        loss.backward()
+        if world > 1:
+            average_gradients_(net.parameters(), local_rows=B)
+        opt.step()
+        opt.zero_grad(set_to_none=False)
+        return loss
+
     for _ in range(args.warmup):
         train_step(8)
         train_step(None)
         forward_only()
         forward_loop()
+        train_loop()
     torch.cuda.synchronize()
     with ClockSampler(dev.index) as clk:
         t_ck = event_time(lambda: train_step(8), args.steps)
     t_plain = event_time(lambda: train_step(None), args.steps)
     t_fwd = event_time(forward_only, args.steps)
     t_loop = event_time(forward_loop, args.steps)
+    t_loop_train = event_time(train_loop, args.steps)
     # the evaluation loop replayed from one CUDA graph (inc_b200.graphs)
     from inc_b200.graphs import GraphedRollout
     gsolver = mk()
@@ -671,9 +805,13 @@ def bench_diff(args, dev, world, which):
     launches = count_own_launches(lambda: train_step(8)) * args.steps
     ms = lambda t: sum(t) / len(t)  # noqa: E731
     times = dict(fused=ms(t_graph), e2e=ms(t_e2e), plain=ms(t_plain), fwd=ms(t_fwd), ckpt=ms(t_ck), loop=ms(t_loop),
-                 gfwd=ms(t_gfwd))
+                 gfwd=ms(t_gfwd), loop_train=ms(t_loop_train))
     extra = dict(clocks=clk.summary(), h2d=(u0.numel() + target.numel()) * 4, d2h=4, launches=launches)
     extra["checks"] = diff_checks(which, net_at_init, cfg, dev)
+    extra["error"] = {k: extra["checks"][k] for k in ("forward_rel_l2_vs_fp64", "grad_max_rel_err_vs_fp64_fd")}
+    extra["error"].update(forward_steps=extra["checks"]["forward_steps"], rows=extra["checks"]["rows"],
+                          tol={"forward": 1e-5, "grad": 1e-4},
+                          vs="FP64 loop on the host (torch corrector in float64, oracle step), FP64 central FD")
     if which == "ks_diff":  # the FNO's spectral convolution layer against the HBM peak
         extra["roofline"] = spectral_layer_roofline(dev, B, N)
     if which == "burgers_diff":  # the fused corrector rollout against the FP32 FMA peak
@@ -891,6 +1029,130 @@ def reference_arm(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+EXTRA_WORKLOADS = ("burgers_plain", "burgers_batched", "burgers_diff", "ks_diff")
+
+
+def run_workload(name, args, dev, world):
+    """Run one workload; device times become the max over ranks."""
+    import torch
+    if name in ("burgers_diff", "ks_diff"):
+        cfg, cells, times, extra = bench_diff(args, dev, world, name)
+    else:
+        fn = {"ks_plain": bench_ks, "burgers_plain": bench_burgers_plain, "burgers_batched": bench_burgers_batched}
+        cfg, cells, times, extra = fn[name](args, dev, world)
+    if world > 1:
+        keys = sorted(times)
+        t = torch.tensor([times[k] for k in keys], device=dev, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        times = dict(zip(keys, t.tolist()))
+    return cfg, cells, times, extra
+
+
+def diff_line(args, world, cfg, cells, times, extra):
+    tot = cells * world
+    rate = lambda ms: tot / (ms * 1e-3)  # noqa: E731
+    return {
+        "metric": "cell-steps/s (fwd+bwd training step)", "value": rate(times["fused"]),
+        "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": times["fused"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "unroll": cfg["steps"],
+                   "scheme": cfg["scheme"], "corrector": cfg["corrector"], "checkpoint_every": 8,
+                   "value_is": "whole training step (rollout, loss, backward, Adam) in one CUDA graph",
+                   "l2": "inputs and activations exceed L2 (not flushed)" if cfg["name"] == "ks_diff"
+                   else "not flushed (the 64 MB step keeps its activations in L2)",
+                   "parallelism": (f"data-parallel over {world} GPUs: per-rank trajectories, corrector "
+                                   "gradients averaged by one all-reduce per step" if world > 1
+                                   else "single GPU")},
+        "eager": {"train_step_ckpt8": rate(times["ckpt"]),
+                  "train_step_no_ckpt": rate(times["plain"]),
+                  "train_step_per_step_loop": rate(times["loop_train"]),
+                  "forward_only": rate(times["fwd"]),
+                  "forward_per_step_loop": rate(times["loop"]),
+                  "forward_graphed_loop": rate(times["gfwd"])},
+        "plain": {"fwd_fused_over_per_step_loop": times["loop"] / times["fwd"],
+                  "fwd_bwd_fused_over_per_step_loop": times["loop_train"] / times["ckpt"],
+                  "fwd_bwd_fused_graph_over_per_step_loop": times["loop_train"] / times["fused"],
+                  "per_step_loop_is": "the reference's loop: one torch corrector call and one step() per step, "
+                                      "autograd through both (eager)"},
+        "forward_only_is": ("fused corrector + solver kernel (inc_burgers_cnn_rollout)"
+                            if cfg["name"] == "burgers_diff" else "corrector in torch, solver step launches"),
+        "e2e": {"value": rate(times["e2e"]), "unit": "cell-steps/s",
+                "h2d_bytes_per_step": extra["h2d"], "d2h_bytes_per_step": extra["d2h"],
+                "api": "eager training step: simulate_rollout, loss.backward(), Adam"},
+        "roofline": extra.get("roofline") or extra.get("fused_inference_roofline"),
+        "fused_inference_roofline": extra.get("fused_inference_roofline"),
+        "error": extra.get("error"),
+        "checks": extra.get("checks"),
+        "clocks": extra["clocks"],
+        "gpu_launches": extra["launches"]}
+
+
+def plain_line(args, world, cfg, cells, times, extra, cpu_b):
+    tot = cells * world
+    rate = lambda ms: tot / (ms * 1e-3)  # noqa: E731
+    l2 = "flushed (256 MB write) before every timed iteration"
+    line = {
+        "metric": "cell-steps/s", "value": rate(times["fused"]), "unit": "cell-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": times["fused"], "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "steps_per_rollout": cfg["steps"],
+                   "scheme": cfg["scheme"], "l2": l2,
+                   "per_gpu": "full workload on every rank (trajectories are independent)",
+                   "layout": cfg.get("layout"), "dealias": cfg.get("dealias")},
+        "e2e": {"value": rate(times["e2e"]), "unit": "cell-steps/s", "h2d_bytes_per_step": extra["h2d"],
+                "d2h_bytes_per_step": extra["d2h"],
+                "api": "inc_b200.batched.RaggedBurgers.rollout" if cfg["name"] == "burgers_batched"
+                else "inc_b200.rollout (fused launch)"},
+        "roofline": {"bound": "fp32", "achieved": extra["achieved"], "peak": extra["peak"], "unit": "TFLOP/s",
+                     "frac": extra["achieved"] / extra["peak"], "traffic": extra.get("traffic"),
+                     "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch, "
+                                        "profiles/ks_rollout_fused_b1024_n256_dram.md")
+                     if extra.get("traffic") else None,
+                     "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run",
+                     "flops_per_cell_step": extra["flops_per_cell_step"],
+                     "flops_source": ("frozen per-cell-step count of the reference algorithm "
+                                      "(inc_b200/roofline.py)"),
+                     "implementation": extra.get("implementation")},
+        "error": extra.get("error"),
+        "cpu_baseline": cpu_b,
+        "clocks": extra["clocks"],
+        "gpu_launches": extra["launches"],
+    }
+    if "plain" in times:
+        p = {"eager_per_step": rate(times["plain"]), "graph_per_step": rate(times["graph"]),
+             "fused_over_eager": times["plain"] / times["fused"],
+             "fused_over_graph": times["graph"] / times["fused"]}
+        if "fused_fb" in times:
+            p.update({"fwd_bwd_fused": rate(times["fused_fb"]), "fwd_bwd_per_step": rate(times["plain_fb"]),
+                      "fwd_bwd_fused_over_per_step": times["plain_fb"] / times["fused_fb"],
+                      "plain_step_hbm_gbs": extra.get("plain_hbm_gbs")})
+        else:
+            p["fwd_bwd"] = "no backward: the ragged batch is a forward-only workload"
+        if "dealias" in times:
+            p["fused_dealias_2_3"] = rate(times["dealias"])
+        if "api" in times:
+            p["api_step_eager"] = rate(times["api"])
+            p["api_step_ms"] = times["api"] / cfg["steps"]
+            p["graph_step_ms"] = times["graph"] / cfg["steps"]
+            p["api_over_graph_time"] = times["api"] / times["graph"]
+            p["api_is"] = "BurgersSolverTorch.step(u) per step, eager (the drop-in API simulate_rollout calls)"
+        line["plain"] = p
+    return line
+
+
+def compact_block(line):
+    """The figures of one workload's line that the headline line carries for it."""
+    keys = ("value", "unit", "ms_per_step", "steps", "warmup", "config", "plain", "roofline", "e2e", "error",
+            "clocks", "gpu_launches", "eager")
+    out = {k: line[k] for k in keys if k in line}
+    if isinstance(out.get("roofline"), dict):
+        out["roofline"] = {k: v for k, v in out["roofline"].items()
+                           if k in ("bound", "achieved", "peak", "unit", "frac", "traffic", "implementation",
+                                    "kernel", "peak_source")}
+    return out
+
+
 def main():
     args = parse_args()
     rank = int(os.environ.get("RANK", "0"))
@@ -912,57 +1174,7 @@ def main():
     if args.profile:
         profile_small(dev, args.profile, args.profile_rows, args.tpp or 32)
         return
-    if args.workload in ("burgers_diff", "ks_diff"):
-        cfg, cells, times, extra = bench_diff(args, dev, world, args.workload)
-        if world > 1:
-            keys = sorted(times)
-            t = torch.tensor([times[k] for k in keys], device=dev, dtype=torch.float64)
-            torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-            times = dict(zip(keys, t.tolist()))
-        if rank == 0:
-            if cpu is not None:
-                cpu.close()
-            tot = cells * world
-            print(json.dumps({
-                "metric": "cell-steps/s (fwd+bwd training step)", "value": tot / (times["fused"] * 1e-3),
-                "unit": "cell-steps/s", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-                "ms_per_step": times["fused"], "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-                "dtype": "f32", "data": "synthetic (seeded)",
-                "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "unroll": cfg["steps"],
-                           "scheme": cfg["scheme"], "corrector": cfg["corrector"], "checkpoint_every": 8,
-                           "value_is": "whole training step (rollout, loss, backward, Adam) in one CUDA graph",
-                           "parallelism": (f"data-parallel over {world} GPUs: per-rank trajectories, corrector "
-                                           "gradients averaged by one all-reduce per step" if world > 1
-                                           else "single GPU")},
-                "eager": {"train_step_ckpt8": tot / (times["ckpt"] * 1e-3),
-                          "train_step_no_ckpt": tot / (times["plain"] * 1e-3),
-                          "forward_only": tot / (times["fwd"] * 1e-3),
-                          "forward_per_step_loop": tot / (times["loop"] * 1e-3),
-                          "forward_graphed_loop": tot / (times["gfwd"] * 1e-3)},
-                "forward_only_is": ("fused corrector + solver kernel (inc_burgers_cnn_rollout)"
-                                    if cfg["name"] == "burgers_diff" else "corrector in torch, solver step launches"),
-                "e2e": {"value": tot / (times["e2e"] * 1e-3), "unit": "cell-steps/s",
-                        "h2d_bytes_per_step": extra["h2d"], "d2h_bytes_per_step": extra["d2h"],
-                        "api": "eager training step: simulate_rollout, loss.backward(), Adam"},
-                "roofline": extra.get("roofline") or extra.get("fused_inference_roofline"),
-                "fused_inference_roofline": extra.get("fused_inference_roofline"),
-                "checks": extra.get("checks"),
-                "clocks": extra["clocks"],
-                "gpu_launches": extra["launches"]}), flush=True)
-        if world > 1:
-            torch.distributed.barrier()
-            torch.distributed.destroy_process_group()
-        return
-    fn = {"ks_plain": bench_ks, "burgers_plain": bench_burgers_plain, "burgers_batched": bench_burgers_batched}
-    cfg, cells, times, extra = fn[args.workload](args, dev, world)
-    # max over ranks of every device time
-    if world > 1:
-        keys = sorted(times)
-        t = torch.tensor([times[k] for k in keys], device=dev, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        times = dict(zip(keys, t.tolist()))
-    total_cells = cells * world
-    rate = lambda ms: total_cells / (ms * 1e-3)  # noqa: E731
+    cfg, cells, times, extra = run_workload(args.workload, args, dev, world)
     line = None
     if rank == 0:
         cpu_b = None
@@ -971,42 +1183,25 @@ def main():
             cpu_b = {"value": v, "unit": "cell-steps/s", "cores": cpu.cores, "kind": "port", "sample": desc}
         if cpu is not None:
             cpu.close()
-        clk = extra["clocks"]
-        line = {
-            "metric": "cell-steps/s", "value": rate(times["fused"]), "unit": "cell-steps/s", "n_gpus": world,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": times["fused"], "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "steps_per_rollout": cfg["steps"],
-                       "scheme": cfg["scheme"], "l2": "flushed (256 MB write) before every timed iteration",
-                       "per_gpu": "full workload on every rank (trajectories are independent)",
-                       "layout": cfg.get("layout"), "dealias": cfg.get("dealias")},
-            "e2e": {"value": rate(times["e2e"]), "unit": "cell-steps/s", "h2d_bytes_per_step": extra["h2d"],
-                    "d2h_bytes_per_step": extra["d2h"], "api": "inc_b200.rollout (fused launch)"},
-            "roofline": {"bound": "fp32", "achieved": extra["achieved"], "peak": extra["peak"], "unit": "TFLOP/s",
-                         "frac": extra["achieved"] / extra["peak"], "traffic": extra.get("traffic"),
-                         "traffic_source": ("ncu dram__bytes_read.sum + dram__bytes_write.sum of one full launch, "
-                                            "profiles/ks_rollout_fused_b1024_n256_dram.md")
-                         if extra.get("traffic") else None,
-                         "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run",
-                         "flops_per_cell_step": extra["flops_per_cell_step"],
-                         "flops_source": ("frozen per-cell-step count of the reference algorithm "
-                                          "(inc_b200/roofline.py)"),
-                         "implementation": extra.get("implementation")},
-            "cpu_baseline": cpu_b,
-            "clocks": clk,
-            "gpu_launches": extra["launches"],
-        }
-        if "plain" in times:
-            line["plain"] = {
-                "eager_per_step": rate(times["plain"]), "graph_per_step": rate(times["graph"]),
-                "fwd_bwd_fused": rate(times["fused_fb"]), "fwd_bwd_per_step": rate(times["plain_fb"]),
-                "fused_over_eager": times["plain"] / times["fused"],
-                "fused_over_graph": times["graph"] / times["fused"],
-                "fwd_bwd_fused_over_per_step": times["plain_fb"] / times["fused_fb"],
-                "plain_step_hbm_gbs": extra.get("plain_hbm_gbs"),
-            }
-            if "dealias" in times:
-                line["plain"]["fused_dealias_2_3"] = rate(times["dealias"])
+        if args.workload in ("burgers_diff", "ks_diff"):
+            line = diff_line(args, world, cfg, cells, times, extra)
+        else:
+            line = plain_line(args, world, cfg, cells, times, extra, cpu_b)
+    # The default run also measures the other configurations, each as a compact block of
+    # the headline line (fewer timed repeats; every rank runs every block).
+    if args.workload == "ks_plain" and not args.no_extra:
+        sub = copy.copy(args)
+        sub.steps, sub.warmup = max(2, min(args.steps, args.extra_steps)), max(3, min(args.warmup, 3))
+        blocks = {}
+        for name in EXTRA_WORKLOADS:
+            c, n, t, e = run_workload(name, sub, dev, world)
+            if rank == 0:
+                full = (diff_line(sub, world, c, n, t, e) if name in ("burgers_diff", "ks_diff")
+                        else plain_line(sub, world, c, n, t, e, None))
+                blocks[name] = compact_block(full)
+        if rank == 0:
+            line["configs"] = blocks
+    if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
         torch.distributed.barrier()

@@ -61,6 +61,10 @@ SIGNATURES = {
                                           _vp, _vp, _vp, _vp, _vp]),
     "inc_burgers_step_adaptive": (C.c_int, [C.POINTER(BurgersDesc), C.c_float, C.c_int32, _vp, _vp, _vp,
                                             C.c_double, _vp, _vp, _vp, _vp, _vp]),
+    "inc_burgers_terms": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, C.c_double, _vp, _vp, _vp, _vp]),
+    "inc_ks_substep": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, _vp, _vp]),
+    "inc_ks_substep_bwd": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, _vp, _vp, _vp, _vp]),
+    "inc_ks_fft_rows": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, C.c_int32, _vp]),
     "inc_burgers_ragged_rollout": (C.c_int, [C.POINTER(BurgersRaggedDesc), _vp, C.c_int32, _vp, _vp, C.c_int32,
                                              _vp]),
     "inc_ks_plan_size": (C.c_int64, [C.c_int32, C.c_int32]),
@@ -139,5 +143,33 @@ def ptr(t) -> int | None:
 
 
 def stream_of(device) -> int:
+    """The raw cudaStream_t of torch's current stream on `device`."""
     import torch
-    return torch.cuda.current_stream(device).cuda_stream
+    idx = device.index if isinstance(device, torch.device) else device
+    if idx is None:
+        idx = torch.cuda.current_device()
+    raw = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+    return raw(idx) if raw is not None else torch.cuda.current_stream(idx).cuda_stream
+
+
+class on_device:
+    """Make `device` current for a launch (a no-op when it already is)."""
+
+    __slots__ = ("idx", "prev")
+
+    def __init__(self, device):
+        self.idx = device.index
+
+    def __enter__(self):
+        import torch
+        cur = torch.cuda.current_device()
+        self.prev = None if (self.idx is None or cur == self.idx) else cur
+        if self.prev is not None:
+            torch.cuda.set_device(self.idx)
+        return self
+
+    def __exit__(self, *exc):
+        if self.prev is not None:
+            import torch
+            torch.cuda.set_device(self.prev)
+        return False

@@ -41,7 +41,7 @@ __global__ void __launch_bounds__(512) k_cnn_rollout(Args a, const float* __rest
     Ctx<1> cx;
     make_ctx<1, N>(a, valid ? row : 0, g, true, cx);
     cx.has_s = true;
-    float u[1];
+    float u[1], cmp[1] = {0.f};  // cmp: compensation carried from step to step (see advance)
     u[0] = valid ? __ldg(a.u + (int64_t)row * N + g) : 0.f;
     int parity = 0;
     float (*act0)[row_len<N>()] = S.act[0][rl];
@@ -67,7 +67,7 @@ __global__ void __launch_bounds__(512) k_cnn_rollout(Args a, const float* __rest
         const int64_t at = ((int64_t)row * a.steps + k) * N + g;
         if (corr && valid) corr[at] = s;
         // the stage's first barrier also orders these reads of act0 before the next step's writes
-        advance_wide<1, N>(a, cx, u, cx.t + k * cx.dt, S.sh[rl], parity, g);
+        advance_wide<1, N>(a, cx, u, cmp, cx.t + k * cx.dt, S.sh[rl], parity, g);
         if (a.frames && valid) a.frames[at] = u[0];
     }
     if (a.out && valid) a.out[(int64_t)row * N + g] = u[0];

@@ -48,9 +48,11 @@ INC_DEV void ragged_rows(const RaggedArgs& ra, int row, int lane) {
 #pragma unroll
     for (int c = 0; c < CPT; ++c) cx.s[c] = 0.f;
     const int64_t base = __ldg(ra.offsets + r) + g * CPT;
-    float u[CPT];
+    float u[CPT], cmp[CPT];  // cmp: compensation carried from step to step (see advance)
     load_row_chunk<CPT>(u, ra.u0 + base, valid);
-    for (int k = 0; k < ra.steps; ++k) advance<CPT, TPR>(a, cx, u, 0.f, left, right);
+#pragma unroll
+    for (int c = 0; c < CPT; ++c) cmp[c] = 0.f;
+    for (int k = 0; k < ra.steps; ++k) advance<CPT, TPR>(a, cx, u, cmp, 0.f, left, right);
     store_row_chunk<CPT>(ra.out + base, u, valid);
 }
 
@@ -182,11 +184,90 @@ __global__ void __launch_bounds__(1024) k_adaptive(AdaptArgs ad) {
     }
 }
 
+// ---- right-hand-side terms of one state -----------------------------------------
+// The reference solver's term methods, each to its own array: calc_nonlinear_weno
+// / calc_nonlinear_FDM (solver_1d.py:125-142), calc_linear (:144-146) and
+// _compute_source (:104-114, without correction_s).  One CTA per row, one cell
+// per thread (n <= 512), the row in shared memory.  The same device functions as
+// the step kernels evaluate the fluxes, so the terms agree with what a step adds.
+__global__ void __launch_bounds__(512) k_terms(Args a, float* __restrict__ nl_out, float* __restrict__ lin_out,
+                                               float* __restrict__ src_out) {
+    __shared__ float su[512];
+    __shared__ float sh[512];
+    __shared__ unsigned smax;
+    const int n = a.n, i = threadIdx.x, row = blockIdx.x;
+    const int64_t off = (int64_t)row * n + i;
+    const float ui = __ldg(a.u + off);
+    su[i] = ui;
+    if (i == 0) smax = 0u;
+    __syncthreads();
+    // per-row max |u| (solver_1d.py:133) on the bit patterns: NaN wins, as in torch.max
+    atomicMax(&smax, __float_as_uint(fabsf(ui)));
+    const int im1 = (i + n - 1) % n, ip1 = (i + 1) % n;
+    const float um1 = su[im1], up1 = su[ip1];
+    __syncthreads();
+    if (nl_out) {
+        if (a.conv == INC_CONV_WENO) {
+            const float ha = 0.5f * __uint_as_float(smax);
+            float fp[7], fm[7];  // cells i-3 .. i+3
+#pragma unroll
+            for (int k = 0; k < 7; ++k) flux_split(su[(i + k - 3 + 2 * n) % n], ha, fp[k], fm[k]);
+            const float h = weno5<false>(fp[1], fp[2], fp[3], fp[4], fp[5]) +
+                            weno5<true>(fm[2], fm[3], fm[4], fm[5], fm[6]);
+            sh[i] = h;
+            __syncthreads();
+            nl_out[off] = a.inv_dx * (sh[im1] - h);
+        } else {
+            nl_out[off] = -ui * ((up1 - um1) * a.inv_2dx);
+        }
+    }
+    const float nu = a.nu_rows ? __ldg(a.nu_rows + row) : a.nu;
+    if (lin_out) lin_out[off] = (nu * a.inv_dx2) * fmaf(-2.f, ui, um1 + up1);
+    if (src_out) {
+        float r = 0.f;
+        if (a.src == INC_SRC_LINEAR) {
+            r = (a.beta_rows ? __ldg(a.beta_rows + row) : a.beta) * ui;
+        } else if (a.src == INC_SRC_FORCING) {
+            const float t = a.t_rows ? __ldg(a.t_rows + row) : a.t0;
+            const float* fp = a.forcing + (int64_t)row * 4 * a.J;
+            const float x = __ldg(a.x + i);
+            for (int j = 0; j < a.J; ++j) {
+                const float A = __ldg(fp + j), om = __ldg(fp + a.J + j), ph = __ldg(fp + 2 * a.J + j),
+                            kx = __ldg(fp + 3 * a.J + j);
+                r = fmaf(A, sinf((om * t + kx * x) + ph), r);
+            }
+        }
+        src_out[off] = r;
+    }
+}
+
 }  // namespace burgers
 }  // namespace inc
 
 using namespace inc;
 using namespace inc::burgers;
+
+namespace inc {
+namespace burgers {
+int fill_args(const inc_burgers_desc* d, Args& a);
+}
+}  // namespace inc
+
+extern "C" int inc_burgers_terms(const inc_burgers_desc* d, const float* u, const float* t_rows, double t0,
+                                 float* nonlinear, float* linear, float* source, void* stream) {
+    Args a;
+    int rc = fill_args(d, a);
+    if (rc) return rc;
+    if (!u) { set_error("burgers_terms: null u"); return INC_E_INVALID; }
+    if (!is_pow2(d->n) || d->n < 8 || d->n > 512) {
+        set_error("burgers_terms: n must be a power of two in [8, 512] (got %d)", d->n);
+        return INC_E_UNSUPPORTED;
+    }
+    a.u = u; a.t_rows = t_rows; a.t0 = (float)t0;
+    if (!nonlinear && !linear && !source) return INC_OK;
+    k_terms<<<d->rows, d->n, 0, as_stream(stream)>>>(a, nonlinear, linear, source);
+    return check_launch("burgers_terms");
+}
 
 extern "C" int inc_burgers_ragged_rollout(const inc_burgers_ragged_desc* d, const float* u0, int32_t steps,
                                           float* u_final, int32_t* queue, int32_t grid_blocks, void* stream) {
@@ -218,12 +299,6 @@ extern "C" int inc_burgers_ragged_rollout(const inc_burgers_ragged_desc* d, cons
     k_ragged<<<grid, block, 0, st>>>(ra);
     return check_launch("ragged_rollout");
 }
-
-namespace inc {
-namespace burgers {
-int fill_args(const inc_burgers_desc* d, Args& a);
-}
-}  // namespace inc
 
 extern "C" int inc_burgers_step_adaptive(const inc_burgers_desc* d, float cfl, int32_t max_substeps, const float* u,
                                          const float* s, const float* t_rows, double t0, float* u_out, float* t_out,

@@ -230,6 +230,25 @@ extern "C" int inc_ks_step_bwd(const inc_ks_plan* p, const float* u, const float
     return dispatch(Kind::StepBwd, p, a, as_stream(stream));
 }
 
+extern "C" int inc_ks_substep(const inc_ks_plan* p, const float* u, const float* s, float* u_out, void* stream) {
+    Args a;
+    int rc = fill_args(p, a);
+    if (rc) return rc;
+    if (!ok_ptr(u) || !ok_ptr(u_out)) { set_error("ks_substep: bad u/u_out"); return INC_E_INVALID; }
+    a.u = u; a.s = s; a.out = u_out; a.substeps = 1;
+    return dispatch(Kind::Step, p, a, as_stream(stream));
+}
+
+extern "C" int inc_ks_substep_bwd(const inc_ks_plan* p, const float* u, const float* s, const float* g_out,
+                                  float* g_u, float* g_s, void* stream) {
+    Args a;
+    int rc = fill_args(p, a);
+    if (rc) return rc;
+    if (!ok_ptr(u) || !ok_ptr(g_out) || !ok_ptr(g_u)) { set_error("ks_substep_bwd: bad pointer"); return INC_E_INVALID; }
+    a.u = u; a.s = s; a.g_out = g_out; a.g_u = g_u; a.g_s = g_s; a.substeps = 1;
+    return dispatch(Kind::StepBwd, p, a, as_stream(stream));
+}
+
 extern "C" int inc_ks_rollout(const inc_ks_plan* p, const float* u0, const float* s, int32_t steps, float* frames,
                               float* u_final, int32_t ckpt_every, float* ckpts, void* stream) {
     Args a;

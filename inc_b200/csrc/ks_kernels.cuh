@@ -537,6 +537,7 @@ struct Args {
     const float2* tw;     // [N] FFT twiddles (layout of fft())
     float2* stage;        // rollout backward scratch: per launched group [ckpt_every][3][N] (or null)
     int rows, n, npairs, scheme, split, dealias, steps, ckpt_every, nhp;
+    int substeps;         // k_step / k_step_bwd: 1 = one substep (etd1_step / etrk2_step), else a step()
     float invN;
 };
 
@@ -862,7 +863,9 @@ __global__ void __launch_bounds__(128) k_step(Args a) {
     float2 x[P];
     load_pair<P, T>(x, a.u, c, N);
     if (a.cu) add_pair<P, T>(x, a.cu, c, N);  // u + correction_u, solver_1d.py:281/286
-    forward_program<P, T>(a, c, x, 1, buf, tw, false, 0);
+    // a single substep runs the first half of the step's half-substeps
+    const int skip = a.substeps == 1 ? (a.scheme == INC_KS_ETRK2 ? 2 : 1) : 0;
+    forward_program<P, T>(a, c, x, 1, buf, tw, false, 0, true, nullptr, nullptr, skip);
     store_pair<P, T>(a.out, x, c, N);
 }
 
@@ -921,6 +924,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
+    const bool single = !STG && a.substeps == 1;  // one substep: its states are x0 (and xi1)
     const float2* x1s = STG ? stg + (rk2 ? N : 0) : st;
     const float2* xi1s = STG ? stg : st + N;
     const float2* xi2s = STG ? stg + 2 * N : st + 2 * N;
@@ -940,14 +944,14 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
             else X[m] = z;
         }
     }
-    const int nrec = rk2 ? 3 : 1;
-    const int nunits = nrec + (rk2 ? 4 : 2);
+    const int nrec = single ? (rk2 ? 1 : 0) : (rk2 ? 3 : 1);
+    const int nunits = nrec + (rk2 ? 2 : 1) * (single ? 1 : 2);
 #pragma unroll 1
     for (int k = STG ? nrec : 0; k < nunits; ++k) {
         const bool rec = !STG && k < nrec;
         const int j = k - nrec;                        // adjoint unit
         const bool unit_w2 = rk2 && !rec && !(j & 1);  // w2 unit (ETRK2 only)
-        const bool sub1 = rk2 ? j < 2 : j < 1;         // second substep first
+        const bool sub1 = !single && (rk2 ? j < 2 : j < 1);  // second substep first
         float2 v[P];
         // STG: the adjoint unit's state is loaded from scratch before its first
         // transform, so the load overlaps the transform

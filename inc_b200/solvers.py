@@ -12,6 +12,7 @@ path: a missing library raises ``NativeLibraryError``.
 """
 from __future__ import annotations
 
+import copy
 import ctypes as C
 import math
 
@@ -58,6 +59,7 @@ class _BurgersLaunch:
         p = solver.param
         rows, n = u.shape
         dev = u.device
+        self.dev = dev
         d = nat.BurgersDesc()
         d.rows, d.n = rows, n
         d.scheme = _SCHEMES[solver.time_scheme]
@@ -75,6 +77,7 @@ class _BurgersLaunch:
         self.keep.append(nu_rows)
         eq = p.equation_type
         self.t0, self.t_rows = 0.0, None
+        self.timed = eq == "learning"  # only the forcing source reads the time
         if eq in ("homogeneous", "viscosity"):
             d.source = nat.INC_SRC_NONE
         elif eq == "linear":
@@ -91,39 +94,53 @@ class _BurgersLaunch:
             x = solver._x32(dev)
             d.x = x.data_ptr()
             self.keep += [forcing, x]
-            if isinstance(t, torch.Tensor):
-                if t.numel() != rows:
-                    raise ValueError("t tensor must have shape [batch_size,1]")
-                self.t_rows = t.detach().reshape(rows).to(device=dev, dtype=torch.float32).clone()
-            else:
-                self.t0 = float(t)
+            self._bind_time(t, rows)
         else:
             raise ValueError("Unknown equation type.")
         self.desc = d
-        self.dev = dev
+
+    def _bind_time(self, t, rows):
+        if isinstance(t, torch.Tensor):
+            if t.numel() != rows:
+                raise ValueError("t tensor must have shape [batch_size,1]")
+            # a snapshot: the solver advances its t in place after the step, and a
+            # backward launched later must see the time of this step
+            self.t_rows = t.detach().reshape(rows).to(device=self.dev, dtype=torch.float32).clone()
+            self.t0 = 0.0
+        else:
+            self.t0, self.t_rows = float(t), None
+
+    def at(self, t):
+        """This launch at time t: itself when the equation does not read the time, else a
+        shallow copy with the time bound (the descriptor and its tensors are shared)."""
+        if not self.timed:
+            return self
+        c = copy.copy(self)
+        c._bind_time(t, self.desc.rows)
+        return c
 
     def step(self, u, s, out):
-        with torch.cuda.device(self.dev):
+        with nat.on_device(self.dev):
             rc = nat.lib().inc_burgers_step(C.byref(self.desc), u.data_ptr(), nat.ptr(s), nat.ptr(self.t_rows),
                                             self.t0, out.data_ptr(), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_step")
 
     def step_bwd(self, u, s, g, gu, gs):
-        with torch.cuda.device(self.dev):
+        with nat.on_device(self.dev):
             rc = nat.lib().inc_burgers_step_bwd(C.byref(self.desc), u.data_ptr(), nat.ptr(s), nat.ptr(self.t_rows),
                                                 self.t0, g.data_ptr(), gu.data_ptr(), nat.ptr(gs),
                                                 nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_step_bwd")
 
     def rollout(self, u0, s, steps, frames, u_final, ckpt_every, ckpts):
-        with torch.cuda.device(self.dev):
+        with nat.on_device(self.dev):
             rc = nat.lib().inc_burgers_rollout(C.byref(self.desc), u0.data_ptr(), nat.ptr(s), nat.ptr(self.t_rows),
                                                self.t0, steps, nat.ptr(frames), nat.ptr(u_final), ckpt_every,
                                                nat.ptr(ckpts), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_rollout")
 
     def cnn_rollout(self, weights, u0, steps, frames, corrections, u_final, ckpt_every=0, ckpts=None):
-        with torch.cuda.device(self.dev):
+        with nat.on_device(self.dev):
             rc = nat.lib().inc_burgers_cnn_rollout(C.byref(self.desc), weights.data_ptr(), u0.data_ptr(),
                                                    nat.ptr(self.t_rows), self.t0, steps, nat.ptr(frames),
                                                    nat.ptr(corrections), nat.ptr(u_final), int(ckpt_every),
@@ -132,7 +149,7 @@ class _BurgersLaunch:
 
     def cnn_rollout_bwd(self, weights, ckpts, corrections, steps, ckpt_every, g_frames, g_corrections, g_final,
                         g_u0, g_weights, work):
-        with torch.cuda.device(self.dev):
+        with nat.on_device(self.dev):
             rc = nat.lib().inc_burgers_cnn_rollout_bwd(
                 C.byref(self.desc), weights.data_ptr(), ckpts.data_ptr(), corrections.data_ptr(),
                 nat.ptr(self.t_rows), self.t0, steps, ckpt_every, nat.ptr(g_frames), nat.ptr(g_corrections),
@@ -140,7 +157,7 @@ class _BurgersLaunch:
         nat.check(rc, "inc_burgers_cnn_rollout_bwd")
 
     def rollout_bwd(self, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s):
-        with torch.cuda.device(self.dev):
+        with nat.on_device(self.dev):
             rc = nat.lib().inc_burgers_rollout_bwd(C.byref(self.desc), ckpts.data_ptr(), nat.ptr(s),
                                                    nat.ptr(self.t_rows), self.t0, steps, ckpt_every,
                                                    nat.ptr(g_frames), nat.ptr(g_final), g_u0.data_ptr(),
@@ -206,6 +223,8 @@ class BurgersSolverTorch:
         self._forcing_cache = None
         self._x_cache = None
         self._cpt_cache = None
+        self._launch_cache = None
+        self._d2t = self._d1t = None
 
     def _tuned_cpt(self, n, rows, dev):
         """Cells per lane from the autotuner cache (0 = library default)."""
@@ -218,9 +237,11 @@ class BurgersSolverTorch:
     # -- parameters packed for the kernels ------------------------------------
     def _forcing_pack(self, rows, dev):
         p = self.param
-        key = (id(p.A), id(p.omega), id(p.phi), id(p.l), rows, str(dev))
-        if self._forcing_cache is not None and self._forcing_cache[0] == key:
-            return self._forcing_cache[1]
+        objs = (p.A, p.omega, p.phi, p.l)
+        key = (rows, str(dev), p.J, p.L) + tuple(getattr(o, "_version", None) for o in objs)
+        c = self._forcing_cache
+        if c is not None and c[0] == key and all(a is b for a, b in zip(c[2], objs)):
+            return c[1]
         J = int(p.J)
 
         def rj(v):
@@ -229,7 +250,7 @@ class BurgersSolverTorch:
 
         kx = 2 * math.pi * rj(p.l) / float(p.L)
         pack = torch.stack([rj(p.A), rj(p.omega), rj(p.phi), kx], dim=1).to(torch.float32).contiguous()
-        self._forcing_cache = (key, pack)
+        self._forcing_cache = (key, pack, objs)  # holds objs: their ids cannot be reused
         return pack
 
     def _x32(self, dev):
@@ -257,30 +278,127 @@ class BurgersSolverTorch:
             delta = delta + p.A[..., j] * torch.sin(arg)
         return delta
 
+    # -- the reference's term methods (solver_1d.py:87-146) -------------------------
+    # Each is one launch of inc_burgers_terms on the solver's parameters: the same
+    # device arithmetic as the step kernels, each term to its own array.  They are
+    # not differentiable here (step() and the rollouts are); under autograd they
+    # raise instead of returning a result without a gradient.
+    def _terms(self, u, conv=None, want=("nonlinear",)):
+        _check_state(u, self.resolution)
+        if torch.is_grad_enabled() and u.requires_grad:
+            raise RuntimeError("BurgersSolverTorch term methods are not differentiable here; "
+                               "differentiate step() or the rollouts instead")
+        u = u.contiguous()
+        outs = {k: torch.empty_like(u) for k in want}
+        if u.shape[0] == 0:
+            return outs
+        launch = _BurgersLaunch(self, u, self.t)
+        d = launch.desc
+        if conv is not None:
+            d = nat.BurgersDesc.from_buffer_copy(d)
+            d.convection = nat.INC_CONV_WENO if conv == "WENO" else nat.INC_CONV_FDM
+        with nat.on_device(launch.dev):
+            rc = nat.lib().inc_burgers_terms(C.byref(d), u.data_ptr(), nat.ptr(launch.t_rows), launch.t0,
+                                             nat.ptr(outs.get("nonlinear")), nat.ptr(outs.get("linear")),
+                                             nat.ptr(outs.get("source")), nat.stream_of(launch.dev))
+        nat.check(rc, "inc_burgers_terms")
+        return outs
+
     def calc_nonlinear_weno(self, u):
-        """WENO5-LF convection term alone (solver_1d.py:129-142), via a one-step kernel."""
-        return self._term(u, "WENO")
+        """-(D- f+ + D- f-)/dx with WENO5 Lax-Friedrichs fluxes (solver_1d.py:129-142)."""
+        return self._terms(u, "WENO")["nonlinear"]
 
     def calc_nonlinear_FDM(self, u):
-        return self._term(u, "FDM")
+        """-u D1 u with the periodic central difference (solver_1d.py:125-127)."""
+        return self._terms(u, "FDM")["nonlinear"]
 
-    def _term(self, u, conv):
-        _check_state(u, self.resolution)
-        saved = (self.param.convection_term, self.nu, self.dt, self.param.equation_type, self.time_scheme)
-        try:
-            self.param.convection_term, self.nu, self.dt = conv, 0.0, 1.0
-            self.param.equation_type, self.time_scheme = "homogeneous", "euler"
-            launch = _BurgersLaunch(self, u, 0.0)
-            out = torch.empty_like(u)
-            launch.step(u.contiguous(), None, out)
-        finally:
-            (self.param.convection_term, self.nu, self.dt, self.param.equation_type, self.time_scheme) = saved
-        return out - u
+    def calc_linear(self, u):
+        """nu D2 u (solver_1d.py:144-146); the kernels apply D2 as its three-point stencil."""
+        return self._terms(u, want=("linear",))["linear"]
+
+    def _compute_source(self, u):
+        """The equation's source term (solver_1d.py:104-114): 0.0 for homogeneous /
+        viscosity, beta u for linear, the forcing sum at self.t for learning."""
+        eq = self.param.equation_type
+        if eq in ("homogeneous", "viscosity"):
+            return 0.0
+        if eq not in ("linear", "learning"):
+            raise ValueError("Unknown equation type.")
+        return self._terms(u, want=("source",))["source"]
+
+    def _apply_corrections(self, source):
+        """source + correction_s when a correction is set (solver_1d.py:116-123)."""
+        if self.correction_s is not None:
+            source = source + self.correction_s
+        return source
+
+    def _create_diffusion_matrix(self):
+        """The dense periodic second-difference matrix / dx^2 (solver_1d.py:95-102).  Only
+        for callers that read it: the kernels never form it."""
+        n = self.resolution
+        i = torch.arange(n, device=self.device)
+        m = torch.zeros(n, n, device=self.device)
+        m[i, (i - 1) % n] += 1.0 / self.dx ** 2
+        m[i, i] += -2.0 / self.dx ** 2
+        m[i, (i + 1) % n] += 1.0 / self.dx ** 2
+        return m
+
+    def _create_convection_matrix(self):
+        """The dense periodic central first-difference matrix (solver_1d.py:87-93)."""
+        n = self.resolution
+        i = torch.arange(n, device=self.device)
+        m = torch.zeros(n, n, device=self.device)
+        m[i, (i - 1) % n] += -1.0 / (2 * self.dx)
+        m[i, (i + 1) % n] += 1.0 / (2 * self.dx)
+        return m
+
+    @property
+    def D2_T(self):
+        """Transpose of the diffusion matrix (solver_1d.py:58), built on first access."""
+        if self._d2t is None:
+            self._d2t = self._create_diffusion_matrix().T
+        return self._d2t
+
+    @property
+    def D1_T(self):
+        """Transpose of the convection matrix; the reference defines it for FDM convection
+        only (solver_1d.py:61)."""
+        if self.param.convection_term != "FDM":
+            raise AttributeError("'BurgersSolverTorch' object has no attribute 'D1_T' (WENO convection)")
+        if self._d1t is None:
+            self._d1t = self._create_convection_matrix().T
+        return self._d1t
 
     def launch_for(self, u, t=None):
         """The kernel configuration of this solver for state u at time t (default self.t)."""
         _check_state(u, self.resolution)
         return _BurgersLaunch(self, u, self.t if t is None else t)
+
+    def _launch_key(self, u):
+        p = self.param
+        eq = p.equation_type
+        static = (tuple(u.shape), u.device, self.time_scheme, p.convection_term, eq, self.dt, self.dx,
+                  self.cells_per_thread)
+        objs = (self.nu,)
+        if eq == "linear":
+            objs += (p.beta,)
+        elif eq == "learning":
+            objs += (p.A, p.omega, p.phi, p.l, p.J, p.L, self.x)
+        return static, objs, tuple(getattr(o, "_version", None) for o in objs)
+
+    def _cached_launch(self, u):
+        """The launch descriptor of the last step, rebuilt only when the shape, the scheme or
+        a parameter changes (a parameter tensor replaced by another, or modified in place);
+        step() then only binds the time."""
+        static, objs, versions = self._launch_key(u)
+        c = self._launch_cache
+        if (c is not None and c[0] == static and c[2] == versions and len(c[1]) == len(objs)
+                and all(a is b or (not isinstance(a, torch.Tensor) and not isinstance(b, torch.Tensor) and a == b)
+                        for a, b in zip(c[1], objs))):
+            return c[3]
+        launch = _BurgersLaunch(self, u, self.t)
+        self._launch_cache = (static, objs, versions, launch)  # holds objs: their ids cannot be reused
+        return launch
 
     def step(self, u):
         """Advance by dt (forward Euler, or SSP-RK3 when configured); solver_1d.py:181-195."""
@@ -291,7 +409,7 @@ class BurgersSolverTorch:
         if u.shape[0] == 0:  # an empty batch: nothing to launch
             self.t += self.dt
             return u.clone()
-        launch = self.launch_for(u)
+        launch = self._cached_launch(u).at(self.t)
         s = _contig(self.correction_s)
         if s is not None:
             _check_state(s, self.resolution, "correction_s")
@@ -336,26 +454,26 @@ class KSPlan:
         p.rows, p.n, p.scheme, p.dealias = rows, n, _KS_SCHEMES[scheme], int(bool(dealias))
         p.threads_per_pair, p.dt, p.dev = int(threads_per_pair), float(dt), self.buf.data_ptr()
         host = (C.c_float * rows)(*[float(v) for v in domain_size_host])
-        with torch.cuda.device(self.device):
+        with nat.on_device(self.device):
             rc = nat.lib().inc_ks_plan_init(C.byref(p), host, nat.stream_of(self.device))
         nat.check(rc, "inc_ks_plan_init")
         self.c = p
         self.rows, self.n = rows, n
 
     def step(self, u, s, cu, out):
-        with torch.cuda.device(self.device):
+        with nat.on_device(self.device):
             rc = nat.lib().inc_ks_step(C.byref(self.c), u.data_ptr(), nat.ptr(s), nat.ptr(cu), out.data_ptr(),
                                        nat.stream_of(self.device))
         nat.check(rc, "inc_ks_step")
 
     def step_bwd(self, u, s, cu, g, gu, gs):
-        with torch.cuda.device(self.device):
+        with nat.on_device(self.device):
             rc = nat.lib().inc_ks_step_bwd(C.byref(self.c), u.data_ptr(), nat.ptr(s), nat.ptr(cu), g.data_ptr(),
                                            gu.data_ptr(), nat.ptr(gs), nat.stream_of(self.device))
         nat.check(rc, "inc_ks_step_bwd")
 
     def rollout(self, u0, s, steps, frames, u_final, ckpt_every, ckpts):
-        with torch.cuda.device(self.device):
+        with nat.on_device(self.device):
             rc = nat.lib().inc_ks_rollout(C.byref(self.c), u0.data_ptr(), nat.ptr(s), steps, nat.ptr(frames),
                                           nat.ptr(u_final), ckpt_every, nat.ptr(ckpts), nat.stream_of(self.device))
         nat.check(rc, "inc_ks_rollout")
@@ -365,7 +483,7 @@ class KSPlan:
         scratch of ``rollout_bwd_work_size(ckpt_every)`` bytes in which the
         segment replay keeps the substep states; ``work=False`` rebuilds them
         per step instead (fewer bytes, more transforms)."""
-        with torch.cuda.device(self.device):
+        with nat.on_device(self.device):
             if work is False:
                 rc = nat.lib().inc_ks_rollout_bwd(C.byref(self.c), ckpts.data_ptr(), nat.ptr(s), steps, ckpt_every,
                                                   nat.ptr(g_frames), nat.ptr(g_final), g_u0.data_ptr(), nat.ptr(g_s),
@@ -409,6 +527,64 @@ class KSStepFn(torch.autograd.Function):
         ctx.plan.step_bwd(u, s, cu, g.contiguous(), gu, gs)
         gcu = gu if (has_cu and ctx.needs_input_grad[2]) else None
         return gu, gs, gcu, None
+
+
+class KSSubstepFn(torch.autograd.Function):
+    """One ETRK2 / ETD1 substep (etrk2_step / etd1_step) and its adjoint kernel."""
+
+    @staticmethod
+    def forward(ctx, u, s, plan):
+        out = torch.empty_like(u)
+        with nat.on_device(plan.device):
+            rc = nat.lib().inc_ks_substep(C.byref(plan.c), u.data_ptr(), nat.ptr(s), out.data_ptr(),
+                                          nat.stream_of(plan.device))
+        nat.check(rc, "inc_ks_substep")
+        ctx.plan, ctx.has_s = plan, s is not None
+        ctx.save_for_backward(u, s if s is not None else u.new_empty(0))
+        return out
+
+    @staticmethod
+    def backward(ctx, g):
+        u, s = ctx.saved_tensors
+        s = s if ctx.has_s else None
+        gu = torch.empty_like(u)
+        gs = torch.empty_like(u) if (ctx.has_s and ctx.needs_input_grad[1]) else None
+        plan = ctx.plan
+        with nat.on_device(plan.device):
+            rc = nat.lib().inc_ks_substep_bwd(C.byref(plan.c), u.data_ptr(), nat.ptr(s), g.contiguous().data_ptr(),
+                                              gu.data_ptr(), nat.ptr(gs), nat.stream_of(plan.device))
+        nat.check(rc, "inc_ks_substep_bwd")
+        return gu, gs, None
+
+
+def _fft_rows(v, mode, out):
+    with nat.on_device(v.device):
+        rc = nat.lib().inc_ks_fft_rows(v.data_ptr(), out.data_ptr(), v.shape[0], v.shape[1], mode,
+                                       nat.stream_of(v.device))
+    nat.check(rc, "inc_ks_fft_rows")
+    return out
+
+
+class FFTSquareFn(torch.autograd.Function):
+    """FFT(u^2) of each real row (complex [B, N], unnormalised as torch.fft.fft) on the
+    row-pair FFT kernel; the backward is 2 u Re(sum_k g_k exp(+2 pi i k j / N)), the
+    adjoint of a real row's FFT, on the same kernel."""
+
+    @staticmethod
+    def forward(ctx, u):
+        u = u.contiguous()
+        out = torch.empty(u.shape[0], u.shape[1], 2, device=u.device, dtype=torch.float32)
+        _fft_rows(u, 1, out)
+        ctx.save_for_backward(u)
+        return torch.view_as_complex(out)
+
+    @staticmethod
+    def backward(ctx, g):
+        u, = ctx.saved_tensors
+        gr = torch.view_as_real(g.to(torch.complex64).contiguous())
+        re = torch.empty_like(u)
+        _fft_rows(gr, 2, re)
+        return 2.0 * u * re
 
 
 class KSSolverTorch:
@@ -508,3 +684,38 @@ class KSSolverTorch:
     def etd1(self, u, domain_size):
         """u (+ correction_u), then two ETD1 substeps (solver_1d.py:280-283)."""
         return self._step(u, domain_size, "ETD1")
+
+    # -- the reference's single-substep and term methods (solver_1d.py:225-278) ------
+    def _substep(self, u, domain_size, scheme):
+        _check_state(u, self.resolution)
+        u = u.contiguous()
+        if u.shape[0] == 0:
+            return u.clone()
+        plan = self.plan_for(u, domain_size, scheme)
+        s = _contig(self.correction_s)
+        if s is not None:
+            _check_state(s, self.resolution, "correction_s")
+        return KSSubstepFn.apply(u, s, plan)
+
+    def etrk2_step(self, u, domain_size):
+        """One ETRK2 substep with correction_s, without correction_u (solver_1d.py:257-278)."""
+        return self._substep(u, domain_size, "ETRK2")
+
+    def etd1_step(self, u, domain_size):
+        """One ETD1 substep with correction_s, without correction_u (solver_1d.py:242-255)."""
+        return self._substep(u, domain_size, "ETD1")
+
+    def calc_linear(self, domain_size):
+        """(L, wavenumbers) of solver_1d.py:235-240, complex [B, N]: wavenumbers = i k
+        with k = 2 pi fftfreq(N) N / domain_size, L = k^2 - k^4 (= -(ik)^2 - (ik)^4).
+        Set-up data, computed with torch on the solver's device."""
+        ds = torch.as_tensor(domain_size, device=self.device)
+        k = (2 * math.pi) * self.fft_indices / ds.unsqueeze(-1)
+        zero = torch.zeros_like(k)
+        return torch.complex(k * k - k ** 4, zero), torch.complex(zero, k)
+
+    def calc_nonlinear(self, u, wavenumbers):
+        """-0.5 wavenumbers FFT(u^2) (solver_1d.py:225-233; the reference's zero padding in
+        physical space changes nothing).  FFT(u^2) runs on the row-pair FFT kernel."""
+        _check_state(u, self.resolution)
+        return -0.5 * wavenumbers * FFTSquareFn.apply(u)

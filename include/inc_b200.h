@@ -17,11 +17,15 @@
  *      SSP-RK3 composed on the same right-hand side)
  *   autograd backward through BurgersSolverTorch.step -> inc_burgers_step_bwd
  *   BurgersSolverTorch.step_adaptive(u)           :148-179 -> inc_burgers_step_adaptive
+ *   calc_nonlinear_weno / _FDM, calc_linear, _compute_source
+ *                                   :104-146 -> inc_burgers_terms
  *   simulate_rollout(model=None, BurgersSolverTorch) trainer/trainer_1d.py:154-183
  *                                                  -> inc_burgers_rollout (+ _bwd)
  *   KSSolverTorch.__init__ / calc_linear / etd coefficients :199-212, :235-267
  *                                                  -> inc_ks_plan_size, inc_ks_plan_init
  *   KSSolverTorch.step(u, L) = etrk2 / etd1        :280-288 -> inc_ks_step
+ *   KSSolverTorch.etrk2_step / etd1_step          :242-278 -> inc_ks_substep (+ _bwd)
+ *   KSSolverTorch.calc_nonlinear's FFT(u^2)       :225-233 -> inc_ks_fft_rows
  *   autograd backward through KSSolverTorch.step   -> inc_ks_step_bwd
  *   simulate_rollout(model=None, KSSolverTorch)    -> inc_ks_rollout (+ _bwd)
  */
@@ -143,6 +147,17 @@ int inc_burgers_rollout_bwd(const inc_burgers_desc* d, const float* ckpts,
                             const float* g_frames, const float* g_final,
                             float* g_u0, float* g_s, void* stream);
 
+/* The right-hand side's terms for a state u [rows][n], each to its own array
+ * (any of the three may be NULL): nonlinear = calc_nonlinear_weno or
+ * calc_nonlinear_FDM (solver_1d.py:125-142, per the descriptor's convection),
+ * linear = calc_linear, nu * D2 u (:144-146), source = _compute_source (:104-114;
+ * zero for homogeneous / viscosity, beta u for linear, the forcing sum at time
+ * t_rows / t0 for learning; correction_s is not added, as in the reference).
+ * The same device arithmetic as the step kernels.  n: a power of two in [8, 512]. */
+int inc_burgers_terms(const inc_burgers_desc* d, const float* u, const float* t_rows,
+                      double t0, float* nonlinear, float* linear, float* source,
+                      void* stream);
+
 /* Adaptive-CFL Euler sub-stepping over one dt with the global max |u|
  * (solver_1d.py:148-179), all on the device: no host synchronisation.  One
  * CTA runs the whole batch (block barriers between substeps).  t_out [rows]
@@ -240,6 +255,13 @@ int inc_ks_step(const inc_ks_plan* plan, const float* u, const float* s,
 int inc_ks_step_bwd(const inc_ks_plan* plan, const float* u, const float* s,
                     const float* cu, const float* g_out, float* g_u, float* g_s,
                     void* stream);
+/* One substep: etrk2_step / etd1_step (solver_1d.py:242-278) per the plan's
+ * scheme, without correction_u (the reference adds it in etrk2 / etd1 only).  */
+int inc_ks_substep(const inc_ks_plan* plan, const float* u, const float* s,
+                   float* u_out, void* stream);
+/* Vector-Jacobian product of inc_ks_substep (g_s may be NULL).              */
+int inc_ks_substep_bwd(const inc_ks_plan* plan, const float* u, const float* s,
+                       const float* g_out, float* g_u, float* g_s, void* stream);
 /* `steps` step() calls in one launch with s held constant; frames, u_final,
  * ckpts as for inc_burgers_rollout.                                          */
 int inc_ks_rollout(const inc_ks_plan* plan, const float* u0, const float* s,
@@ -265,6 +287,14 @@ int inc_ks_rollout_bwd_ws(const inc_ks_plan* plan, const float* ckpts, const flo
  * doubled.  Replaces calculate_energy_spectrum (analysis/Plot_KS.py:196-235),
  * which the reference runs on the CPU after a rollout.                        */
 int inc_energy_spectrum(const float* u, float* out, int32_t rows, int32_t n, void* stream);
+
+/* Spectra of real rows for KSSolverTorch.calc_nonlinear (solver_1d.py:225-233):
+ * mode 0: out = FFT(v), mode 1: out = FFT(v^2), both [rows][n] complex (re, im
+ * interleaved; 8-byte aligned), unnormalised as torch.fft.fft; mode 2: v is
+ * [rows][n] complex and out [rows][n] real, the real part of the unnormalised
+ * inverse DFT (the adjoint of a real row's FFT).  n: power of two in [16, 512]. */
+int inc_ks_fft_rows(const float* v, float* out, int32_t rows, int32_t n, int32_t mode,
+                    void* stream);
 
 /* ---- corrector: FNO spectral convolution ----------------------------------- */
 /* y[b][o] = irfft(sum_c rfft(x[b][c])[k] * (w_re + i w_im)[c][o][k] for

@@ -131,7 +131,17 @@ def test_fused_rollout_matches_steps(cuda):
             frames.append(u)
         b = BurgersSolverTorch(_sim_params(p, B, scheme))
         fused = burgers_rollout(b, u0, 23, s=s)
-        assert torch.equal(fused, torch.stack(frames, 1)), scheme
+        # the fused launch carries the rounding error of each update into the next step
+        # (compensated summation), the per-step launches cannot: equal up to that rounding
+        stepped = torch.stack(frames, 1)
+        assert rel_l2(fused.cpu().numpy(), stepped.cpu().numpy()) < 1e-6, scheme
+        fn = ob.step_ssprk3 if scheme == "ssprk3" else ob.step_euler
+        ref, t, rf = u0.cpu().double().numpy(), 0.0, []
+        for _ in range(23):
+            ref, t = fn(ref, p, t, s.cpu().double().numpy())
+            rf.append(ref)
+        rf = np.stack(rf, 1)
+        assert rel_l2(fused.cpu().numpy(), rf) <= rel_l2(stepped.cpu().numpy(), rf) * 1.5 + 1e-9, scheme
 
 
 def test_simulate_rollout_dropin_no_model(cuda):
@@ -353,3 +363,54 @@ def test_nonfinite_propagates(cuda):
     u[1, 7] = float("nan")
     out = solver.step(u)
     assert torch.isnan(out[1]).any() and torch.isfinite(out[0]).all() and torch.isfinite(out[2]).all()
+
+
+def test_step_descriptor_cache_follows_parameters(cuda):
+    """step() reuses its launch descriptor across calls: a parameter modified in place or
+    replaced, and the time of a forcing ('learning') step under autograd, must still reach
+    the kernel exactly as a freshly built descriptor would pass them."""
+    from inc_b200.solvers import BurgersSolverTorch, BurgersStepFn
+    B, n = 5, 64
+    rng = np.random.default_rng(21)
+    p = ob.BurgersParams(resolution=n, L=2 * math.pi, dt=0.01, nu=rng.uniform(0.005, 0.05, (B, 1)),
+                         equation_type="learning", A=rng.uniform(-0.5, 0.5, (B, 1, 3)),
+                         omega=rng.uniform(-0.4, 0.4, (B, 1, 3)), phi=rng.uniform(0, 6.28, (B, 1, 3)),
+                         l=rng.integers(1, 4, (B, 1, 3)).astype(np.float64), x=np.arange(n) * (2 * math.pi / n))
+    sp = _sim_params(p, B, "ssprk3")
+    solver = BurgersSolverTorch(sp)
+    solver.t = torch.tensor(rng.uniform(0, 1, (B, 1)), dtype=torch.float32, device=cuda)
+    u0 = torch.tensor(_rand_u0(B, n, 8), dtype=torch.float32, device=cuda)
+
+    def fresh_step(u, t):
+        launch = solver.launch_for(u, t)
+        out = torch.empty_like(u)
+        launch.step(u, None, out)
+        return out
+
+    t0 = solver.t.clone()
+    a = solver.step(u0)
+    assert torch.equal(a, fresh_step(u0, t0))
+    sp.nu.mul_(2.0)                      # in place: same tensor object, new version
+    t1 = solver.t.clone()
+    b = solver.step(u0)
+    assert torch.equal(b, fresh_step(u0, t1)) and not torch.equal(a, b)
+    sp.A = sp.A * 0.5                    # replaced by a new tensor
+    t2 = solver.t.clone()
+    c = solver.step(u0)
+    assert torch.equal(c, fresh_step(u0, t2)) and not torch.equal(b, c)
+    # autograd over three cached steps while solver.t advances in place: the backward of each
+    # step sees that step's time
+    u = u0.clone().requires_grad_(True)
+    solver.t = t0.clone()
+    x, ts = u, []
+    for _ in range(3):
+        ts.append(solver.t.clone())
+        x = solver.step(x)
+    w = torch.randn_like(x)
+    g_cached, = torch.autograd.grad((x * w).sum(), (u,))
+    u2 = u0.clone().requires_grad_(True)
+    y = u2
+    for t in ts:
+        y = BurgersStepFn.apply(y, None, solver.launch_for(y, t))
+    g_fresh, = torch.autograd.grad((y * w).sum(), (u2,))
+    assert torch.equal(x, y) and torch.equal(g_cached, g_fresh)

@@ -216,6 +216,38 @@ def test_rollout_backward_scratch_matches_rebuild(cuda, N, tpp, scheme):
         plan.rollout_bwd(ck, s, steps, K, gf, gfin, gu, gs, work=small)
 
 
+@pytest.mark.parametrize("B,tpp", [(1031, 16), (4101, 32)])
+def test_rollout_backward_scratch_many_groups(cuda, B, tpp):
+    """The scratch backward on grids of many blocks with several row pairs per block
+    and a partial last block (odd B: a lone row too), against the rebuilding form:
+    each launched group's scratch slot and the padding of the scratch size."""
+    N, steps, K, dt = 256, 11, 4, 0.25
+    Ls = [64.0] * B
+    solver = _solver(N, dt, "ETRK2", Ls, tpp=tpp)
+    from inc_b200.workloads import ks_plain_config
+    cfg = ks_plain_config(B=B, steps=steps)
+    u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=cuda)
+    s = torch.tensor(cfg["s"], dtype=torch.float32, device=cuda)
+    ds = torch.full((B,), 64.0, device=cuda)
+    plan = solver.plan_for(u0, ds)
+    frames = torch.empty(B, steps, N, device=cuda)
+    ck = torch.empty(B, (steps + K - 1) // K, N, device=cuda)
+    plan.rollout(u0, s, steps, frames, None, K, ck)
+    g = torch.Generator(device=cuda).manual_seed(B)
+    gf = torch.randn(B, steps, N, device=cuda, generator=g)
+    out = []
+    for work in (None, False):
+        gu, gs = torch.empty_like(u0), torch.empty_like(u0)
+        plan.rollout_bwd(ck, s, steps, K, gf, None, gu, gs, work=work)
+        out.append((gu.cpu().numpy(), gs.cpu().numpy()))
+    for a, b in zip(*out):
+        assert np.isfinite(a).all()
+        assert rel_l2(a, b) < 1e-5
+        # row by row: no row's slot was shared or skipped
+        per_row = np.linalg.norm(a - b, axis=1) / np.linalg.norm(b, axis=1)
+        assert per_row.max() < 1e-4
+
+
 def test_fd_check_fp64_oracle(cuda):
     N, B, dt, steps = 64, 3, 0.25, 2
     Ls = [64.0, 64.0, 50.0]
