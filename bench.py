@@ -700,7 +700,7 @@ def bench_diff(args, dev, world, which):
         mk = lambda: KSSolverTorch(SimpleNamespace(  # noqa: E731
             resolution=N, dt=cfg["dt"], device=dev, domain_size=L, alpha=torch.zeros(B, device=dev),
             time_scheme=cfg["scheme"]))
-        net = FNO1D(modes=16, width=64, layers=4).to(dev)
+        net = FNO1D(L=int(cfg["L"]), modes=16, width=64).to(dev)  # the reference's FNO corrector
     cells = B * N * steps
     u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=dev)
     with torch.no_grad():  # target: the uncorrected solver's trajectory
@@ -824,7 +824,7 @@ def bench_diff(args, dev, world, which):
             "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak, "traffic": None, "flops_per_cell_step": fpc,
             "peak_source": "FP32 FMA loop (inc_bench_fma) measured in this run"}
     cfg = dict(name=which, B=B, N=N, steps=steps, scheme=cfg["scheme"],
-               corrector=("PeriodicCNN1D(4x32ch,k5,GELU)" if which == "burgers_diff" else "FNO1D(4 layers,w64,16 modes)"))
+               corrector=("PeriodicCNN1D(4x32ch,k5,GELU)" if which == "burgers_diff" else "FNO1D(L=100, modes=16, width=64), the reference's corrector"))
     del graph, graphed  # a CUDA graph holding NCCL calls must be released before the process group
     torch.cuda.synchronize()
     return cfg, cells, times, extra
@@ -914,7 +914,8 @@ def diff_checks(which, net, cfg, dev, rows=4, fwd_steps=10, grad_steps=8, direct
     N = cfg["N"]
     u0_np = np.asarray(cfg["u0"], dtype=np.float64)[:rows]
     rng = np.random.default_rng(11)
-    net64 = copy.deepcopy(net).double().cpu()
+    from inc_b200.correctors import fp64_copy
+    net64 = fp64_copy(net).cpu()
     params64 = list(net64.parameters())
     if which == "burgers_diff":
         p = ob.BurgersParams(resolution=N, L=cfg["L"], dt=cfg["dt"], nu=cfg["nu"])
@@ -962,7 +963,8 @@ def diff_checks(which, net, cfg, dev, rows=4, fwd_steps=10, grad_steps=8, direct
     fr, _ = simulate_rollout(net, mk(), u0g, grad_steps, "INC", L_dev, checkpoint_every=4)
     (fr * torch.tensor(wgt, dtype=torch.float32, device=dev)).sum().backward()
     g_u = u0g.grad.double().cpu().numpy()
-    g_p = [q.grad.double().cpu().numpy() for q in net.parameters()]
+    g_p = [(torch.view_as_real(q.grad) if q.is_complex() else q.grad).double().cpu().numpy()
+           for q in net.parameters()]
     net.zero_grad()
 
     def loss64(u):
@@ -974,12 +976,15 @@ def diff_checks(which, net, cfg, dev, rows=4, fwd_steps=10, grad_steps=8, direct
             fd = (loss64(u0_np + h * d) - loss64(u0_np - h * d)) / (2 * h)
             errs_u.append(abs(float((g_u * d).sum()) - fd) / max(abs(fd), 1e-12))
         for _ in range(directions):  # in the parameters
-            ds = [rng.standard_normal(tuple(q.shape)) for q in params64]
+            # a complex parameter (the FNO's weights1) moves along a complex direction; its
+            # directional derivative is sum(Re g Re d + Im g Im d) with torch's complex gradient
+            ds = [rng.standard_normal(tuple(q.shape) + ((2,) if q.is_complex() else ())) for q in params64]
             base = [q.detach().clone() for q in params64]
             vals = []
             for sign in (1.0, -1.0):
                 for q, b, d in zip(params64, base, ds):
-                    q.copy_(b + sign * h * torch.from_numpy(d))
+                    dt = torch.from_numpy(d)
+                    q.copy_(b + sign * h * (torch.view_as_complex(dt) if q.is_complex() else dt))
                 vals.append(loss64(u0_np))
             for q, b in zip(params64, base):
                 q.copy_(b)

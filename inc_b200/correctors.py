@@ -4,12 +4,11 @@ Two architectures from the benchmark configurations:
 
 * ``PeriodicCNN1D`` - 4 circular Conv1d layers (32 channels, kernel 5) with
   GELU between them: [B, N] -> [B, N].
-* ``FNO1D`` - a Fourier neural operator (Li et al., 2021): lift (u, x/L grid)
-  to `width` channels, 4 layers of spectral convolution (keep the lowest
-  `modes` rFFT modes, complex weights) plus a 1x1 convolution, GELU between
-  layers, project with two linear layers.  ``forward(u, L)`` takes the
-  per-trajectory domain size like the reference's FNO corrector
-  (models/models_1d/fno.py:39-105) does.
+* ``FNO1D`` - the reference's FNO corrector (models/models_1d/fno.py:39-105):
+  the same constructor ``FNO1D(L=16, modes=16, width=64)``, submodules and
+  parameter names (fc0, conv0..3 with complex ``weights1``, w0..3, fc1, fc2), so
+  a reference state_dict loads unchanged, and the same ``forward(u, L=None)``
+  with the grid of ``get_grid`` (models/models_1d/utils.py:3-31).
 
 On CUDA tensors each FNO layer's ``spectral(x) + W x + b`` runs through
 ``inc_spectral_conv1d`` with a hand-written adjoint.  Its kernels are streaming
@@ -153,17 +152,44 @@ def spectral_conv1d(x, w_re, w_im, modes: int, bias=None, addend=None):
 
 
 class SpectralConv1d(nn.Module):
-    """Multiply the lowest `modes` rFFT modes by learned complex in x out matrices."""
+    """The reference's Fourier layer (models/models_1d/fno.py:6-37), same constructor
+    and parameter: ``weights1`` [in, out, modes1] complex64, drawn as
+    scale * (U[0,1) + i U[0,1)) with scale = 1 / (in * out), so its state_dict loads
+    unchanged.  forward(x [B, in, n]) -> [B, out, n]: rfft, the lowest modes1 modes
+    mixed by weights1, irfft; on CUDA through ``inc_spectral_conv1d``."""
 
-    def __init__(self, cin: int, cout: int, modes: int):
+    def __init__(self, in_channels: int, out_channels: int, modes1: int):
         super().__init__()
-        self.modes = modes
-        scale = 1.0 / (cin * cout)
-        self.w_re = nn.Parameter(scale * torch.rand(cin, cout, modes))
-        self.w_im = nn.Parameter(scale * torch.rand(cin, cout, modes))
+        self.in_channels = in_channels
+        self.out_channels = out_channels
+        self.modes1 = modes1
+        self.scale = 1 / (in_channels * out_channels)
+        self.weights1 = nn.Parameter(self.scale * torch.rand(in_channels, out_channels, modes1, dtype=torch.cfloat))
 
-    def forward(self, x):
-        return spectral_conv1d(x, self.w_re, self.w_im, self.modes)
+    def weights_re_im(self, dtype):
+        """(re, im) views of weights1 in `dtype` (gradients flow back to weights1)."""
+        w = self.weights1
+        if dtype == torch.float64 and w.dtype != torch.complex128:
+            w = w.to(torch.complex128)
+        wr = torch.view_as_real(w)
+        return wr[..., 0], wr[..., 1]
+
+    def forward(self, x, bias=None, addend=None):
+        w_re, w_im = self.weights_re_im(x.dtype)
+        return spectral_conv1d(x, w_re, w_im, self.modes1, bias=bias, addend=addend)
+
+
+def get_grid(x, L):
+    """Grid coordinates [B, D] of models/models_1d/utils.py:3-31: a float or int L gives
+    linspace(0, L, D) for every row, a tensor L ([B] or [B, 1]) gives L[b] *
+    linspace(0, 1, D); anything else raises ValueError."""
+    B, D = x.shape[:2]
+    if isinstance(L, (float, int)):
+        return torch.linspace(0, L, steps=D, dtype=x.dtype, device=x.device).expand(B, D)
+    if isinstance(L, torch.Tensor):
+        base = torch.linspace(0, 1, steps=D, dtype=x.dtype, device=x.device)
+        return L.reshape(B, 1).to(x.dtype) * base
+    raise ValueError("L must be a float, int, or a torch.Tensor")
 
 
 def _channel_mm(w, x):
@@ -220,33 +246,57 @@ def _channel_linear(lin: nn.Linear, x):
 
 
 class FNO1D(nn.Module):
-    def __init__(self, modes: int = 16, width: int = 64, layers: int = 4):
-        super().__init__()
-        self.lift = nn.Linear(2, width)
-        self.spectral = nn.ModuleList(SpectralConv1d(width, width, modes) for _ in range(layers))
-        self.pointwise = nn.ModuleList(nn.Conv1d(width, width, 1) for _ in range(layers))
-        self.proj1 = nn.Linear(width, 128)
-        self.proj2 = nn.Linear(128, 1)
+    """The reference's FNO corrector (models/models_1d/fno.py:39-105), same constructor
+    ``FNO1D(L=16, modes=16, width=64)``, same submodules and parameter names (fc0,
+    conv0..conv3 with complex weights1, w0..w3, fc1, fc2), so a state_dict trained with
+    the reference loads unchanged; forward(x [B, D], L=None) -> [B, D] with the grid of
+    ``get_grid(x, L if L is not None else self.L)``.
 
-    def forward(self, u, L=None):
-        B, n = u.shape
-        base = torch.linspace(0, 1, n, dtype=u.dtype, device=u.device)
-        if L is None:
-            grid = base.expand(B, n)
-        elif isinstance(L, torch.Tensor):
-            grid = L.reshape(B, 1).to(u.dtype) * base
-        else:
-            grid = float(L) * base.expand(B, n)
-        # The hidden state stays [B, width, n] (contiguous) from the lift to the
-        # projection: the Linear layers act on the channel axis as channel matmuls
-        # (same parameters, same result), so no permuted view reaches an
-        # elementwise kernel or a gradient.
-        x = _channel_linear(self.lift, torch.stack([u, grid], dim=1))
-        for i, (sc, pw) in enumerate(zip(self.spectral, self.pointwise)):
-            # sc(x) + pw(x) with pw's bias and product added in the spectral kernel's epilogue
-            x = spectral_conv1d(x, sc.w_re, sc.w_im, sc.modes, bias=pw.bias,
-                                addend=_channel_mm(pw.weight[:, :, 0], x))
-            if i + 1 < len(self.spectral):
-                x = F.gelu(x)
-        x = bias_gelu(_channel_mm(self.proj1.weight, x), self.proj1.bias)
-        return _channel_linear(self.proj2, x).squeeze(1)
+    Computed as the reference computes it, with the hidden state kept [B, width, D]
+    (contiguous) from the lift to the projection: the Linear layers act on the channel
+    axis as channel matmuls (same parameters, same result), each layer's conv_i(x) +
+    w_i(x) is one ``inc_spectral_conv1d`` call with w_i's product and bias added in its
+    epilogue, and fc1's bias and GELU are one ``inc_bias_gelu`` pass."""
+
+    def __init__(self, L=16, modes=16, width=64):
+        super().__init__()
+        self.modes1 = modes
+        self.width = width
+        self.L = L
+        self.padding = 2  # unused, as in the reference (its padding lines are commented out)
+        self.fc0 = nn.Linear(2, self.width)
+        self.conv0 = SpectralConv1d(self.width, self.width, self.modes1)
+        self.conv1 = SpectralConv1d(self.width, self.width, self.modes1)
+        self.conv2 = SpectralConv1d(self.width, self.width, self.modes1)
+        self.conv3 = SpectralConv1d(self.width, self.width, self.modes1)
+        self.w0 = nn.Conv1d(self.width, self.width, 1)
+        self.w1 = nn.Conv1d(self.width, self.width, 1)
+        self.w2 = nn.Conv1d(self.width, self.width, 1)
+        self.w3 = nn.Conv1d(self.width, self.width, 1)
+        self.fc1 = nn.Linear(self.width, 128)
+        self.fc2 = nn.Linear(128, 1)
+
+    def forward(self, x, L=None):
+        L = L if L is not None else self.L
+        grid = get_grid(x, L)
+        h = _channel_linear(self.fc0, torch.stack([x, grid], dim=1))  # [B, width, D]
+        layers = ((self.conv0, self.w0), (self.conv1, self.w1), (self.conv2, self.w2), (self.conv3, self.w3))
+        for i, (conv, w) in enumerate(layers):
+            h = conv(h, bias=w.bias, addend=_channel_mm(w.weight[:, :, 0], h))
+            if i + 1 < len(layers):
+                h = F.gelu(h)
+        h = bias_gelu(_channel_mm(self.fc1.weight, h), self.fc1.bias)
+        return _channel_linear(self.fc2, h).squeeze(1)
+
+
+def fp64_copy(net: nn.Module) -> nn.Module:
+    """A float64 copy of a corrector (for FP64 reference runs): real parameters to
+    float64 and complex ones (the FNO's weights1) to complex128, which Module.double()
+    leaves as complex64."""
+    import copy
+    out = copy.deepcopy(net).double()
+    for m in out.modules():
+        for name, prm in list(m.named_parameters(recurse=False)):
+            if prm.is_complex() and prm.dtype != torch.complex128:
+                setattr(m, name, nn.Parameter(prm.detach().to(torch.complex128)))
+    return out

@@ -294,11 +294,94 @@ def make_ks():
     np.savez_compressed(os.path.join(OUT, "ks_golden.npz"), **out)
 
 
+def _reference_fno_module():
+    """models/models_1d/fno.py imported by file path.  Its package __init__ imports
+    modules the reference does not ship, so a bare package object stands in for
+    ``models.models_1d``; fno.py's ``from .utils import get_grid`` then loads the
+    reference's utils.py from the same directory."""
+    import importlib.util
+    import types
+    name = "_ref_models_1d"
+    if name not in sys.modules:
+        pkg = types.ModuleType(name)
+        pkg.__path__ = [os.path.join(REF, "models", "models_1d")]
+        sys.modules[name] = pkg
+    if f"{name}.fno" not in sys.modules:
+        spec = importlib.util.spec_from_file_location(f"{name}.fno", os.path.join(REF, "models", "models_1d", "fno.py"))
+        m = importlib.util.module_from_spec(spec)
+        sys.modules[f"{name}.fno"] = m
+        spec.loader.exec_module(m)
+    return sys.modules[f"{name}.fno"]
+
+
+def _fno64(cls, **kw):
+    """A reference FNO1D initialised as a float32 model (the RNG stream of its default
+    construction), then run in FP64: real parameters to float64, the complex64
+    weights1 to complex128 (same values)."""
+    prev = torch.get_default_dtype()
+    torch.set_default_dtype(torch.float32)
+    try:
+        net = cls(**kw)
+    finally:
+        torch.set_default_dtype(prev)
+    for m in net.modules():
+        for pn, prm in list(m.named_parameters(recurse=False)):
+            dt = torch.complex128 if prm.is_complex() else torch.float64
+            setattr(m, pn, torch.nn.Parameter(prm.detach().to(dt)))
+    return net
+
+
+def make_fno():
+    """The reference's FNO corrector (models/models_1d/fno.py:39-105) in FP64: outputs for
+    the three grid forms of get_grid (L=None -> self.L, a float, a per-row tensor) and
+    gradients of a weighted sum w.r.t. the input and every parameter.  Small case: all
+    parameters and gradients stored.  Benchmark-sized case (width 64, 16 modes): the
+    network is rebuilt from its seed, so only parameter checksums, outputs, the input
+    gradient and each parameter gradient's projection on a seeded direction are stored."""
+    FNO1D = _reference_fno_module().FNO1D
+    rng = np.random.default_rng(55)
+    out = {}
+    for name, seed, kw, (B, N) in (("f_small", 21, dict(L=16, modes=4, width=8), (3, 32)),
+                                   ("f_bench", 22, dict(L=16, modes=16, width=64), (2, 128))):
+        torch.manual_seed(seed)
+        net = _fno64(FNO1D, **kw)
+        x = torch.from_numpy(rng.standard_normal((B, N)))
+        Lt = torch.from_numpy(rng.uniform(20, 60, B))
+        out[f"{name}.seed"] = np.int64(seed)
+        out[f"{name}.kw"] = np.array([kw["L"], kw["modes"], kw["width"]], dtype=np.int64)
+        out[f"{name}.x"] = x.numpy()
+        out[f"{name}.Lt"] = Lt.numpy()
+        with torch.no_grad():
+            out[f"{name}.y_none"] = net(x).numpy()
+            out[f"{name}.y_float"] = net(x, 5.0).numpy()
+        xg = x.clone().requires_grad_(True)
+        y = net(xg, Lt)
+        w = torch.from_numpy(rng.standard_normal((B, N)))
+        grads = torch.autograd.grad((y * w).sum(), [xg] + list(net.parameters()))
+        out[f"{name}.y_tensor"] = y.detach().numpy()
+        out[f"{name}.w"] = w.numpy()
+        out[f"{name}.grad_x"] = grads[0].numpy()
+        g = torch.Generator().manual_seed(seed)
+        for (pn, prm), gp in zip(net.named_parameters(), grads[1:]):
+            d = torch.randn(prm.shape, generator=g, dtype=torch.float64)
+            gr = torch.view_as_real(gp).double() if gp.is_complex() else gp.double()
+            pr = torch.view_as_real(prm.detach()).double() if prm.is_complex() else prm.detach().double()
+            if gp.is_complex():
+                d = torch.stack([d, torch.randn(prm.shape, generator=g, dtype=torch.float64)], -1)
+            out[f"{name}.pgrad_proj.{pn}"] = np.float64((gr * d).sum())
+            out[f"{name}.param_sum.{pn}"] = np.float64(pr.sum())
+            if name == "f_small":
+                out[f"{name}.param.{pn}"] = pr.numpy()
+                out[f"{name}.pgrad.{pn}"] = gr.numpy()
+    np.savez_compressed(os.path.join(OUT, "fno_golden.npz"), **out)
+
+
 def make_hybrid():
     """A corrector network in the loop: s = net(u) before every reference step()
     (trainer_1d.py:168-175), loss = MSE(frames, target), FP64 autograd."""
     sys.path.insert(0, os.path.dirname(os.path.dirname(OUT)))
-    from inc_b200.correctors import FNO1D, PeriodicCNN1D
+    from inc_b200.correctors import PeriodicCNN1D
+    FNO1D = _reference_fno_module().FNO1D
     rng = np.random.default_rng(77)
     out = {}
     # Burgers, SSP-RK3 and Euler, with a periodic CNN corrector
@@ -332,7 +415,7 @@ def make_hybrid():
     name = "h_ks"
     B, N, steps, dt = 2, 32, 2, 0.2
     Ls = [32.0, 40.0]
-    net = FNO1D(modes=4, width=8, layers=2)
+    net = _fno64(FNO1D, L=16, modes=4, width=8)  # the reference's own FNO corrector
     ds = torch.tensor(Ls)
     sp = SimpleNamespace(resolution=N, dt=dt, device="cpu", domain_size=ds, alpha=torch.zeros(B),
                          time_scheme="ETRK2")
@@ -417,7 +500,8 @@ def make_analysis_and_data():
 
 def main():
     import argparse
-    gens = {"burgers": make_burgers, "ks": make_ks, "hybrid": make_hybrid, "analysis_data": make_analysis_and_data}
+    gens = {"burgers": make_burgers, "ks": make_ks, "hybrid": make_hybrid, "analysis_data": make_analysis_and_data,
+            "fno": make_fno}
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
     ap.add_argument("--reference", default=os.environ.get("INC_REFERENCE"),
                     help="checkout of the reference (default: $INC_REFERENCE; required)")

@@ -202,8 +202,11 @@ def test_rollout_backward_matches_stepwise(cuda, scheme):
     s2 = s0.clone().requires_grad_(True)
     fr = burgers_rollout(b, u2, steps, s=s2, ckpt_every=8)
     gb = torch.autograd.grad((fr * w).sum(), (u2, s2))
+    # the fused forward carries its update rounding from step to step (compensated
+    # summation) and the per-step launches do not, so the states the two backward
+    # passes linearise at differ by FP32 rounding: equal to 1e-5, not to the last bit
     for x1, x2 in zip(ga, gb):
-        assert rel_l2(x2.cpu().numpy(), x1.cpu().numpy()) < 1e-6
+        assert rel_l2(x2.cpu().numpy(), x1.cpu().numpy()) < 1e-5
 
 
 _WARP_CPT = {64: 4, 128: 4, 256: 8, 512: 16}

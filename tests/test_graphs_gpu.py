@@ -33,7 +33,7 @@ def test_graphed_ks_fno_matches_eager(cuda):
     def solver():
         return KSSolverTorch(SimpleNamespace(resolution=N, dt=0.05, device=cuda, domain_size=L,
                                              alpha=torch.zeros(B, device=cuda), time_scheme="ETRK2"))
-    net = FNO1D(modes=4, width=8, layers=2).to(cuda)
+    net = FNO1D(L=16, modes=4, width=8).to(cuda)
     g = torch.Generator().manual_seed(1)
     u_a = torch.randn(B, N, generator=g).to(cuda)
     u_b = torch.randn(B, N, generator=g).to(cuda)

@@ -203,5 +203,6 @@ def test_spectral_conv_dispatch_on_cpu():
     torch.manual_seed(0)
     layer = SpectralConv1d(8, 8, 4)
     x = torch.randn(3, 8, 32)
-    assert not spectral_conv_supported(x, layer.w_re, layer.w_im, 4)
-    torch.testing.assert_close(layer(x), spectral_conv1d_torch(x, layer.w_re, layer.w_im, 4), rtol=0, atol=0)
+    w_re, w_im = layer.weights_re_im(x.dtype)
+    assert not spectral_conv_supported(x, w_re, w_im, 4)
+    torch.testing.assert_close(layer(x), spectral_conv1d_torch(x, w_re, w_im, 4), rtol=0, atol=0)
