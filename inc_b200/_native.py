@@ -59,8 +59,11 @@ SIGNATURES = {
                                       C.c_int32, _vp, _vp]),
     "inc_burgers_rollout_bwd": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, C.c_int32, C.c_int32,
                                           _vp, _vp, _vp, _vp, _vp]),
+    "inc_burgers_step_adaptive_work_size": (C.c_int64, [C.c_int32]),
     "inc_burgers_step_adaptive": (C.c_int, [C.POINTER(BurgersDesc), C.c_float, C.c_int32, _vp, _vp, _vp,
                                             C.c_double, _vp, _vp, _vp, _vp, _vp]),
+    "inc_burgers_step_adaptive_bwd": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, _vp, C.c_int32,
+                                                C.c_int32, _vp, _vp, _vp, _vp, _vp]),
     "inc_burgers_terms": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, C.c_double, _vp, _vp, _vp, _vp]),
     "inc_ks_substep": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, _vp, _vp]),
     "inc_ks_substep_bwd": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, _vp, _vp, _vp, _vp]),

@@ -1,15 +1,10 @@
-// Burgers: ragged persistent batch and device-side adaptive-CFL stepping.
+// Burgers: ragged persistent batch and the reference's term methods.
 //
 // Ragged batch: rows of different n / nu / dt / dx packed back to back.  A
 // persistent grid of warps pulls row indices from one atomic counter
 // (fetch-and-add only, no waiting) in the caller's longest-first order; each
 // warp advances its row (or, for rows narrower than 128, 32 / (n/4) rows of one
 // width, one per lane group) through all steps with the state in registers.
-//
-// Adaptive step (solver_1d.py:148-179): Euler substeps with
-// dt_local = min(remaining, CFL * dx / max|u|) where the max runs over the
-// whole batch.  One CTA does it all with block barriers, so the substep loop
-// needs no host round trip and no inter-CTA waiting.
 #include "burgers_kernels.cuh"
 
 namespace inc {
@@ -107,79 +102,6 @@ __global__ void __launch_bounds__(256) k_ragged(RaggedArgs ra) {
             const int nn = __ldg(ra.n_rows + r);
             if (nn == n) continue;
             ragged_dispatch(ra, nn, (lane < (nn >= 128 ? 32 : nn / 4)) ? r : -1, lane);
-        }
-    }
-}
-
-// ---- adaptive CFL ---------------------------------------------------------------
-struct AdaptArgs {
-    Args a;
-    float* work;       // u in/out lives in a.out
-    float* t_out;      // [rows] or null
-    int* substeps_out;
-    float cfl;
-    int max_substeps;
-    double dt_total;
-};
-
-template <int CPT, int TPR>
-__global__ void __launch_bounds__(1024) k_adaptive(AdaptArgs ad) {
-    __shared__ float red[32];
-    __shared__ double sh_dt;
-    __shared__ int sh_go;
-    const Args& a = ad.a;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
-    const int rows_per_warp = 32 / TPR;
-    const int g = lane % TPR;
-    const int left = (g + TPR - 1) & (TPR - 1), right = (g + 1) & (TPR - 1);
-    double target = ad.dt_total, tacc = 0.0;
-    int substeps = 0;
-    for (int it = 0;; ++it) {
-        // global max |u| over the batch (solver_1d.py:158)
-        float m = 0.f;
-        for (int r0 = warp * rows_per_warp; r0 < a.rows; r0 += nwarps * rows_per_warp) {
-            const int row = r0 + lane / TPR;
-            float u[CPT];
-            load_row_chunk<CPT>(u, a.out + (int64_t)row * a.n + g * CPT, row < a.rows);
-#pragma unroll
-            for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
-        }
-        m = group_max_nonneg<32>(m);
-        if (lane == 0) red[warp] = m;
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            float mx = 0.f;
-            for (int w = 0; w < nwarps; ++w) mx = fmaxf(mx, red[w]);
-            const double allowed = mx > 0.f ? (double)ad.cfl * (double)a.dx / (double)mx : target;
-            sh_dt = target < allowed ? target : allowed;
-            sh_go = target > 0.0;
-        }
-        __syncthreads();
-        if (!sh_go) break;
-        const double dtl = sh_dt;
-        for (int r0 = warp * rows_per_warp; r0 < a.rows; r0 += nwarps * rows_per_warp) {
-            const int row = r0 + lane / TPR;
-            const bool valid = row < a.rows;
-            Ctx<CPT> cx;
-            make_ctx<CPT, TPR>(a, row, g, valid, cx);
-            cx.dt = (float)dtl;
-            float u[CPT];
-            float* p = a.out + (int64_t)(valid ? row : 0) * a.n + g * CPT;
-            load_row_chunk<CPT>(u, p, valid);
-            advance<CPT, TPR>(a, cx, u, cx.t + (float)tacc, left, right);
-            store_row_chunk<CPT>(p, u, valid);
-        }
-        tacc += dtl;
-        target -= dtl;
-        __syncthreads();  // all rows written before the next max
-        if (target > 0.0 && (int)ceil(target / dtl) > ad.max_substeps) break;  // :173-176
-        ++substeps;
-    }
-    if (threadIdx.x == 0 && ad.substeps_out) *ad.substeps_out = substeps;
-    if (ad.t_out) {
-        for (int r = threadIdx.x; r < a.rows; r += blockDim.x) {
-            const float t0 = a.t_rows ? a.t_rows[r] : a.t0;
-            ad.t_out[r] = (float)((double)t0 + tacc);
         }
     }
 }
@@ -298,32 +220,4 @@ extern "C" int inc_burgers_ragged_rollout(const inc_burgers_ragged_desc* d, cons
     if (e != cudaSuccess) { set_error("ragged_rollout: %s", cudaGetErrorString(e)); return INC_E_LAUNCH; }
     k_ragged<<<grid, block, 0, st>>>(ra);
     return check_launch("ragged_rollout");
-}
-
-extern "C" int inc_burgers_step_adaptive(const inc_burgers_desc* d, float cfl, int32_t max_substeps, const float* u,
-                                         const float* s, const float* t_rows, double t0, float* u_out, float* t_out,
-                                         float* work, int32_t* substeps_out, void* stream) {
-    AdaptArgs ad;
-    int rc = fill_args(d, ad.a);
-    if (rc) return rc;
-    if (!u || !u_out || !(cfl > 0.f) || max_substeps <= 0) { set_error("step_adaptive: bad arguments"); return INC_E_INVALID; }
-    if (d->scheme != INC_TS_EULER) { set_error("step_adaptive: the reference sub-steps with forward Euler only"); return INC_E_INVALID; }
-    ad.a.s = s; ad.a.t_rows = t_rows; ad.a.t0 = (float)t0; ad.a.out = u_out;
-    ad.work = work; ad.t_out = t_out; ad.substeps_out = substeps_out; ad.cfl = cfl; ad.max_substeps = max_substeps;
-    ad.dt_total = (double)d->dt;
-    cudaStream_t st = as_stream(stream);
-    if (u != u_out) {
-        cudaError_t e = cudaMemcpyAsync(u_out, u, (size_t)d->rows * d->n * sizeof(float), cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) { set_error("step_adaptive: %s", cudaGetErrorString(e)); return INC_E_LAUNCH; }
-    }
-    const int n = d->n;
-    const int cpt = n <= 128 ? 4 : (n <= 256 ? 8 : 16);
-    const int tpr = n / cpt;
-    if (!is_pow2(n) || n < 8 || n > 512) { set_error("step_adaptive: n must be a power of two in [8,512]"); return INC_E_UNSUPPORTED; }
-#define INC_A(C, T) \
-    if (cpt == C && tpr == T) { k_adaptive<C, T><<<1, 1024, 0, st>>>(ad); return check_launch("step_adaptive"); }
-    INC_A(4, 2) INC_A(4, 4) INC_A(4, 8) INC_A(4, 16) INC_A(4, 32) INC_A(8, 32) INC_A(16, 32)
-#undef INC_A
-    set_error("step_adaptive: no kernel for n=%d", n);
-    return INC_E_UNSUPPORTED;
 }

@@ -16,7 +16,7 @@
  *      _compute_source :104, _apply_corrections :116, forward Euler :192;
  *      SSP-RK3 composed on the same right-hand side)
  *   autograd backward through BurgersSolverTorch.step -> inc_burgers_step_bwd
- *   BurgersSolverTorch.step_adaptive(u)           :148-179 -> inc_burgers_step_adaptive
+ *   BurgersSolverTorch.step_adaptive(u)           :148-179 -> inc_burgers_step_adaptive (+ _bwd)
  *   calc_nonlinear_weno / _FDM, calc_linear, _compute_source
  *                                   :104-146 -> inc_burgers_terms
  *   simulate_rollout(model=None, BurgersSolverTorch) trainer/trainer_1d.py:154-183
@@ -160,14 +160,34 @@ int inc_burgers_terms(const inc_burgers_desc* d, const float* u, const float* t_
 
 /* Adaptive-CFL Euler sub-stepping over one dt with the global max |u|
  * (solver_1d.py:148-179), all on the device: no host synchronisation.  One
- * CTA runs the whole batch (block barriers between substeps).  t_out [rows]
- * (or NULL) receives t + sum(dt_local); substeps_out (device int32, or NULL)
- * the substep count.  work is reserved and may be NULL.                     */
+ * cooperative launch spreads the rows over every SM; a grid barrier between
+ * substeps lets all CTAs take dt_local = min(remaining, cfl dx / max|u|) from
+ * the same batch maximum; the loop stops as the reference's does (remaining
+ * time spent, or ceil(remaining / dt_local) > max_substeps).  t_out [rows] (or
+ * NULL) receives t + sum(dt_local); substeps_out (device int32, or NULL) the
+ * reference's substep count.  work: inc_burgers_step_adaptive_work_size(
+ * max_substeps) bytes of device memory, 256-byte aligned, which receives the
+ * run: int32 at byte 20 = error (0 ok; 1 a barrier wait gave up; 2 more than
+ * max_substeps + 1 substeps), int32 at byte 24 = substeps run, then the
+ * dt_local and time offset of each (read by inc_burgers_step_adaptive_bwd).  */
+int64_t inc_burgers_step_adaptive_work_size(int32_t max_substeps);
 int inc_burgers_step_adaptive(const inc_burgers_desc* d, float cfl,
                               int32_t max_substeps, const float* u,
                               const float* s, const float* t_rows, double t0,
-                              float* u_out, float* t_out, float* work,
+                              float* u_out, float* t_out, void* work,
                               int32_t* substeps_out, void* stream);
+/* Vector-Jacobian product of one inc_burgers_step_adaptive call with its
+ * substep sizes held constant (as autograd through the reference, whose
+ * dt_local comes from .item()): the run recorded in `work` (same max_substeps;
+ * `executed` = its substeps run, read from work by the caller) is replayed from
+ * u with its states in `states` ([executed][rows][n] floats of device scratch),
+ * then differentiated in reverse.  g_s (dL/d correction_s) may be NULL.       */
+int inc_burgers_step_adaptive_bwd(const inc_burgers_desc* d, const float* u,
+                                  const float* s, const float* t_rows, double t0,
+                                  const void* work, int32_t max_substeps,
+                                  int32_t executed, const float* g_out,
+                                  float* g_u, float* g_s, float* states,
+                                  void* stream);
 
 /* Ragged batch: every row advances `steps` steps in one persistent launch.
  * queue: one device int32 of caller memory, zeroed by this call.            */
