@@ -81,6 +81,9 @@ def burgers_step_adaptive(solver, u):
     if s is not None:
         _check_state(s, solver.resolution, "correction_s")
     rows = u.shape[0]
+    # the step's start time for every row (the forcing source reads it; t_out is built on it
+    # whatever the equation type)
+    launch._bind_time(solver.t, rows)
     t_out = torch.empty(rows, device=u.device, dtype=torch.float32)
     subs = torch.zeros(1, device=u.device, dtype=torch.int32)
     out = AdaptiveStepFn.apply(u, s, launch, solver.adaptive_CFL, t_out, subs)
