@@ -408,12 +408,21 @@ def bench_ks(args, dev, world):
             g_s.add_(gsk)
             ga.copy_(gb)
 
+    tape = torch.empty(plan.tape_size(steps), dtype=torch.uint8, device=dev)  # 1.3 GB at 1024 x 256 x 400
+
+    def fused_fb_tape():  # the forward records every step's states; the backward replays nothing
+        plan.rollout_tape(u0, s, steps, frames, None, tape)
+        plan.rollout_bwd_tape(tape, s, steps, g_frames, None, g_u0, g_s)
+
     for _ in range(max(1, args.warmup)):
         fused_fb()
+        fused_fb_tape()
         plain_fb()
     torch.cuda.synchronize()
     t_ffb = event_time(fused_fb, max(2, args.steps // 2), flush)
+    t_ffbt = event_time(fused_fb_tape, max(2, args.steps // 2), flush)
     t_pfb = event_time(plain_fb, 2, flush)
+    del tape
 
     # --- e2e through the public API with host buffers -----------------------------
     u_final_h = torch.empty(B, N).pin_memory()
@@ -442,7 +451,8 @@ def bench_ks(args, dev, world):
     plain_ms_step = sum(t_plain) / len(t_plain) / steps
     times = dict(fused=ms_fused, plain=sum(t_plain) / len(t_plain), graph=sum(t_graph) / len(t_graph),
                  fused_fb=sum(t_ffb) / len(t_ffb), plain_fb=sum(t_pfb) / len(t_pfb),
-                 e2e=sum(t_e2e) / len(t_e2e), dealias=sum(t_dealias) / len(t_dealias))
+                 e2e=sum(t_e2e) / len(t_e2e), dealias=sum(t_dealias) / len(t_dealias),
+                 fused_fb_tape=sum(t_ffbt) / len(t_ffbt))
     cfg["dealias"] = ("as the reference: its 3/2 physical-space padding is a no-op (solver_1d.py:228-233); "
                       "the opt-in 2/3 rule is timed as plain.fused_dealias_2_3")
     extra = dict(
@@ -662,6 +672,36 @@ def bench_burgers_batched(args, dev, world):
     cfg = dict(name="burgers_batched", B=cfg["rows"], N="64..512", steps=steps, scheme=cfg["scheme"],
                layout=cfg["layout"])
     return cfg, cells, times, extra
+
+
+def bench_adaptive(dev, reps=5):
+    """One adaptive-CFL step (solver_1d.py:148-179) on 4096 x 256 rows, dt spanning about ten
+    substeps, beside one fixed-dt Euler step of the same batch: the cooperative kernel's cost
+    per substep against a plain step launch (both CUDA-event timed, inputs in L2)."""
+    import math
+    import torch
+    from types import SimpleNamespace
+    from inc_b200.solvers import BurgersSolverTorch
+    from inc_b200.workloads import burgers_plain_config
+    B, N = 4096, 256
+    cfg = burgers_plain_config(B=B, N=N)
+    u0 = torch.tensor(cfg["u0"], dtype=torch.float32, device=dev)
+    mk = lambda cfl: BurgersSolverTorch(SimpleNamespace(  # noqa: E731
+        resolution=N, dt=0.05, x=None, adaptive_CFL=cfl, L=2 * math.pi, nu=0.01, device=dev,
+        convection_term="WENO", equation_type="viscosity", batch_size=B, time_scheme="euler"))
+    ad, fx = mk(0.2), mk(None)
+    with torch.no_grad():
+        for _ in range(3):
+            ad.step(u0)
+            fx.step(u0)
+        torch.cuda.synchronize()
+        t_ad = min(event_time(lambda: ad.step(u0), reps))
+        subs = ad.last_substeps
+        t_fx = min(event_time(lambda: fx.step(u0), reps))
+    return {"batch": B, "n": N, "dt": 0.05, "cfl": 0.2, "substeps": subs, "adaptive_step_ms": t_ad,
+            "fixed_dt_step_ms": t_fx, "adaptive_ms_per_substep": t_ad / max(subs, 1),
+            "per_substep_over_fixed_step": t_ad / max(subs, 1) / t_fx,
+            "kernel": "k_adaptive_grid (one cooperative launch, grid barrier per substep)"}
 
 
 # ----------------------------------------------------------------------------
@@ -1136,6 +1176,12 @@ def plain_line(args, world, cfg, cells, times, extra, cpu_b):
             p["fwd_bwd"] = "no backward: the ragged batch is a forward-only workload"
         if "dealias" in times:
             p["fused_dealias_2_3"] = rate(times["dealias"])
+        if "fused_fb_tape" in times:
+            p["fwd_bwd_fused_tape"] = rate(times["fused_fb_tape"])
+            p["fwd_bwd_fused_tape_over_per_step"] = times["plain_fb"] / times["fused_fb_tape"]
+            p["fwd_bwd_fused_tape_is"] = ("the forward records every step's states in a device tape "
+                                          "(inc_ks_rollout_tape) and the backward reads them instead of "
+                                          "replaying checkpointed segments")
         if "api" in times:
             p["api_step_eager"] = rate(times["api"])
             p["api_step_ms"] = times["api"] / cfg["steps"]
@@ -1205,6 +1251,7 @@ def main():
                         else plain_line(sub, world, c, n, t, e, None))
                 blocks[name] = compact_block(full)
         if rank == 0:
+            blocks["burgers_adaptive"] = bench_adaptive(dev)
             line["configs"] = blocks
     if rank == 0:
         print(json.dumps(line), flush=True)

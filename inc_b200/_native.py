@@ -80,6 +80,10 @@ SIGNATURES = {
     "inc_ks_rollout_bwd_work_size": (C.c_int64, [C.POINTER(KSPlan), C.c_int32]),
     "inc_ks_rollout_bwd_ws": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, C.c_int32, C.c_int32, _vp, _vp, _vp, _vp,
                                         _vp, C.c_int64, _vp]),
+    "inc_ks_tape_size": (C.c_int64, [C.POINTER(KSPlan), C.c_int32]),
+    "inc_ks_rollout_tape": (C.c_int, [C.POINTER(KSPlan), _vp, _vp, C.c_int32, _vp, _vp, _vp, C.c_int64, _vp]),
+    "inc_ks_rollout_bwd_tape": (C.c_int, [C.POINTER(KSPlan), _vp, C.c_int64, _vp, C.c_int32, _vp, _vp, _vp, _vp,
+                                          _vp]),
     "inc_bench_fma": (C.c_int, [_vp, C.c_int32, C.c_int32, _vp]),
     "inc_energy_spectrum": (C.c_int, [_vp, _vp, C.c_int32, C.c_int32, _vp]),
     "inc_spectral_conv1d": (C.c_int, [_vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, C.c_int32, C.c_int32, C.c_int32,

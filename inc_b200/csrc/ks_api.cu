@@ -121,7 +121,7 @@ int pick_block(Kind kind, int npairs, int T, int n, int K) {
     auto smem = [&](int b) {
         const int groups = b / T;
         int64_t per = 2 * (n + n / 4 + 64) + 16;  // bound on the exchange buffers' padded layouts
-        if (kind == Kind::StepBwd || kind == Kind::RolloutBwd) per += 5 * n;
+        if (kind == Kind::StepBwd || kind == Kind::RolloutBwd || kind == Kind::TapeBwd) per += 5 * n;
         if (kind == Kind::RolloutBwd) per += (int64_t)K * n;
         return (int64_t)(4 * n + groups * per) * 8;
     };
@@ -138,7 +138,7 @@ int dispatch(Kind kind, const inc_ks_plan* p, const Args& a, cudaStream_t st) {
     }
     const int P = n / T;
     const int block = pick_block(kind, a.npairs, T, n, a.ckpt_every);
-    const bool bwd = kind == Kind::StepBwd || kind == Kind::RolloutBwd;
+    const bool bwd = kind == Kind::StepBwd || kind == Kind::RolloutBwd || kind == Kind::TapeBwd;
 #define INC_CASE(PP, TT) \
     if (P == PP && T == TT) return bwd ? launch_bwd<PP, TT>(kind, a, st, block) : launch_fwd<PP, TT>(kind, a, st, block);
     INC_KS_SHAPES(INC_CASE)
@@ -301,4 +301,49 @@ extern "C" int inc_ks_rollout_bwd_ws(const inc_ks_plan* p, const float* ckpts, c
         return INC_E_INVALID;
     }
     return ks_rollout_bwd(p, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s, work, stream);
+}
+
+// ---- tape rollouts: the forward records every step's states, the backward reads them
+// Row pairs rounded up to 32: the padding absorbs the writes of launched groups past the
+// last pair (at most 32 groups per block for the narrowest layout).
+extern "C" int64_t inc_ks_tape_size(const inc_ks_plan* p, int32_t steps) {
+    if (!p || p->npairs <= 0 || steps <= 0) return -1;
+    const int64_t pairs = ((int64_t)p->npairs + 31) / 32 * 32;
+    return pairs * steps * 4 * p->n * (int64_t)sizeof(float2);
+}
+
+static int check_tape(const inc_ks_plan* p, int32_t steps, const void* tape, int64_t tape_bytes, const char* who) {
+    const int64_t need = inc_ks_tape_size(p, steps);
+    if (need < 0) { set_error("%s: bad plan or steps", who); return INC_E_INVALID; }
+    if (!tape || tape_bytes < need || (reinterpret_cast<uintptr_t>(tape) & 15u)) {
+        set_error("%s: tape needs %lld bytes, 16-byte aligned (got %lld)", who, (long long)need, (long long)tape_bytes);
+        return INC_E_INVALID;
+    }
+    return INC_OK;
+}
+
+extern "C" int inc_ks_rollout_tape(const inc_ks_plan* p, const float* u0, const float* s, int32_t steps,
+                                   float* frames, float* u_final, void* tape, int64_t tape_bytes, void* stream) {
+    Args a;
+    int rc = fill_args(p, a);
+    if (rc) return rc;
+    if (!ok_ptr(u0) || steps <= 0) { set_error("ks_rollout_tape: bad arguments"); return INC_E_INVALID; }
+    rc = check_tape(p, steps, tape, tape_bytes, "ks_rollout_tape");
+    if (rc) return rc;
+    a.u = u0; a.s = s; a.steps = steps; a.frames = frames; a.out = u_final; a.tape = static_cast<float2*>(tape);
+    return dispatch(Kind::Rollout, p, a, as_stream(stream));
+}
+
+extern "C" int inc_ks_rollout_bwd_tape(const inc_ks_plan* p, const void* tape, int64_t tape_bytes, const float* s,
+                                       int32_t steps, const float* g_frames, const float* g_final, float* g_u0,
+                                       float* g_s, void* stream) {
+    Args a;
+    int rc = fill_args(p, a);
+    if (rc) return rc;
+    if (!ok_ptr(g_u0) || steps <= 0) { set_error("ks_rollout_bwd_tape: bad arguments"); return INC_E_INVALID; }
+    rc = check_tape(p, steps, tape, tape_bytes, "ks_rollout_bwd_tape");
+    if (rc) return rc;
+    a.s = s; a.steps = steps; a.tape = const_cast<float2*>(static_cast<const float2*>(tape));
+    a.g_frames = g_frames; a.g_final = g_final; a.g_u = g_u0; a.g_s = g_s;
+    return dispatch(Kind::TapeBwd, p, a, as_stream(stream));
 }

@@ -536,6 +536,7 @@ struct Args {
     const float* coef;    // [rows][3][nhp]: exp(L dt), phi1, phi2
     const float2* tw;     // [N] FFT twiddles (layout of fft())
     float2* stage;        // rollout backward scratch: per launched group [ckpt_every][3][N] (or null)
+    float2* tape;         // rollout tape: per row pair [steps][4][N], lane layout (or null)
     int rows, n, npairs, scheme, split, dealias, steps, ckpt_every, nhp;
     int substeps;         // k_step / k_step_bwd: 1 = one substep (etd1_step / etrk2_step), else a step()
     float invN;
@@ -760,10 +761,20 @@ INC_DEV void st_get(float2 (&v)[P], const float2* st, int t) {
 // step's first three half-substeps (ETRK2: xi1, x1, xi2; ETD1: x1 after the
 // first), in lane layout [step][3][m][t]; tail_skip half-substeps are left out
 // at the end (the last step's states are needed, its result is not).
+// tape (optional, the tape rollout): receives per step [4][m][t] the step's start
+// state and its states after the first three half-substeps (ETD1: start state and
+// the state between its substeps), by streaming stores.
+template <int P, int T>
+INC_DEV void tape_put(float2* dst, const float2 (&v)[P], int t) {
+#pragma unroll
+    for (int m = 0; m < P; ++m) __stcs(dst + m * T + t, v[m]);
+}
+
 template <int P, int T>
 INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, const Buf<P, T>& buf,
                              const Twiddles<P, T>& tw, bool frames_on, int nseg, bool ckpt_on = true,
-                             float2* seg = nullptr, float2* stg = nullptr, int tail_skip = 0) {
+                             float2* seg = nullptr, float2* stg = nullptr, int tail_skip = 0,
+                             float2* tape = nullptr) {
     constexpr int N = P * T;
     const int t = c.t;
     const bool rk2 = a.scheme == INC_KS_ETRK2;
@@ -811,6 +822,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
                 --ck_left;
             }
             if (seg) st_put<P, T>(seg + step * N, x, t);
+            if (tape) tape_put<P, T>(tape + (int64_t)step * 4 * N, x, t);
         }
         float2 v[P];
 #pragma unroll
@@ -841,6 +853,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
 #pragma unroll
         for (int m = 0; m < P; ++m) x[m] = cswap(v[m]);
         if (stg && h < per_step - 1) st_put<P, T>(stg + (step * 3 + h) * N, x, t);
+        if (tape && h < per_step - 1) tape_put<P, T>(tape + ((int64_t)step * 4 + 1 + h) * N, x, t);
         if (rk2) stage2 = !stage2;
         if (++h == per_step) {
             if (frames_on) store_pair_strided<P, T>(a.frames, x, c, N, frame_stride, (int64_t)step * N);
@@ -883,7 +896,10 @@ __global__ void __launch_bounds__(128) k_rollout(Args a) {
     float2 x[P];
     load_pair<P, T>(x, a.u, c, N);
     const int nseg = a.ckpt_every > 0 ? (a.steps + a.ckpt_every - 1) / a.ckpt_every : 0;
-    forward_program<P, T>(a, c, x, a.steps, buf, tw, a.frames != nullptr, nseg);
+    // the tape holds a slot for every launched group (its size is rounded up), so
+    // groups past the last row pair write padding
+    float2* tape = a.tape ? a.tape + (int64_t)pair * a.steps * 4 * N : nullptr;
+    forward_program<P, T>(a, c, x, a.steps, buf, tw, a.frames != nullptr, nseg, true, nullptr, nullptr, 0, tape);
     if (a.out) store_pair<P, T>(a.out, x, c, N);
 }
 
@@ -1163,8 +1179,39 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
 
+// Backward of a tape rollout: every step's start and substep states come from the
+// tape the forward wrote, so no segment is replayed: per step() the frame
+// adjoint's transform and the adjoint units' eight (ETRK2) against 17 with the
+// replay.
+template <int P, int T>
+__global__ void __launch_bounds__(128) k_rollout_bwd_tape(Args a) {
+    extern __shared__ float2 sm[];
+    constexpr int N = P * T;
+    const int t = threadIdx.x % T;
+    const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
+    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>(0));
+    const Buf<P, T> buf = group_buf<P, T>(g, t);
+    float2* st = g + 2 * buf_len<P, T>();
+    const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
+    Ctx c;
+    make_ctx(a, pair, t, pair < a.npairs, c);
+    SlotCache<P, T> cc;
+    cc.load(a, c);
+    float2 G[P], Sacc[P], SS[P];
+    adjoint_prologue<P, T>(a, c, cc, a.g_final, SS, G, buf, tw);
+#pragma unroll
+    for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
+    const float2* tape = a.tape + (int64_t)pair * a.steps * 4 * N;
+    for (int k = a.steps - 1; k >= 0; --k) {
+        const float2* ts = tape + (int64_t)k * 4 * N;
+        step_bwd_program<P, T, true>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N, ts, st,
+                                     buf, tw, ts + N);
+    }
+    adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
+}
+
 // ---- launchers (instantiated per shape in ks_{fwd,bwd}_*.cu) ---------------------
-enum class Kind { Step, Rollout, StepBwd, RolloutBwd };
+enum class Kind { Step, Rollout, StepBwd, RolloutBwd, TapeBwd };
 
 template <int P, int T>
 int launch_fwd(Kind kind, const Args& a, cudaStream_t st, int block);
@@ -1175,7 +1222,7 @@ template <int P, int T>
 size_t smem_bytes(Kind kind, int block, int K) {
     const int groups = block / T;
     size_t per = (kind == Kind::Step || kind == Kind::Rollout) ? fwd_group_smem<P, T>()
-               : bwd_group_smem<P, T>(kind == Kind::StepBwd ? 0 : K);
+               : bwd_group_smem<P, T>(kind == Kind::RolloutBwd ? K : 0);
     return (tw_size<P, T>() + groups * per) * sizeof(float2);
 }
 
@@ -1205,6 +1252,7 @@ int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     const int grid = (a.npairs + gpb - 1) / gpb;
     const size_t smem = smem_bytes<P, T>(kind, block, a.ckpt_every);
     if (kind == Kind::StepBwd) return launch_with_smem(k_step_bwd<P, T>, grid, block, smem, st, a);
+    if (kind == Kind::TapeBwd) return launch_with_smem(k_rollout_bwd_tape<P, T>, grid, block, smem, st, a);
     if (a.stage) return launch_with_smem(k_rollout_bwd<P, T, true>, grid, block, smem, st, a);
     return launch_with_smem(k_rollout_bwd<P, T, false>, grid, block, smem, st, a);
 }

@@ -46,24 +46,36 @@ class BurgersRolloutFn(torch.autograd.Function):
 
 
 class KSRolloutFn(torch.autograd.Function):
+    """ckpt_every > 0: checkpoints every ckpt_every steps, segments replayed in the
+    backward; ckpt_every == 0: a tape of every step's states (no replay, more memory)."""
+
     @staticmethod
     def forward(ctx, u0, s, plan, steps, ckpt_every, want_grad):
         B, N = u0.shape
         frames = torch.empty(B, steps, N, device=u0.device, dtype=u0.dtype)
-        ckpts = torch.empty(B, _nseg(steps, ckpt_every), N, device=u0.device, dtype=u0.dtype) if want_grad else None
-        plan.rollout(u0, s, steps, frames, None, ckpt_every, ckpts)
+        if want_grad and ckpt_every == 0:
+            saved = torch.empty(plan.tape_size(steps), dtype=torch.uint8, device=u0.device)
+            plan.rollout_tape(u0, s, steps, frames, None, saved)
+        else:
+            k = ckpt_every if ckpt_every > 0 else 8
+            saved = torch.empty(B, _nseg(steps, k), N, device=u0.device, dtype=u0.dtype) if want_grad else None
+            plan.rollout(u0, s, steps, frames, None, k, saved)
         ctx.plan, ctx.steps, ctx.k, ctx.has_s = plan, steps, ckpt_every, s is not None
+        ctx.shape = (B, N)
         if want_grad:
-            ctx.save_for_backward(ckpts, s if s is not None else u0.new_empty(0))
+            ctx.save_for_backward(saved, s if s is not None else u0.new_empty(0))
         return frames
 
     @staticmethod
     def backward(ctx, g_frames):
-        ckpts, s = ctx.saved_tensors
+        saved, s = ctx.saved_tensors
         s = s if ctx.has_s else None
-        g_u0 = torch.empty(ckpts.shape[0], ckpts.shape[2], device=ckpts.device, dtype=ckpts.dtype)
+        g_u0 = torch.empty(ctx.shape, device=saved.device, dtype=torch.float32)
         g_s = torch.empty_like(g_u0) if (ctx.has_s and ctx.needs_input_grad[1]) else None
-        ctx.plan.rollout_bwd(ckpts, s, ctx.steps, ctx.k, g_frames.contiguous(), None, g_u0, g_s)
+        if ctx.k == 0:
+            ctx.plan.rollout_bwd_tape(saved, s, ctx.steps, g_frames.contiguous(), None, g_u0, g_s)
+        else:
+            ctx.plan.rollout_bwd(saved, s, ctx.steps, ctx.k, g_frames.contiguous(), None, g_u0, g_s)
         return g_u0, g_s, None, None, None, None
 
 
@@ -89,7 +101,11 @@ def burgers_rollout(solver: BurgersSolverTorch, u0, steps, s=None, ckpt_every=8)
 
 
 def ks_rollout(solver: KSSolverTorch, u0, steps, domain_size, s=None, ckpt_every=8):
-    """Frames [B, steps, N] of `steps` KS step() calls in one launch (s held constant)."""
+    """Frames [B, steps, N] of `steps` KS step() calls in one launch (s held constant).
+
+    Differentiable w.r.t. u0 and s.  The backward replays ckpt_every-step segments from
+    checkpoints; ckpt_every=0 records every step's states in a tape instead (32 bytes per
+    row pair, cell and step) and the backward reads them, with no replay."""
     _check_state(u0, solver.resolution)
     u0 = u0.contiguous()
     s = _contig(s)

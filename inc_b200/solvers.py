@@ -497,6 +497,30 @@ class KSPlan:
                                                      nat.stream_of(self.device))
         nat.check(rc, "inc_ks_rollout_bwd")
 
+    def tape_size(self, steps):
+        """Bytes of the tape a tape rollout of `steps` step() calls records."""
+        n = int(nat.lib().inc_ks_tape_size(C.byref(self.c), int(steps)))
+        if n < 0:
+            raise ValueError(f"steps must be positive (got {steps})")
+        return n
+
+    def rollout_tape(self, u0, s, steps, frames, u_final, tape):
+        """rollout() that also records every step's start and substep states in `tape`
+        (a uint8 device tensor of tape_size(steps) bytes) for rollout_bwd_tape."""
+        with nat.on_device(self.device):
+            rc = nat.lib().inc_ks_rollout_tape(C.byref(self.c), u0.data_ptr(), nat.ptr(s), steps, nat.ptr(frames),
+                                               nat.ptr(u_final), tape.data_ptr(), tape.numel(),
+                                               nat.stream_of(self.device))
+        nat.check(rc, "inc_ks_rollout_tape")
+
+    def rollout_bwd_tape(self, tape, s, steps, g_frames, g_final, g_u0, g_s):
+        """The VJP of a tape rollout from its recorded states (no replay)."""
+        with nat.on_device(self.device):
+            rc = nat.lib().inc_ks_rollout_bwd_tape(C.byref(self.c), tape.data_ptr(), tape.numel(), nat.ptr(s), steps,
+                                                   nat.ptr(g_frames), nat.ptr(g_final), g_u0.data_ptr(),
+                                                   nat.ptr(g_s), nat.stream_of(self.device))
+        nat.check(rc, "inc_ks_rollout_bwd_tape")
+
     def rollout_bwd_work_size(self, ckpt_every):
         """Bytes of device scratch rollout_bwd uses for this plan and ckpt_every."""
         n = int(nat.lib().inc_ks_rollout_bwd_work_size(C.byref(self.c), int(ckpt_every)))

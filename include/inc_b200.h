@@ -301,6 +301,23 @@ int inc_ks_rollout_bwd_ws(const inc_ks_plan* plan, const float* ckpts, const flo
                           const float* g_final, float* g_u0, float* g_s, void* work,
                           int64_t work_bytes, void* stream);
 
+/* Tape rollouts: inc_ks_rollout (ckpt_every = 0) that also records, for every
+ * step, its start state and its three intermediate substep states (ETD1: the
+ * one between its substeps) in `tape`, inc_ks_tape_size(plan, steps) bytes of
+ * device memory (16-byte aligned; -1 for a bad plan or steps); and the
+ * backward that reads them instead of replaying segments from checkpoints:
+ * 9 row-pair transforms per step() (ETRK2) instead of 17.  For callers with
+ * the memory to spare (4 x 8 bytes per row pair, cell and step: 1.3 GB for
+ * 1024 rows x 256 cells x 400 steps).  Same results as the checkpointed pair to
+ * rounding.  No counterpart in the reference (autograd keeps its whole graph). */
+int64_t inc_ks_tape_size(const inc_ks_plan* plan, int32_t steps);
+int inc_ks_rollout_tape(const inc_ks_plan* plan, const float* u0, const float* s,
+                        int32_t steps, float* frames, float* u_final, void* tape,
+                        int64_t tape_bytes, void* stream);
+int inc_ks_rollout_bwd_tape(const inc_ks_plan* plan, const void* tape, int64_t tape_bytes,
+                            const float* s, int32_t steps, const float* g_frames,
+                            const float* g_final, float* g_u0, float* g_s, void* stream);
+
 /* ---- analysis -------------------------------------------------------------- */
 /* Energy spectrum of each of `rows` real rows of length n (a power of two in
  * [16, 512]): out[row][k] = |FFT(u)[k]|^2 for k in [0, n/2], bins 1..n/2-1

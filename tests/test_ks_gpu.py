@@ -248,6 +248,60 @@ def test_rollout_backward_scratch_many_groups(cuda, B, tpp):
         assert per_row.max() < 1e-4
 
 
+@pytest.mark.parametrize("N,tpp,B", [(16, 4, 7), (64, 16, 7), (128, 32, 7), (256, 32, 7), (256, 64, 7),
+                                     (512, 32, 7), (256, 32, 1031), (256, 16, 4101)])
+@pytest.mark.parametrize("scheme", ["ETRK2", "ETD1"])
+def test_rollout_tape_matches_checkpointed(cuda, N, tpp, B, scheme):
+    """The tape rollout (every step's states recorded, no replay in the backward) against
+    the checkpointed rollout and its scratch backward: the same frames bit for bit, and
+    gradients (u0, s; frame and final-state adjoints) equal to rounding."""
+    steps, K = 11, 4
+    dt = 0.2 if scheme == "ETRK2" else 0.05
+    Ls = [40.0 + 9 * (i % 7) for i in range(B)]
+    solver = _solver(N, dt, scheme, Ls, tpp=tpp)
+    u0 = torch.tensor(_u0(B, N, Ls, 5) if B < 100 else np.tile(_u0(7, N, Ls[:7], 5), (B // 7 + 1, 1))[:B],
+                      dtype=torch.float32, device=cuda)
+    g = torch.Generator(device=cuda).manual_seed(N + tpp + B)
+    s = 0.01 * torch.randn(B, N, device=cuda, generator=g)
+    ds = torch.tensor(Ls, device=cuda)
+    plan = solver.plan_for(u0, ds)
+    fa = torch.empty(B, steps, N, device=cuda)
+    ck = torch.empty(B, (steps + K - 1) // K, N, device=cuda)
+    plan.rollout(u0, s, steps, fa, None, K, ck)
+    fb = torch.empty(B, steps, N, device=cuda)
+    tape = torch.empty(plan.tape_size(steps), dtype=torch.uint8, device=cuda)
+    plan.rollout_tape(u0, s, steps, fb, None, tape)
+    assert torch.equal(fa, fb)
+    gf = torch.randn(B, steps, N, device=cuda, generator=g)
+    gfin = torch.randn(B, N, device=cuda, generator=g)
+    ga = [torch.empty_like(u0) for _ in range(2)]
+    gb = [torch.empty_like(u0) for _ in range(2)]
+    plan.rollout_bwd(ck, s, steps, K, gf, gfin, ga[0], ga[1])
+    plan.rollout_bwd_tape(tape, s, steps, gf, gfin, gb[0], gb[1])
+    for a, b in zip(ga, gb):
+        assert torch.isfinite(b).all()
+        assert rel_l2(b.cpu().numpy(), a.cpu().numpy()) < 1e-5
+    with pytest.raises(ValueError):
+        plan.rollout_bwd_tape(tape[:-16], s, steps, gf, gfin, gb[0], gb[1])
+
+
+def test_ks_rollout_tape_autograd(cuda):
+    from inc_b200.rollout import ks_rollout
+    N, B, steps, dt = 128, 6, 9, 0.2
+    Ls = [40.0, 44.0, 50.0, 60.0, 64.0, 100.0]
+    u0 = torch.tensor(_u0(B, N, Ls, 13), dtype=torch.float32, device=cuda)
+    s0 = 0.01 * torch.randn(B, N, device=cuda)
+    w = torch.randn(B, steps, N, device=cuda)
+    ds = torch.tensor(Ls, device=cuda)
+    out = []
+    for k in (4, 0):
+        u, s = u0.clone().requires_grad_(True), s0.clone().requires_grad_(True)
+        fr = ks_rollout(_solver(N, dt, "ETRK2", Ls), u, steps, ds, s=s, ckpt_every=k)
+        out.append(torch.autograd.grad((fr * w).sum(), (u, s)))
+    for a, b in zip(*out):
+        assert rel_l2(b.cpu().numpy(), a.cpu().numpy()) < 1e-5
+
+
 def test_fd_check_fp64_oracle(cuda):
     N, B, dt, steps = 64, 3, 0.25, 2
     Ls = [64.0, 64.0, 50.0]
