@@ -770,14 +770,18 @@ INC_DEV void tape_put(float2* dst, const float2 (&v)[P], int t) {
     for (int m = 0; m < P; ++m) __stcs(dst + m * T + t, v[m]);
 }
 
-template <int P, int T>
+// FAST = 1: the common case compiled alone (ETRK2, both rows of every pair with one
+// domain size, so packed spectra): no scheme or storage branches in the loop body,
+// which is then smaller (instruction cache) and straight-line.
+template <int P, int T, int FAST = 0>
 INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int steps, const Buf<P, T>& buf,
                              const Twiddles<P, T>& tw, bool frames_on, int nseg, bool ckpt_on = true,
                              float2* seg = nullptr, float2* stg = nullptr, int tail_skip = 0,
                              float2* tape = nullptr) {
     constexpr int N = P * T;
     const int t = c.t;
-    const bool rk2 = a.scheme == INC_KS_ETRK2;
+    const bool rk2 = FAST ? true : a.scheme == INC_KS_ETRK2;
+    const bool split = FAST ? false : a.split != 0;
     float2 X[P], SS[P];
     SlotCache<P, T> cc;
     cc.load(a, c);
@@ -794,7 +798,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
             for (int m = 0; m < P; ++m) v[m] = x[m];
         }
         fft_fwd<P, T>(v, buf, tw, t);
-        if (a.split) to_split<P, T>(v, t, buf.a);
+        if (split) to_split<P, T>(v, t, buf.a);
 #pragma unroll
         for (int m = 0; m < P; ++m) {
             const float2 z = cscale(v[m], a.invN);
@@ -828,7 +832,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
 #pragma unroll
         for (int m = 0; m < P; ++m) v[m] = sq2(x[m]);
         fft_fwd<P, T>(v, buf, tw, t);
-        if (a.split) to_split<P, T>(v, t, buf.a);
+        if (split) to_split<P, T>(v, t, buf.a);
         if (!stage2) {  // Zi = E X + phi1 (D V + S);  ETRK2 carries Y = Zi - phi2 D V
 #pragma unroll
             for (int m = 0; m < P; ++m) {
@@ -846,7 +850,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
                 v[m] = X[m];
             }
         }
-        if (a.split) to_packed<P, T>(v, t, buf.a);
+        if (split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
         for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);  // inverse transform by swapping
         fft_fwd<P, T>(v, buf, tw, t);
@@ -863,7 +867,7 @@ INC_DEV void forward_program(const Args& a, const Ctx& c, float2 (&x)[P], int st
     }
 }
 
-template <int P, int T>
+template <int P, int T, int FAST = 0>
 __global__ void __launch_bounds__(128) k_step(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
@@ -878,12 +882,12 @@ __global__ void __launch_bounds__(128) k_step(Args a) {
     if (a.cu) add_pair<P, T>(x, a.cu, c, N);  // u + correction_u, solver_1d.py:281/286
     // a single substep runs the first half of the step's half-substeps
     const int skip = a.substeps == 1 ? (a.scheme == INC_KS_ETRK2 ? 2 : 1) : 0;
-    forward_program<P, T>(a, c, x, 1, buf, tw, false, 0, true, nullptr, nullptr, skip);
+    forward_program<P, T, FAST>(a, c, x, 1, buf, tw, false, 0, true, nullptr, nullptr, skip);
     store_pair<P, T>(a.out, x, c, N);
 }
 
 // Fused rollout of `steps` step() calls with s held constant.
-template <int P, int T>
+template <int P, int T, int FAST = 0>
 __global__ void __launch_bounds__(128) k_rollout(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
@@ -899,7 +903,8 @@ __global__ void __launch_bounds__(128) k_rollout(Args a) {
     // the tape holds a slot for every launched group (its size is rounded up), so
     // groups past the last row pair write padding
     float2* tape = a.tape ? a.tape + (int64_t)pair * a.steps * 4 * N : nullptr;
-    forward_program<P, T>(a, c, x, a.steps, buf, tw, a.frames != nullptr, nseg, true, nullptr, nullptr, 0, tape);
+    forward_program<P, T, FAST>(a, c, x, a.steps, buf, tw, a.frames != nullptr, nseg, true, nullptr, nullptr, 0,
+                                tape);
     if (a.out) store_pair<P, T>(a.out, x, c, N);
 }
 
@@ -932,14 +937,15 @@ INC_DEV void pair_mul2(float2 (&v)[P], const float2 (&x)[P], float s) {
 //
 // STG: stg holds the step's states xi1, x1, xi2 (ETD1: x1) kept by the segment
 // replay in lane layout [3][m][t]; the replay units and FFT(x0) are skipped.
-template <int P, int T, bool STG = false>
+template <int P, int T, bool STG = false, int FAST = 0>
 INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>& cc, const float2 (&SS)[P],
                               float2 (&G)[P], float2 (&Sacc)[P], const float* gframe, int64_t gf_row_stride,
                               int64_t gf_off, const float2* x0s, float2* st, const Buf<P, T>& buf, const Twiddles<P, T>& tw,
                               const float2* stg = nullptr) {
     constexpr int N = P * T;
     const int t = c.t;
-    const bool rk2 = a.scheme == INC_KS_ETRK2;
+    const bool rk2 = FAST ? true : a.scheme == INC_KS_ETRK2;
+    const bool split = FAST ? false : a.split != 0;
     const bool single = !STG && a.substeps == 1;  // one substep: its states are x0 (and xi1)
     const float2* x1s = STG ? stg + (rk2 ? N : 0) : st;
     const float2* xi1s = STG ? stg : st + N;
@@ -952,7 +958,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
         if (k == 0) load_pair_strided<P, T>(v, gframe, c, N, gf_row_stride, gf_off);
         else st_get<P, T>(v, x0s, t);
         fft_fwd<P, T>(v, buf, tw, t);
-        if (a.split) to_split<P, T>(v, t, buf.a);
+        if (split) to_split<P, T>(v, t, buf.a);
 #pragma unroll
         for (int m = 0; m < P; ++m) {
             const float2 z = cscale(v[m], a.invN);
@@ -986,14 +992,14 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
                 v[m] = cscale(dmul(G[m], sl.d), unit_w2 ? sl.p2 : sl.p1);
                 if (!unit_w2) Sacc[m] = cadd(Sacc[m], rmul(G[m], sl.p1, sl.p1b));
             }
-            if (a.split) to_packed<P, T>(v, t, buf.a);
+            if (split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
             for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
         }
         fft_fwd<P, T>(v, buf, tw, t);
         // ---- operand of the second transform
         if (rec) {
-            if (a.split) to_split<P, T>(v, t, buf.a);
+            if (split) to_split<P, T>(v, t, buf.a);
             if (rk2 && k == 1) {  // stage 2
 #pragma unroll
                 for (int m = 0; m < P; ++m) {
@@ -1011,7 +1017,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
                     v[m] = Zi;
                 }
             }
-            if (a.split) to_packed<P, T>(v, t, buf.a);
+            if (split) to_packed<P, T>(v, t, buf.a);
 #pragma unroll
             for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
         } else {
@@ -1041,7 +1047,7 @@ INC_DEV void step_bwd_program(const Args& a, const Ctx& c, const SlotCache<P, T>
             for (int m = 0; m < P; ++m) v[m] = cswap(v[m]);
             st_put<P, T>(rk2 ? (k == 0 ? st + N : (k == 1 ? st : st + 2 * N)) : st, v, t);
         } else {
-            if (a.split) to_split<P, T>(v, t, buf.a);
+            if (split) to_split<P, T>(v, t, buf.a);
             if (unit_w2) {
 #pragma unroll
                 for (int m = 0; m < P; ++m) G[m] = csub(G[m], cscale(v[m], a.invN));
@@ -1104,7 +1110,7 @@ INC_DEV void adjoint_epilogue(const Args& a, const Ctx& c, const float2 (&G)[P],
 }
 
 
-template <int P, int T>
+template <int P, int T, int FAST = 0>
 __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
@@ -1128,13 +1134,13 @@ __global__ void __launch_bounds__(128) k_step_bwd(Args a) {
     }
 #pragma unroll
     for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
-    step_bwd_program<P, T>(a, c, cc, SS, G, Sacc, nullptr, 0, 0, st + 4 * N, st, buf, tw);
+    step_bwd_program<P, T, false, FAST>(a, c, cc, SS, G, Sacc, nullptr, 0, 0, st + 4 * N, st, buf, tw);
     adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
 
 // Backward of the fused rollout: each ckpt_every-step segment is replayed from
 // its checkpoint (states kept in shared memory), then differentiated step by step.
-template <int P, int T, bool STG>
+template <int P, int T, bool STG, int FAST = 0>
 __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
@@ -1164,15 +1170,15 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
             float2 x[P];
             load_pair_strided<P, T>(x, a.ckpts, c, N, (int64_t)nseg * N, (int64_t)sidx * N);
             if (STG) {  // every step's start state and its substep states, the last step's result left out
-                forward_program<P, T>(a, c, x, len, buf, tw, false, nseg, false, seg, stg, 1);
+                forward_program<P, T, FAST>(a, c, x, len, buf, tw, false, nseg, false, seg, stg, 1);
             } else {
-                forward_program<P, T>(a, c, x, len - 1, buf, tw, false, nseg, false, seg);
+                forward_program<P, T, FAST>(a, c, x, len - 1, buf, tw, false, nseg, false, seg);
                 st_put<P, T>(seg + (len - 1) * N, x, t);
             }
         }
         for (int j = len - 1; j >= 0; --j) {
             const int k = k0 + j;
-            step_bwd_program<P, T, STG>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N,
+            step_bwd_program<P, T, STG, FAST>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N,
                                         seg + j * N, st, buf, tw, STG ? stg + (size_t)j * 3 * N : nullptr);
         }
     }
@@ -1183,7 +1189,7 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
 // tape the forward wrote, so no segment is replayed: per step() the frame
 // adjoint's transform and the adjoint units' eight (ETRK2) against 17 with the
 // replay.
-template <int P, int T>
+template <int P, int T, int FAST = 0>
 __global__ void __launch_bounds__(128) k_rollout_bwd_tape(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
@@ -1204,8 +1210,8 @@ __global__ void __launch_bounds__(128) k_rollout_bwd_tape(Args a) {
     const float2* tape = a.tape + (int64_t)pair * a.steps * 4 * N;
     for (int k = a.steps - 1; k >= 0; --k) {
         const float2* ts = tape + (int64_t)k * 4 * N;
-        step_bwd_program<P, T, true>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N, ts, st,
-                                     buf, tw, ts + N);
+        step_bwd_program<P, T, true, FAST>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N,
+                                           ts, st, buf, tw, ts + N);
     }
     adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
@@ -1226,6 +1232,9 @@ size_t smem_bytes(Kind kind, int block, int K) {
     return (tw_size<P, T>() + groups * per) * sizeof(float2);
 }
 
+// The kernels compiled for the common case alone (see forward_program).
+inline bool fast_case(const Args& a) { return a.scheme == INC_KS_ETRK2 && !a.split; }
+
 template <typename F>
 int launch_with_smem(F kernel, int grid, int block, size_t smem, cudaStream_t st, const Args& a) {
     if (smem > 227 * 1024) {
@@ -1242,6 +1251,10 @@ int launch_fwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     const int gpb = block / T;
     const int grid = (a.npairs + gpb - 1) / gpb;
     const size_t smem = smem_bytes<P, T>(kind, block, a.ckpt_every);
+    if (fast_case(a)) {
+        if (kind == Kind::Step) return launch_with_smem(k_step<P, T, 1>, grid, block, smem, st, a);
+        return launch_with_smem(k_rollout<P, T, 1>, grid, block, smem, st, a);
+    }
     if (kind == Kind::Step) return launch_with_smem(k_step<P, T>, grid, block, smem, st, a);
     return launch_with_smem(k_rollout<P, T>, grid, block, smem, st, a);
 }
@@ -1251,6 +1264,12 @@ int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     const int gpb = block / T;
     const int grid = (a.npairs + gpb - 1) / gpb;
     const size_t smem = smem_bytes<P, T>(kind, block, a.ckpt_every);
+    if (fast_case(a)) {
+        if (kind == Kind::StepBwd) return launch_with_smem(k_step_bwd<P, T, 1>, grid, block, smem, st, a);
+        if (kind == Kind::TapeBwd) return launch_with_smem(k_rollout_bwd_tape<P, T, 1>, grid, block, smem, st, a);
+        if (a.stage) return launch_with_smem(k_rollout_bwd<P, T, true, 1>, grid, block, smem, st, a);
+        return launch_with_smem(k_rollout_bwd<P, T, false, 1>, grid, block, smem, st, a);
+    }
     if (kind == Kind::StepBwd) return launch_with_smem(k_step_bwd<P, T>, grid, block, smem, st, a);
     if (kind == Kind::TapeBwd) return launch_with_smem(k_rollout_bwd_tape<P, T>, grid, block, smem, st, a);
     if (a.stage) return launch_with_smem(k_rollout_bwd<P, T, true>, grid, block, smem, st, a);
