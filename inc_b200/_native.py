@@ -149,6 +149,13 @@ def ptr(t) -> int | None:
     return None if t is None else t.data_ptr()
 
 
+def raw_stream(idx: int) -> int:
+    """The raw cudaStream_t of torch's current stream on device index `idx`."""
+    import torch
+    raw = getattr(torch._C, "_cuda_getCurrentRawStream", None)
+    return raw(idx) if raw is not None else torch.cuda.current_stream(idx).cuda_stream
+
+
 def stream_of(device) -> int:
     """The raw cudaStream_t of torch's current stream on `device`."""
     import torch

@@ -123,6 +123,7 @@ int pick_block(Kind kind, int npairs, int T, int n, int K) {
         int64_t per = 2 * (n + n / 4 + 64) + 16;  // bound on the exchange buffers' padded layouts
         if (kind == Kind::StepBwd || kind == Kind::RolloutBwd || kind == Kind::TapeBwd) per += 5 * n;
         if (kind == Kind::RolloutBwd) per += (int64_t)K * n;
+        if (kind == Kind::TapeBwd) per += (int64_t)8 * n;  // two staged tape slots
         return (int64_t)(4 * n + groups * per) * 8;
     };
     while (block > 32 && smem(block) > 100 * 1024) block >>= 1;

@@ -1185,33 +1185,73 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
 
+// Asynchronous 8-byte copies global -> shared (cp.async), in commit groups.
+INC_DEV void cp_async8(float2* smem_dst, const float2* gsrc) {
+    const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gsrc) : "memory");
+}
+INC_DEV void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int NPENDING>
+INC_DEV void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(NPENDING) : "memory"); }
+
+// This lane's share of one step's tape slot ([4][m][t]) copied into shared memory.
+template <int P, int T>
+INC_DEV void tape_prefetch(float2* dst, const float2* src, int t) {
+#pragma unroll
+    for (int q = 0; q < 4 * P; ++q) cp_async8(dst + q * T + t, src + q * T + t);
+    cp_async_commit();
+}
+
 // Backward of a tape rollout: every step's start and substep states come from the
 // tape the forward wrote, so no segment is replayed: per step() the frame
 // adjoint's transform and the adjoint units' eight (ETRK2) against 17 with the
-// replay.
+// replay.  The tape lives in HBM (it outgrows L2), so each step's states are
+// copied into shared memory (cp.async) while the step before them is
+// differentiated, and each frame adjoint is loaded a step ahead.
 template <int P, int T, int FAST = 0>
 __global__ void __launch_bounds__(128) k_rollout_bwd_tape(Args a) {
     extern __shared__ float2 sm[];
     constexpr int N = P * T;
     const int t = threadIdx.x % T;
     const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
-    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>(0));
+    float2* g = group_smem<P, T>(sm, bwd_group_smem<P, T>(8));
     const Buf<P, T> buf = group_buf<P, T>(g, t);
     float2* st = g + 2 * buf_len<P, T>();
+    float2* stage = st + 5 * N;  // two [4][m][t] slots
     const int pair = blockIdx.x * (blockDim.x / T) + threadIdx.x / T;
     Ctx c;
     make_ctx(a, pair, t, pair < a.npairs, c);
     SlotCache<P, T> cc;
     cc.load(a, c);
+    const bool split = FAST ? false : a.split != 0;
     float2 G[P], Sacc[P], SS[P];
     adjoint_prologue<P, T>(a, c, cc, a.g_final, SS, G, buf, tw);
 #pragma unroll
     for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
     const float2* tape = a.tape + (int64_t)pair * a.steps * 4 * N;
+    const int64_t gf_stride = (int64_t)a.steps * N;
+    tape_prefetch<P, T>(stage + ((a.steps - 1) & 1) * 4 * N, tape + (int64_t)(a.steps - 1) * 4 * N, t);
+    float2 gf[P];
+    if (a.g_frames) load_pair_strided<P, T>(gf, a.g_frames, c, N, gf_stride, (int64_t)(a.steps - 1) * N);
     for (int k = a.steps - 1; k >= 0; --k) {
-        const float2* ts = tape + (int64_t)k * 4 * N;
-        step_bwd_program<P, T, true, FAST>(a, c, cc, SS, G, Sacc, a.g_frames, (int64_t)a.steps * N, (int64_t)k * N,
-                                           ts, st, buf, tw, ts + N);
+        if (k > 0) {
+            tape_prefetch<P, T>(stage + ((k - 1) & 1) * 4 * N, tape + (int64_t)(k - 1) * 4 * N, t);
+            cp_async_wait<1>();
+        } else {
+            cp_async_wait<0>();
+        }
+        if (a.g_frames) {  // G += FFT(dL/dframe_k)/N, the next step's frame adjoint loaded meanwhile
+            float2 v[P];
+#pragma unroll
+            for (int m = 0; m < P; ++m) v[m] = gf[m];
+            if (k > 0) load_pair_strided<P, T>(gf, a.g_frames, c, N, gf_stride, (int64_t)(k - 1) * N);
+            fft_fwd<P, T>(v, buf, tw, t);
+            if (split) to_split<P, T>(v, t, buf.a);
+#pragma unroll
+            for (int m = 0; m < P; ++m) G[m] = cadd(G[m], cscale(v[m], a.invN));
+        }
+        const float2* ts = stage + (k & 1) * 4 * N;
+        step_bwd_program<P, T, true, FAST>(a, c, cc, SS, G, Sacc, nullptr, 0, 0, ts, st, buf, tw, ts + N);
     }
     adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
@@ -1228,7 +1268,7 @@ template <int P, int T>
 size_t smem_bytes(Kind kind, int block, int K) {
     const int groups = block / T;
     size_t per = (kind == Kind::Step || kind == Kind::Rollout) ? fwd_group_smem<P, T>()
-               : bwd_group_smem<P, T>(kind == Kind::RolloutBwd ? K : 0);
+               : bwd_group_smem<P, T>(kind == Kind::RolloutBwd ? K : (kind == Kind::TapeBwd ? 8 : 0));
     return (tw_size<P, T>() + groups * per) * sizeof(float2);
 }
 

@@ -98,6 +98,9 @@ class _BurgersLaunch:
         else:
             raise ValueError("Unknown equation type.")
         self.desc = d
+        self.t_ptr = None if self.t_rows is None else self.t_rows.data_ptr()
+        self.dref = C.byref(d)  # the descriptor's address, built once (it keeps d alive)
+        self.dev_index = dev.index
 
     def _bind_time(self, t, rows):
         if isinstance(t, torch.Tensor):
@@ -109,6 +112,7 @@ class _BurgersLaunch:
             self.t0 = 0.0
         else:
             self.t0, self.t_rows = float(t), None
+        self.t_ptr = None if self.t_rows is None else self.t_rows.data_ptr()
 
     def at(self, t):
         """This launch at time t: itself when the equation does not read the time, else a
@@ -120,10 +124,18 @@ class _BurgersLaunch:
         return c
 
     def step(self, u, s, out):
-        with nat.on_device(self.dev):
-            rc = nat.lib().inc_burgers_step(C.byref(self.desc), u.data_ptr(), nat.ptr(s), nat.ptr(self.t_rows),
-                                            self.t0, out.data_ptr(), nat.stream_of(self.dev))
-        nat.check(rc, "inc_burgers_step")
+        # the per-step path of the drop-in solver: the bound function, the descriptor's
+        # address and the raw stream, and a device switch only when another is current
+        idx = self.dev_index
+        fn = nat.lib().inc_burgers_step
+        sp = None if s is None else s.data_ptr()
+        if torch.cuda.current_device() == idx:
+            rc = fn(self.dref, u.data_ptr(), sp, self.t_ptr, self.t0, out.data_ptr(), nat.raw_stream(idx))
+        else:
+            with nat.on_device(self.dev):
+                rc = fn(self.dref, u.data_ptr(), sp, self.t_ptr, self.t0, out.data_ptr(), nat.raw_stream(idx))
+        if rc:
+            nat.check(rc, "inc_burgers_step")
 
     def step_bwd(self, u, s, g, gu, gs):
         with nat.on_device(self.dev):
@@ -377,7 +389,7 @@ class BurgersSolverTorch:
     def _launch_key(self, u):
         p = self.param
         eq = p.equation_type
-        static = (tuple(u.shape), u.device, self.time_scheme, p.convection_term, eq, self.dt, self.dx,
+        static = (u.shape, u.get_device(), self.time_scheme, p.convection_term, eq, self.dt, self.dx,
                   self.cells_per_thread)
         objs = (self.nu,)
         if eq == "linear":
