@@ -64,8 +64,8 @@ def parse_args():
     ap.add_argument("--extra-steps", type=int, default=3, help="timed repeats of each compact block")
     ap.add_argument("--cpu-seconds", type=float, default=12.0, help="CPU baseline sample budget")
     ap.add_argument("--profile", nargs="?", const="ks", default=None,
-                    choices=["ks", "burgers_ragged", "burgers_plain", "burgers_plain_bwd", "ks_bwd", "burgers_cnn",
-                             "spectral_conv"],
+                    choices=["ks", "burgers_ragged", "burgers_plain", "burgers_plain_bwd", "ks_bwd", "ks_tape",
+                             "burgers_cnn", "spectral_conv", "adaptive"],
                     help="a small case of one kernel for ncu (no JSON)")
     ap.add_argument("--profile-rows", type=int, default=1024, help="rows of the KS profile case")
     ap.add_argument("--tpp", type=int, default=None,
@@ -1266,6 +1266,10 @@ def profile_small(dev, which="ks", rows=1024, tpp=32):
     the 32x128 Burgers rollout, the fused CNN rollout, or one FNO spectral layer (512 x 64 x 512)."""
     import torch
     from types import SimpleNamespace
+    if which == "adaptive":  # one adaptive-CFL step of 4096 x 256 rows (about 20 substeps)
+        bench_adaptive(dev, reps=2)
+        torch.cuda.synchronize()
+        return
     if which == "burgers_ragged":
         from inc_b200.batched import RaggedBurgers
         from inc_b200.workloads import burgers_batched_config
@@ -1346,6 +1350,15 @@ def profile_small(dev, which="ks", rows=1024, tpp=32):
     s = torch.tensor(cfg["s"], dtype=torch.float32, device=dev)
     plan = solver.plan_for(u0, ds)
     frames = torch.empty(B, cfg["steps"], N, device=dev)
+    if which == "ks_tape":  # the tape rollout and its backward (no replay)
+        tape = torch.empty(plan.tape_size(cfg["steps"]), dtype=torch.uint8, device=dev)
+        g = torch.randn(B, cfg["steps"], N, device=dev)
+        gu, gs = torch.empty_like(u0), torch.empty_like(u0)
+        for _ in range(2):
+            plan.rollout_tape(u0, s, cfg["steps"], frames, None, tape)
+            plan.rollout_bwd_tape(tape, s, cfg["steps"], g, None, gu, gs)
+        torch.cuda.synchronize()
+        return
     if which == "ks_bwd":
         K = 8
         ck = torch.empty(B, (cfg["steps"] + K - 1) // K, N, device=dev)
