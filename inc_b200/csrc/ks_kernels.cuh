@@ -1163,11 +1163,13 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     const int nseg = (a.steps + K - 1) / K;
     // STG: this group's scratch for the replayed substep states (every launched group has one)
     float2* stg = STG ? a.stage + (size_t)pair * 3 * K * N : nullptr;
-    // STG: each step's frame adjoint is loaded one step ahead (it comes from HBM)
+    // STG with up to 8 values per lane: each step's frame adjoint is loaded one step
+    // ahead (it comes from HBM; wider lanes have no registers to spare for it)
+    constexpr bool GPRE = STG && P <= 8;
     const bool split = FAST ? false : a.split != 0;
     const int64_t gf_stride = (int64_t)a.steps * N;
     float2 gf[P];
-    if (STG && a.g_frames) load_pair_strided<P, T>(gf, a.g_frames, c, N, gf_stride, (int64_t)(a.steps - 1) * N);
+    if (GPRE && a.g_frames) load_pair_strided<P, T>(gf, a.g_frames, c, N, gf_stride, (int64_t)(a.steps - 1) * N);
     for (int sidx = nseg - 1; sidx >= 0; --sidx) {
         const int k0 = sidx * K;
         const int len = min(K, a.steps - k0);
@@ -1183,7 +1185,7 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
         }
         for (int j = len - 1; j >= 0; --j) {
             const int k = k0 + j;
-            if (STG && a.g_frames) {  // G += FFT(dL/dframe_k)/N, the next step's frame adjoint loaded meanwhile
+            if (GPRE && a.g_frames) {  // G += FFT(dL/dframe_k)/N, the next step's frame adjoint loaded meanwhile
                 float2 v[P];
 #pragma unroll
                 for (int m = 0; m < P; ++m) v[m] = gf[m];
@@ -1193,7 +1195,7 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
 #pragma unroll
                 for (int m = 0; m < P; ++m) G[m] = cadd(G[m], cscale(v[m], a.invN));
             }
-            step_bwd_program<P, T, STG, FAST>(a, c, cc, SS, G, Sacc, STG ? nullptr : a.g_frames, gf_stride,
+            step_bwd_program<P, T, STG, FAST>(a, c, cc, SS, G, Sacc, GPRE ? nullptr : a.g_frames, gf_stride,
                                               (int64_t)k * N, seg + j * N, st, buf, tw,
                                               STG ? stg + (size_t)j * 3 * N : nullptr);
         }
