@@ -7,6 +7,12 @@
 // width, one per lane group) through all steps with the state in registers.
 #include "burgers_kernels.cuh"
 
+// The ragged batch evaluates each interface's two WENO reconstructions in packed
+// FP32 pairs (weno5_pair); it is issue-bound, not FMA-pipe bound.
+#ifndef INC_RAGGED_PACKED
+#define INC_RAGGED_PACKED true
+#endif
+
 namespace inc {
 namespace burgers {
 
@@ -47,7 +53,7 @@ INC_DEV void ragged_rows(const RaggedArgs& ra, int row, int lane) {
     load_row_chunk<CPT>(u, ra.u0 + base, valid);
 #pragma unroll
     for (int c = 0; c < CPT; ++c) cmp[c] = 0.f;
-    for (int k = 0; k < ra.steps; ++k) advance<CPT, TPR>(a, cx, u, cmp, 0.f, left, right);
+    for (int k = 0; k < ra.steps; ++k) advance<CPT, TPR, INC_RAGGED_PACKED>(a, cx, u, cmp, 0.f, left, right);
     store_row_chunk<CPT>(ra.out + base, u, valid);
 }
 

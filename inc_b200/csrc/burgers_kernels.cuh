@@ -82,6 +82,39 @@ INC_DEV float weno5(float g0, float g1, float g2, float g3, float g4) {
     return w.h;
 }
 
+// weno5<false>(g0..g4) + weno5<true>(h0..h4), the two reconstructions of one
+// interface evaluated together in the two lanes of Blackwell's packed FP32 pairs
+// (fma/add/mul.f32x2: half the issue slots; the reciprocals stay scalar).  Same
+// operations per lane as weno5_eval, so the same values.
+INC_DEV float2 f2(float a, float b) { return make_float2(a, b); }
+INC_DEV float2 f2s(float a) { return make_float2(a, a); }
+INC_DEV float weno5_pair(float g0, float g1, float g2, float g3, float g4, float h0, float h1, float h2, float h3,
+                         float h4) {
+    const float2 G0 = f2(g0, h0), G1 = f2(g1, h1), G2 = f2(g2, h2), G3 = f2(g3, h3), G4 = f2(g4, h4);
+    const float2 qg0 = __ffma2_rn(f2s(0.0333333333f), G0, __ffma2_rn(f2s(-0.1166666667f), G1,
+                                                                      __fmul2_rn(f2s(0.1833333333f), G2)));
+    const float2 qg1 = __ffma2_rn(f2s(-0.1f), G1, __ffma2_rn(f2s(0.5f), G2, __fmul2_rn(f2s(0.2f), G3)));
+    const float2 qg2 = __ffma2_rn(f2s(0.1f), G2, __ffma2_rn(f2s(0.25f), G3, __fmul2_rn(f2s(-0.05f), G4)));
+    const float2 d0 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G1, G0), G2);
+    const float2 e0 = __fadd2_rn(__ffma2_rn(f2s(-4.f), G1, G0), __fmul2_rn(f2s(3.f), G2));
+    const float2 d1 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G2, G1), G3);
+    const float2 e1 = __fadd2_rn(G1, __fmul2_rn(f2s(-1.f), G3));
+    const float2 d2 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G3, G2), G4);
+    // left: (-4 g3 + 3 g2) + g4; right: (-4 g3 + g2) + 3 g4
+    const float2 e2 = __fadd2_rn(__ffma2_rn(f2s(-4.f), G3, __fmul2_rn(f2(3.f, 1.f), G2)), __fmul2_rn(f2(1.f, 3.f), G4));
+    const float2 c313 = f2s(3.f / 13.f), eps = f2s(kEpsScaled);
+    const float2 s0 = __fadd2_rn(eps, __ffma2_rn(d0, d0, __fmul2_rn(__fmul2_rn(c313, e0), e0)));
+    const float2 s1 = __fadd2_rn(eps, __ffma2_rn(d1, d1, __fmul2_rn(__fmul2_rn(c313, e1), e1)));
+    const float2 s2 = __fadd2_rn(eps, __ffma2_rn(d2, d2, __fmul2_rn(__fmul2_rn(c313, e2), e2)));
+    const float2 q0 = __fmul2_rn(s0, s0), q1 = __fmul2_rn(s1, s1), q2 = __fmul2_rn(s2, s2);
+    const float2 r0 = f2(rcp_approx(q0.x), rcp_approx(q0.y)), r1 = f2(rcp_approx(q1.x), rcp_approx(q1.y)),
+                 r2 = f2(rcp_approx(q2.x), rcp_approx(q2.y));
+    const float2 den = __ffma2_rn(f2s(0.1f), r0, __ffma2_rn(f2s(0.6f), r1, __fmul2_rn(f2s(0.3f), r2)));
+    const float2 inv = f2(rcp_approx(den.x), rcp_approx(den.y));
+    const float2 h = __fmul2_rn(__ffma2_rn(qg0, r0, __ffma2_rn(qg1, r1, __fmul2_rn(qg2, r2))), inv);
+    return h.x + h.y;
+}
+
 // Adds hb * d h / d g_m to acc[0..4] (the vector-Jacobian product of weno5).
 // With w_k = alpha_k / S:  dh/dq_k = w_k,  dh/dbeta_k = -2 w_k (q_k - h) / (eps + beta_k).
 template <bool RIGHT>
@@ -193,16 +226,21 @@ INC_DEV void halo_window(const float (&u)[CPT], float (&w)[CPT + 6], int left, i
 // same row values by the same operations, so the callers hand it over (a shuffle,
 // or a shared slot) instead of reconstructing it again.  The r loop stays inline
 // at each caller: as a separate function it made the fused CNN kernel 13% slower.
-template <int CPT>
+template <int CPT, bool PK = false>
 INC_DEV void weno_right_fluxes(const float (&w)[CPT + 6], float alpha, float (&hs)[CPT]) {
     const float ha = 0.5f * alpha;
     float fp[CPT + 6], fm[CPT + 6];
 #pragma unroll
     for (int k = 1; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
 #pragma unroll
-    for (int c = 0; c < CPT; ++c)
-        hs[c] = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
-                weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+    for (int c = 0; c < CPT; ++c) {
+        if constexpr (PK)
+            hs[c] = weno5_pair(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5], fm[c + 2], fm[c + 3], fm[c + 4],
+                               fm[c + 5], fm[c + 6]);
+        else
+            hs[c] = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
+                    weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+    }
 }
 
 // central-difference convection (calc_nonlinear_FDM, solver_1d.py:125-127) + diffusion
@@ -216,7 +254,7 @@ INC_DEV void fdm_rhs(const float (&w)[CPT + 6], float nu_dx2, float inv_2dx, flo
 }
 
 // r = nonlinear + linear (no source): calc_nonlinear_weno / _FDM + calc_linear.
-template <int CPT, int TPR>
+template <int CPT, int TPR, bool PK = false>
 INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu,
                       float inv_dx, float inv_dx2, float inv_2dx, int left, int right) {
     float w[CPT + 6];
@@ -229,7 +267,7 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
         const float nu_dx2 = nu * inv_dx2;
         if constexpr (CPT <= 8) {
             float hs[CPT];
-            weno_right_fluxes<CPT>(w, alpha, hs);
+            weno_right_fluxes<CPT, PK>(w, alpha, hs);
             float prev = shfl<TPR>(hs[CPT - 1], left);
 #pragma unroll
             for (int c = 0; c < CPT; ++c) {
@@ -246,11 +284,15 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
             float fp[CPT + 6], fm[CPT + 6];
 #pragma unroll
             for (int k = 0; k < CPT + 6; ++k) flux_split(w[k], ha, fp[k], fm[k]);
-            float prev = weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]) + weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
+            float prev = PK ? weno5_pair(fp[0], fp[1], fp[2], fp[3], fp[4], fm[1], fm[2], fm[3], fm[4], fm[5])
+                            : weno5<false>(fp[0], fp[1], fp[2], fp[3], fp[4]) +
+                                  weno5<true>(fm[1], fm[2], fm[3], fm[4], fm[5]);
 #pragma unroll
             for (int c = 0; c < CPT; ++c) {
-                const float hs = weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
-                                 weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
+                const float hs = PK ? weno5_pair(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5], fm[c + 2],
+                                                 fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6])
+                                    : weno5<false>(fp[c + 1], fp[c + 2], fp[c + 3], fp[c + 4], fp[c + 5]) +
+                                          weno5<true>(fm[c + 2], fm[c + 3], fm[c + 4], fm[c + 5], fm[c + 6]);
                 const float lap = fmaf(-2.f, w[c + 3], w[c + 2] + w[c + 4]);
                 r[c] = fmaf(inv_dx, prev - hs, nu_dx2 * lap);
                 prev = hs;
@@ -286,10 +328,10 @@ INC_DEV void add_source(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT]
     }
 }
 
-template <int CPT, int TPR>
+template <int CPT, int TPR, bool PK = false>
 INC_DEV void full_rhs(const Args& a, const Ctx<CPT>& cx, const float (&u)[CPT], float (&r)[CPT], float t,
                       int left, int right) {
-    rhs_core<CPT, TPR>(u, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, left, right);
+    rhs_core<CPT, TPR, PK>(u, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, left, right);
     add_source<CPT>(a, cx, u, r, t);
 }
 
@@ -317,7 +359,7 @@ INC_DEV float rk3_b(int k) { return k == 0 ? 1.f : (k == 1 ? 0.25f : 2.f / 3.f);
 // relative L2 after 500 SSP-RK3 steps of the ragged benchmark rows (6e-8 with
 // it).  The stages run as a loop around one copy of the right-hand side
 // (instruction cache).
-template <int CPT, int TPR>
+template <int CPT, int TPR, bool PK = false>
 INC_DEV void advance(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], float (&cmp)[CPT], float t, int left,
                      int right) {
     float r[CPT], u0[CPT], d[CPT];
@@ -327,7 +369,7 @@ INC_DEV void advance(const Args& a, const Ctx<CPT>& cx, float (&u)[CPT], float (
     for (int c = 0; c < CPT; ++c) { u0[c] = u[c]; d[c] = 0.f; }
 #pragma unroll 1
     for (int k = 0; k < stages; ++k) {
-        full_rhs<CPT, TPR>(a, cx, u, r, t + rk3_c(k) * dt, left, right);
+        full_rhs<CPT, TPR, PK>(a, cx, u, r, t + rk3_c(k) * dt, left, right);
         const float kb = rk3_b(k);
 #pragma unroll
         for (int c = 0; c < CPT; ++c) {
