@@ -541,9 +541,17 @@ def bench_burgers_plain(args, dev, world):
             u = api.step(u)
             frames[:, k] = u
 
+    def api_steps():  # the drop-in step alone, without the frame copies
+        api.t = 0.0
+        u = u0
+        for _ in range(steps):
+            u = api.step(u)
+
     with torch.no_grad():
         api_loop()
         t_api = event_time(api_loop, max(2, args.steps // 2), flush)
+        api_steps()
+        t_api_only = event_time(api_steps, max(2, args.steps // 2), flush)
     K = 8
     ckpts = torch.empty(B, (steps + K - 1) // K, N, device=dev)
     g_frames = torch.randn(B, steps, N, device=dev)
@@ -589,7 +597,7 @@ def bench_burgers_plain(args, dev, world):
     plain_ms_step = sum(t_plain) / len(t_plain) / steps
     times = dict(fused=ms_fused, plain=sum(t_plain) / len(t_plain), graph=sum(t_graph) / len(t_graph),
                  fused_fb=sum(t_ffb) / len(t_ffb), plain_fb=sum(t_pfb) / len(t_pfb), e2e=sum(t_e2e) / len(t_e2e),
-                 api=sum(t_api) / len(t_api))
+                 api=sum(t_api) / len(t_api), api_only=sum(t_api_only) / len(t_api_only))
     extra = dict(flops_per_cell_step=flops_cell, peak=peak, achieved=achieved,
                  plain_hbm_gbs=plain_bytes_per_cell_step(False) * B * N / (plain_ms_step * 1e-3) / 1e9,
                  clocks=clk.summary(), h2d=B * N * 4, d2h=B * N * 4, launches=args.steps, error=error)
@@ -1207,6 +1215,7 @@ def plain_line(args, world, cfg, cells, times, extra, cpu_b):
             p["api_step_ms"] = times["api"] / cfg["steps"]
             p["graph_step_ms"] = times["graph"] / cfg["steps"]
             p["api_over_graph_time"] = times["api"] / times["graph"]
+            p["api_step_only_ms"] = times["api_only"] / cfg["steps"]
             p["api_is"] = "BurgersSolverTorch.step(u) per step, eager (the drop-in API simulate_rollout calls)"
         line["plain"] = p
     return line

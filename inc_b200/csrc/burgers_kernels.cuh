@@ -651,7 +651,16 @@ struct WideSmem {
 };
 
 
-template <int CPT, int TPR>
+// The barrier of the threads that run one row: the whole CTA (BAR = 0), or one of
+// the two thread groups of the warp-specialised adjoint (named barrier BAR over NT
+// threads).
+template <int BAR, int NT>
+INC_DEV void row_sync() {
+    if constexpr (BAR == 0) __syncthreads();
+    else asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(NT) : "memory");
+}
+
+template <int CPT, int TPR, int BAR = 0>
 INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, float nu, float inv_dx, float inv_dx2,
                            float inv_2dx, WideSmem<CPT, TPR>& sh, int parity, int g) {
     constexpr int N = CPT * TPR;
@@ -663,7 +672,7 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
     for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
     m = group_max_nonneg<32>(m);
     if ((g & 31) == 0) sh.wmax[parity][g >> 5] = m;
-    __syncthreads();
+    row_sync<BAR, TPR>();
     float w[CPT + 6];
 #pragma unroll
     for (int k = 0; k < CPT + 6; ++k) w[k] = row[(g * CPT - 3 + k + N) & (N - 1)];
@@ -675,7 +684,7 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
         float hs[CPT];
         weno_right_fluxes<CPT>(w, alpha, hs);
         sh.flux[parity][g] = hs[CPT - 1];
-        __syncthreads();
+        row_sync<BAR, TPR>();
         float prev = sh.flux[parity][(g + TPR - 1) % TPR];
         const float nu_dx2 = nu * inv_dx2;
 #pragma unroll
@@ -689,10 +698,10 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
     }
 }
 
-template <int CPT, int TPR>
+template <int CPT, int TPR, int BAR = 0>
 INC_DEV void full_rhs_wide(const Args& a, const Ctx<CPT>& cx, const float (&x)[CPT], float (&r)[CPT], float t,
                            WideSmem<CPT, TPR>& sh, int& parity, int g) {
-    rhs_core_wide<CPT, TPR>(x, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, sh, parity, g);
+    rhs_core_wide<CPT, TPR, BAR>(x, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, sh, parity, g);
     parity ^= 1;
     add_source<CPT>(a, cx, x, r, t);
 }
@@ -756,7 +765,7 @@ struct WideAdjSmem {
 // out = J(u)^T v at this thread's cell: rhs_vjp for one cell per thread, the
 // halos, the row max |u| with its first argmax (alpha's gradient) and the
 // neighbours' contributions through shared memory (two block barriers).
-template <int TPR>
+template <int TPR, int BAR = 0>
 INC_DEV void rhs_vjp_wide(const Args& a, const Ctx<1>& cx, float u, float v, float& out, WideAdjSmem<TPR>& sh,
                           int g) {
     constexpr int N = TPR, NW = TPR / 32;
@@ -774,7 +783,7 @@ INC_DEV void rhs_vjp_wide(const Args& a, const Ctx<1>& cx, float u, float v, flo
             sh.warg[warp] = mi;
         }
     }
-    __syncthreads();
+    row_sync<BAR, TPR>();
     float w[7];
 #pragma unroll
     for (int k = 0; k < 7; ++k) w[k] = sh.urow[(g - 3 + k + N) & (N - 1)];
@@ -810,7 +819,7 @@ INC_DEV void rhs_vjp_wide(const Args& a, const Ctx<1>& cx, float u, float v, flo
         abar = group_sum<32>(abar);
         if (lane == 0) sh.wsum[warp] = abar;
     }
-    __syncthreads();
+    row_sync<BAR, TPR>();
     if (weno) {
         out = sh.ub[0][(g + 2) & (N - 1)] + sh.ub[1][(g + 1) & (N - 1)] + sh.ub[2][g] +
               sh.ub[3][(g + N - 1) & (N - 1)] + sh.ub[4][(g + N - 2) & (N - 1)] + sh.ub[5][(g + N - 3) & (N - 1)];
@@ -830,7 +839,7 @@ INC_DEV void rhs_vjp_wide(const Args& a, const Ctx<1>& cx, float u, float v, flo
 
 // The stages' adjoints in reverse (see advance_bwd) for one cell per thread,
 // given the step's stage inputs u, u1, u2 (u1, u2 unused for Euler).
-template <int TPR>
+template <int TPR, int BAR = 0>
 INC_DEV void stages_bwd_wide(const Args& a, const Ctx<1>& cx, float u, float u1, float u2, float& gu, float& gs,
                              WideAdjSmem<TPR>& sh, int g) {
     const float dt = cx.dt;
@@ -838,7 +847,7 @@ INC_DEV void stages_bwd_wide(const Args& a, const Ctx<1>& cx, float u, float u1,
     float acc = 0.f;
     for (int k = stages - 1; k >= 0; --k) {
         float rv;
-        rhs_vjp_wide<TPR>(a, cx, k == 2 ? u2 : (k == 1 ? u1 : u), gu, rv, sh, g);
+        rhs_vjp_wide<TPR, BAR>(a, cx, k == 2 ? u2 : (k == 1 ? u1 : u), gu, rv, sh, g);
         const float ka = rk3_a(k), kb = rk3_b(k);
         gs += kb * dt * gu;
         acc += ka * gu;
@@ -964,6 +973,84 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
     if (a.g_s) a.g_s[base] = gs;
 }
 
+// The same backward, warp-specialised: 2 TPR threads per row.  Threads [0, TPR)
+// replay segment s - 1 from its checkpoint (every step's three stage inputs, into
+// one half of a double buffer) while threads [TPR, 2 TPR) differentiate segment s
+// from the other half, so the replay leaves the adjoint's critical path.  Each
+// group syncs on its own named barrier (1: replay, 2: adjoint); the two meet at
+// one CTA barrier per segment, where the halves change hands.
+template <int TPR>
+__global__ void __launch_bounds__(2 * TPR, 1) k_rollout_bwd_wide2(Args a) {
+    __shared__ WideSmem<1, TPR> shr;
+    __shared__ WideAdjSmem<TPR> sha;
+    extern __shared__ float segbuf[];  // [2][3 ckpt_every][TPR]
+    const int row = blockIdx.x;
+    const bool rep = threadIdx.x < TPR;
+    const int g = rep ? threadIdx.x : threadIdx.x - TPR;
+    Ctx<1> cx;
+    make_ctx<1, TPR>(a, row, g, true, cx);
+    if (cx.has_s) cx.s[0] = __ldg(a.s + (int64_t)row * TPR + g);
+    const int K = a.ckpt_every;
+    const int nseg = (a.steps + K - 1) / K;
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
+    const float dt = cx.dt;
+    const int64_t base = (int64_t)row * TPR + g;
+    const int half = 3 * K * TPR;
+    const float* ckr = a.ckpts + (int64_t)row * nseg * TPR + g;
+    int parity = 0;
+    // segment sidx replayed into its half of the buffer (replay group)
+    auto replay = [&](int sidx) {
+        float* seg = segbuf + (sidx & 1) * half;
+        const int k0 = sidx * K;
+        const int len = min(K, a.steps - k0);
+        float x[1] = {__ldg(ckr + (int64_t)sidx * TPR)}, r[1];
+        for (int j = 0; j < len; ++j) {
+            const float t = cx.t + (k0 + j) * dt;
+            const float u0 = x[0];
+            seg[3 * j * TPR + g] = u0;
+            const int run = j + 1 < len ? stages : stages - 1;
+            float d = 0.f;
+            for (int k = 0; k < run; ++k) {  // as advance_wide
+                full_rhs_wide<1, TPR, 1>(a, cx, x, r, t + rk3_c(k) * dt, shr, parity, g);
+                d = rk3_b(k) * fmaf(dt, r[0], d);
+                x[0] = u0 + d;
+                if (k + 1 < stages) seg[(3 * j + 1 + k) * TPR + g] = x[0];
+            }
+        }
+    };
+    if (rep) replay(nseg - 1);
+    __syncthreads();
+    const float* gfr = a.g_frames ? a.g_frames + (int64_t)row * a.steps * TPR + g : nullptr;
+    float gu = 0.f, gf = 0.f, gs = 0.f;
+    if (!rep) {
+        gu = a.g_final ? __ldg(a.g_final + base) : 0.f;
+        gf = gfr ? __ldg(gfr + (int64_t)(a.steps - 1) * TPR) : 0.f;
+    }
+    for (int sidx = nseg - 1; sidx >= 0; --sidx) {
+        if (rep) {
+            if (sidx > 0) replay(sidx - 1);
+        } else {
+            const float* seg = segbuf + (sidx & 1) * half;
+            const int k0 = sidx * K;
+            const int len = min(K, a.steps - k0);
+            for (int j = len - 1; j >= 0; --j) {
+                const int k = k0 + j;
+                if (gfr) {
+                    gu += gf;
+                    if (k > 0) gf = __ldg(gfr + (int64_t)(k - 1) * TPR);
+                }
+                stages_bwd_wide<TPR, 2>(a, cx, seg[3 * j * TPR + g], seg[(3 * j + 1) * TPR + g],
+                                        seg[(3 * j + 2) * TPR + g], gu, gs, sha, g);
+            }
+        }
+        __syncthreads();  // segment sidx - 1 replayed, segment sidx's half free
+    }
+    if (!rep) {
+        a.g_u[base] = gu;
+        if (a.g_s) a.g_s[base] = gs;
+    }
+}
+
 // weno_reconstruction(f, direction) as a standalone op (solver_1d.py:4-42).
 template <int CPT, int TPR>
 __global__ void __launch_bounds__(256) k_weno(const float* __restrict__ f, float* __restrict__ out, int rows,
@@ -1042,6 +1129,8 @@ int launch_bwd_wide(Kind kind, const Args& a, cudaStream_t st);
 
 template <int TPR>
 constexpr size_t bwd_wide_static_smem() { return sizeof(WideAdjSmem<TPR>); }
+template <int TPR>
+constexpr size_t bwd_wide2_static_smem() { return sizeof(WideAdjSmem<TPR>) + sizeof(WideSmem<1, TPR>); }
 
 template <int TPR>
 int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
@@ -1054,6 +1143,18 @@ int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
         b.g_frames = nullptr;
     }
     const size_t smem = (size_t)3 * b.ckpt_every * TPR * sizeof(float);
+    const int nseg = (b.steps + b.ckpt_every - 1) / b.ckpt_every;
+    // several segments: the warp-specialised form overlaps each replay with the adjoint
+    // before it (two thread groups; rows up to 256 cells keep 128 registers a thread)
+    if constexpr (TPR <= 256) {
+        if (nseg >= 2 && 2 * smem + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
+            if (2 * smem + bwd_wide2_static_smem<TPR>() > 48 * 1024)
+                cudaFuncSetAttribute(k_rollout_bwd_wide2<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                     (int)(2 * smem));
+            k_rollout_bwd_wide2<TPR><<<b.rows, 2 * TPR, 2 * smem, st>>>(b);
+            return check_launch("burgers_bwd_wide2");
+        }
+    }
     if (smem + bwd_wide_static_smem<TPR>() > 48 * 1024)  // the 48 KB default covers static + dynamic
         cudaFuncSetAttribute(k_rollout_bwd_wide<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     k_rollout_bwd_wide<TPR><<<b.rows, TPR, smem, st>>>(b);
