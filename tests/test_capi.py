@@ -86,3 +86,37 @@ def test_ks_rollout_bwd_work_size_needs_no_gpu(lib):
     p.npairs = 512
     assert lib.inc_ks_rollout_bwd_ws(C.byref(p), None, None, 1, 8, None, None, None, None, None, 0,
                                      None) == nat.INC_E_INVALID
+
+
+def test_new_entry_points_check_arguments_without_gpu(lib):
+    """Sizes and argument checks of the tape, adaptive, term and substep entry points,
+    all decided on the host before any CUDA call."""
+    from inc_b200 import _native as nat
+    p = nat.KSPlan()
+    p.rows, p.n, p.npairs, p.threads_per_pair = 1024, 256, 512, 32
+    # the tape: 4 complex [n] states per row pair and step, row pairs rounded up to 32
+    assert lib.inc_ks_tape_size(C.byref(p), 400) == 512 * 400 * 4 * 256 * 8
+    p.npairs = 513
+    assert lib.inc_ks_tape_size(C.byref(p), 2) == 544 * 2 * 4 * 256 * 8
+    assert lib.inc_ks_tape_size(C.byref(p), 0) == -1
+    assert lib.inc_ks_rollout_bwd_tape(C.byref(p), None, 0, None, 2, None, None, None, None, None) \
+        == nat.INC_E_INVALID
+    # adaptive CFL: the work buffer holds a 64-byte control block and two doubles per substep
+    assert lib.inc_burgers_step_adaptive_work_size(1000) >= 64 + 16 * 1001
+    assert lib.inc_burgers_step_adaptive_work_size(0) == -1
+    d = nat.BurgersDesc()
+    d.rows, d.n, d.dx, d.dt = 2, 64, 0.1, 0.01
+    fake = C.c_void_p(256)  # never dereferenced: the call is rejected before any launch
+    assert lib.inc_burgers_step_adaptive(C.byref(d), 0.2, 1000, fake, None, None, 0.0, fake, None, None, None,
+                                         None) == nat.INC_E_INVALID
+    assert b"work" in lib.inc_last_error_string()
+    d.scheme = nat.INC_TS_SSPRK3
+    assert lib.inc_burgers_step_adaptive(C.byref(d), 0.2, 1000, fake, None, None, 0.0, fake, None, fake, None,
+                                         None) == nat.INC_E_INVALID  # forward Euler only
+    # terms and spectra
+    d.scheme, d.rows = nat.INC_TS_EULER, 0
+    assert lib.inc_burgers_terms(C.byref(d), fake, None, 0.0, None, None, None, None) == nat.INC_E_INVALID
+    assert lib.inc_ks_fft_rows(fake, fake, 4, 64, 3, None) == nat.INC_E_INVALID
+    assert lib.inc_ks_fft_rows(fake, fake, 4, 96, 1, None) == nat.INC_E_UNSUPPORTED
+    p.npairs = 0
+    assert lib.inc_ks_substep(C.byref(p), fake, None, fake, None) == nat.INC_E_INVALID
