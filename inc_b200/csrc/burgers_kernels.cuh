@@ -147,49 +147,6 @@ INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float h
     c4 += (-1.f / 6.f) * qb2 + A2 + (RIGHT ? 3.f : 1.f) * E2;
 }
 
-// weno5_vjp with the direction a runtime value (no divergence when the two
-// directions run on adjacent lanes): c[0..4] += hb * dh/dg.  Same arithmetic as
-// weno5_eval / weno5_vjp for that direction.
-INC_DEV void weno5_vjp_dir(bool right, float g0, float g1, float g2, float g3, float g4, float hb, float (&c)[5]) {
-    Weno w;
-    const float k2 = right ? 1.f : 3.f, k4 = right ? 3.f : 1.f;
-    w.qg0 = fmaf(0.0333333333f, g0, fmaf(-0.1166666667f, g1, 0.1833333333f * g2));
-    w.qg1 = fmaf(-0.1f, g1, fmaf(0.5f, g2, 0.2f * g3));
-    w.qg2 = fmaf(0.1f, g2, fmaf(0.25f, g3, -0.05f * g4));
-    w.d0 = fmaf(-2.f, g1, g0) + g2;
-    w.e0 = fmaf(-4.f, g1, g0) + 3.f * g2;
-    w.d1 = fmaf(-2.f, g2, g1) + g3;
-    w.e1 = g1 - g3;
-    w.d2 = fmaf(-2.f, g3, g2) + g4;
-    w.e2 = fmaf(-4.f, g3, k2 * g2) + k4 * g4;
-    w.s0 = kEpsScaled + fmaf(w.d0, w.d0, (3.f / 13.f) * w.e0 * w.e0);
-    w.s1 = kEpsScaled + fmaf(w.d1, w.d1, (3.f / 13.f) * w.e1 * w.e1);
-    w.s2 = kEpsScaled + fmaf(w.d2, w.d2, (3.f / 13.f) * w.e2 * w.e2);
-    w.r0 = rcp_approx(w.s0 * w.s0);
-    w.r1 = rcp_approx(w.s1 * w.s1);
-    w.r2 = rcp_approx(w.s2 * w.s2);
-    w.inv_den = rcp_approx(fmaf(0.1f, w.r0, fmaf(0.6f, w.r1, 0.3f * w.r2)));
-    w.h = fmaf(w.qg0, w.r0, fmaf(w.qg1, w.r1, w.qg2 * w.r2)) * w.inv_den;
-    const float w0 = 0.1f * w.r0 * w.inv_den, w1 = 0.6f * w.r1 * w.inv_den, w2 = 0.3f * w.r2 * w.inv_den;
-    const float q0 = 10.f * w.qg0, q1 = w.qg1 * (1.f / 0.6f), q2 = w.qg2 * (1.f / 0.3f);
-    const float qb0 = hb * w0, qb1 = hb * w1, qb2 = hb * w2;
-    const float bb0 = (-24.f / 13.f) * qb0 * (q0 - w.h) * rcp_approx(w.s0);
-    const float bb1 = (-24.f / 13.f) * qb1 * (q1 - w.h) * rcp_approx(w.s1);
-    const float bb2 = (-24.f / 13.f) * qb2 * (q2 - w.h) * rcp_approx(w.s2);
-    const float A0 = 13.f / 6.f * w.d0 * bb0, E0 = 0.5f * w.e0 * bb0;
-    const float A1 = 13.f / 6.f * w.d1 * bb1, E1 = 0.5f * w.e1 * bb1;
-    const float A2 = 13.f / 6.f * w.d2 * bb2, E2 = 0.5f * w.e2 * bb2;
-    c[0] += (1.f / 3.f) * qb0 + A0 + E0;
-    c[1] += (-7.f / 6.f) * qb0 - 2.f * A0 - 4.f * E0;
-    c[2] += (11.f / 6.f) * qb0 + A0 + 3.f * E0;
-    c[1] += (-1.f / 6.f) * qb1 + A1 + E1;
-    c[2] += (5.f / 6.f) * qb1 - 2.f * A1;
-    c[3] += (1.f / 3.f) * qb1 + A1 - E1;
-    c[2] += (1.f / 3.f) * qb2 + A2 + k2 * E2;
-    c[3] += (5.f / 6.f) * qb2 - 2.f * A2 - 4.f * E2;
-    c[4] += (-1.f / 6.f) * qb2 + A2 + k4 * E2;
-}
-
 // Lax-Friedrichs flux splitting of f = u^2 / 2 (solver_1d.py:134-137):
 // f+- = (f +- alpha u) / 2 = u (u / 4 +- alpha / 2);  ha = alpha / 2.
 INC_DEV void flux_split(float u, float ha, float& fp, float& fm) {
@@ -1094,202 +1051,6 @@ __global__ void __launch_bounds__(2 * TPR, 1) k_rollout_bwd_wide2(Args a) {
     }
 }
 
-// ---- small-batch adjoint with two threads per cell ------------------------------
-// The adjoint's cost per cell is its two WENO5 vector-Jacobian products; with one
-// row per CTA and few rows the GPU is latency-bound, so each cell's two run on two
-// threads (h = 0: the f+ reconstruction, h = 1: the f- one; adjacent lanes), whose
-// contributions meet by one shuffle.  Everything else a cell needs is computed by
-// both threads of its pair.
-template <int TPR>
-struct SplitAdjSmem {
-    static constexpr int NW = 2 * TPR / 32;  // warps of the adjoint group
-    float urow[TPR];
-    float vrow[TPR];
-    float ub[6][TPR];
-    float wmax[NW];
-    int warg[NW];
-    float wsum[NW];
-};
-
-// rhs_vjp_wide for cell g by the thread pair (g, h); barrier BAR over 2 TPR threads.
-template <int TPR, int BAR>
-INC_DEV void rhs_vjp_split(const Args& a, const Ctx<1>& cx, float u, float v, float& out, SplitAdjSmem<TPR>& sh,
-                           int g, int h, int lane, int warp) {
-    constexpr int N = TPR, NW = SplitAdjSmem<TPR>::NW;
-    if (h == 0) {
-        sh.urow[g] = u;
-        sh.vrow[g] = v;
-    }
-    const bool weno = a.conv == INC_CONV_WENO;
-    if (weno) {  // as the forward's fmaxf: a NaN cell is passed over
-        const float au = fabsf(u);
-        float m = au > 0.f ? au : 0.f;
-        int mi = g;
-        group_argmax_nonneg<32>(m, mi);
-        if (lane == 0) {
-            sh.wmax[warp] = m;
-            sh.warg[warp] = mi;
-        }
-    }
-    row_sync<BAR, 2 * TPR>();
-    float w[7];
-#pragma unroll
-    for (int k = 0; k < 7; ++k) w[k] = sh.urow[(g - 3 + k + N) & (N - 1)];
-    const float v_r = sh.vrow[(g + 1) & (N - 1)], v_l = sh.vrow[(g + N - 1) & (N - 1)];
-    float alpha = 0.f;
-    int am = 0;
-    if (weno) {
-        alpha = sh.wmax[0];
-        am = sh.warg[0];
-#pragma unroll
-        for (int i = 1; i < NW; ++i)
-            if (sh.wmax[i] > alpha) {
-                alpha = sh.wmax[i];
-                am = sh.warg[i];
-            }
-        // this thread's half: f+ (h = 0) at cells g-2..g+2, or f- (h = 1) at g-1..g+3
-        const float sgn = h == 0 ? 1.f : -1.f;
-        float acc[6];  // index e <-> cell g - 2 + e
-#pragma unroll
-        for (int e = 0; e < 6; ++e) acc[e] = 0.f;
-        const float hb = (v_r - v) * a.inv_dx;
-        float fw5[5];  // f+ at cells g-2..g+2 (h = 0) or f- at g-1..g+3 (h = 1)
-#pragma unroll
-        for (int k = 0; k < 5; ++k) {
-            float fp, fm;
-            flux_split(w[k + 1 + h], 0.5f * alpha, fp, fm);
-            fw5[k] = h == 0 ? fp : fm;
-        }
-        float c5[5] = {0.f, 0.f, 0.f, 0.f, 0.f};
-        weno5_vjp_dir(h != 0, fw5[0], fw5[1], fw5[2], fw5[3], fw5[4], hb, c5);
-        // h = 0 covers cells g-2..g+2 (acc[0..4]), h = 1 cells g-1..g+3 (acc[1..5])
-#pragma unroll
-        for (int e = 0; e < 6; ++e) acc[e] = h == 0 ? (e < 5 ? c5[e] : 0.f) : (e > 0 ? c5[e - 1] : 0.f);
-        float abar = 0.f;
-#pragma unroll
-        for (int e = 0; e < 6; ++e) {
-            const float uj = w[e + 1];
-            float part = acc[e] * (0.5f * fmaf(sgn, alpha, uj));
-            abar += sgn * 0.5f * uj * acc[e];
-            part += __shfl_xor_sync(0xffffffffu, part, 1);
-            if (h == 0) sh.ub[e][g] = part;
-        }
-        abar = group_sum<32>(abar);
-        if (lane == 0) sh.wsum[warp] = abar;
-    }
-    row_sync<BAR, 2 * TPR>();
-    if (weno) {
-        out = sh.ub[0][(g + 2) & (N - 1)] + sh.ub[1][(g + 1) & (N - 1)] + sh.ub[2][g] +
-              sh.ub[3][(g + N - 1) & (N - 1)] + sh.ub[4][(g + N - 2) & (N - 1)] + sh.ub[5][(g + N - 3) & (N - 1)];
-        if (g == am) {  // alpha = |u[argmax]|: d|u|/du = sign(u) (torch.abs backward, 0 at 0)
-            float abar = 0.f;
-#pragma unroll
-            for (int i = 0; i < NW; ++i) abar += sh.wsum[i];
-            const float sg = u > 0.f ? 1.f : (u < 0.f ? -1.f : 0.f);
-            out = fmaf(abar, sg, out);
-        }
-    } else {  // R_i = -u_i (u_{i+1} - u_{i-1}) / (2 dx)
-        out = -v * ((w[4] - w[2]) * a.inv_2dx) - v_l * w[2] * a.inv_2dx + v_r * w[4] * a.inv_2dx;
-    }
-    out += cx.nu * ((v_l - 2.f * v + v_r) * a.inv_dx2);
-    if (a.src == INC_SRC_LINEAR) out = fmaf(cx.beta, v, out);
-}
-
-// stages_bwd_wide with two threads per cell.
-template <int TPR, int BAR>
-INC_DEV void stages_bwd_split(const Args& a, const Ctx<1>& cx, float u, float u1, float u2, float& gu, float& gs,
-                              SplitAdjSmem<TPR>& sh, int g, int h, int lane, int warp) {
-    const float dt = cx.dt;
-    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
-    float acc = 0.f;
-    for (int k = stages - 1; k >= 0; --k) {
-        float rv;
-        rhs_vjp_split<TPR, BAR>(a, cx, k == 2 ? u2 : (k == 1 ? u1 : u), gu, rv, sh, g, h, lane, warp);
-        const float ka = rk3_a(k), kb = rk3_b(k);
-        gs += kb * dt * gu;
-        acc += ka * gu;
-        gu = kb * (gu + dt * rv);
-    }
-    gu += acc;
-}
-
-// k_rollout_bwd_wide2 with the adjoint on two threads per cell: 3 TPR threads per
-// row, [0, TPR) replay the next segment, [TPR, 3 TPR) differentiate this one,
-// cell g on threads TPR + 2 g (f+ half) and TPR + 2 g + 1 (f- half).
-template <int TPR>
-__global__ void __launch_bounds__(3 * TPR, 1) k_rollout_bwd_wide3(Args a) {
-    __shared__ WideSmem<1, TPR> shr;
-    __shared__ SplitAdjSmem<TPR> sha;
-    extern __shared__ float segbuf[];  // [2][3 ckpt_every][TPR]
-    const int row = blockIdx.x;
-    const bool rep = threadIdx.x < TPR;
-    const int ai = threadIdx.x - TPR;  // adjoint-group thread
-    const int g = rep ? threadIdx.x : ai >> 1;
-    const int h = rep ? 0 : ai & 1;
-    const int lane = threadIdx.x & 31, warp = rep ? 0 : ai >> 5;
-    Ctx<1> cx;
-    make_ctx<1, TPR>(a, row, g, true, cx);
-    if (cx.has_s) cx.s[0] = __ldg(a.s + (int64_t)row * TPR + g);
-    const int K = a.ckpt_every;
-    const int nseg = (a.steps + K - 1) / K;
-    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
-    const float dt = cx.dt;
-    const int64_t base = (int64_t)row * TPR + g;
-    const int half = 3 * K * TPR;
-    const float* ckr = a.ckpts + (int64_t)row * nseg * TPR + g;
-    int parity = 0;
-    auto replay = [&](int sidx) {
-        float* seg = segbuf + (sidx & 1) * half;
-        const int k0 = sidx * K;
-        const int len = min(K, a.steps - k0);
-        float x[1] = {__ldg(ckr + (int64_t)sidx * TPR)}, r[1];
-        for (int j = 0; j < len; ++j) {
-            const float t = cx.t + (k0 + j) * dt;
-            const float u0 = x[0];
-            seg[3 * j * TPR + g] = u0;
-            const int run = j + 1 < len ? stages : stages - 1;
-            float d = 0.f;
-            for (int k = 0; k < run; ++k) {  // as advance_wide
-                full_rhs_wide<1, TPR, 1>(a, cx, x, r, t + rk3_c(k) * dt, shr, parity, g);
-                d = rk3_b(k) * fmaf(dt, r[0], d);
-                x[0] = u0 + d;
-                if (k + 1 < stages) seg[(3 * j + 1 + k) * TPR + g] = x[0];
-            }
-        }
-    };
-    if (rep) replay(nseg - 1);
-    __syncthreads();
-    const float* gfr = a.g_frames ? a.g_frames + (int64_t)row * a.steps * TPR + g : nullptr;
-    float gu = 0.f, gf = 0.f, gs = 0.f;
-    if (!rep) {
-        gu = a.g_final ? __ldg(a.g_final + base) : 0.f;
-        gf = gfr ? __ldg(gfr + (int64_t)(a.steps - 1) * TPR) : 0.f;
-    }
-    for (int sidx = nseg - 1; sidx >= 0; --sidx) {
-        if (rep) {
-            if (sidx > 0) replay(sidx - 1);
-        } else {
-            const float* seg = segbuf + (sidx & 1) * half;
-            const int k0 = sidx * K;
-            const int len = min(K, a.steps - k0);
-            for (int j = len - 1; j >= 0; --j) {
-                const int k = k0 + j;
-                if (gfr) {
-                    gu += gf;
-                    if (k > 0) gf = __ldg(gfr + (int64_t)(k - 1) * TPR);
-                }
-                stages_bwd_split<TPR, 2>(a, cx, seg[3 * j * TPR + g], seg[(3 * j + 1) * TPR + g],
-                                         seg[(3 * j + 2) * TPR + g], gu, gs, sha, g, h, lane, warp);
-            }
-        }
-        __syncthreads();  // segment sidx - 1 replayed, segment sidx's half free
-    }
-    if (!rep && h == 0) {
-        a.g_u[base] = gu;
-        if (a.g_s) a.g_s[base] = gs;
-    }
-}
-
 // weno_reconstruction(f, direction) as a standalone op (solver_1d.py:4-42).
 template <int CPT, int TPR>
 __global__ void __launch_bounds__(256) k_weno(const float* __restrict__ f, float* __restrict__ out, int rows,
@@ -1385,16 +1146,6 @@ int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
     const int nseg = (b.steps + b.ckpt_every - 1) / b.ckpt_every;
     // several segments: the warp-specialised form overlaps each replay with the adjoint
     // before it (two thread groups; rows up to 256 cells keep 128 registers a thread)
-    if constexpr (TPR <= 128) {  // two threads per cell in the adjoint: 3 TPR threads
-        const size_t st3 = sizeof(SplitAdjSmem<TPR>) + sizeof(WideSmem<1, TPR>);
-        if (nseg >= 2 && 2 * smem + st3 <= 227 * 1024) {
-            if (2 * smem + st3 > 48 * 1024)
-                cudaFuncSetAttribute(k_rollout_bwd_wide3<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(2 * smem));
-            k_rollout_bwd_wide3<TPR><<<b.rows, 3 * TPR, 2 * smem, st>>>(b);
-            return check_launch("burgers_bwd_wide3");
-        }
-    }
     if constexpr (TPR <= 256) {
         if (nseg >= 2 && 2 * smem + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
             if (2 * smem + bwd_wide2_static_smem<TPR>() > 48 * 1024)
