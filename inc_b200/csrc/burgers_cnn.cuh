@@ -82,10 +82,10 @@ INC_DEV void put_cell(float* row, int g, float v) {
     if (g >= N - 2) row[apad(g - N + 2)] = v;
 }
 
-// Layer 1: one input channel -> channels 4 cg .. 4 cg + 3, GELU (or, with
-// GELU_OUT = false, the pre-activations).
-template <int N, bool GELU_OUT = true>
-INC_DEV void conv_first(const float* w, const float* in, float (*out)[row_len<N>()], int cg, int L) {
+// Layer 1, accumulation: acc[c][j] = pre-activation of channel 4 cg + c at cell
+// 8 L + j, from one input row.
+template <int N>
+INC_DEV void conv_first_acc(const float* w, const float* in, float (&acc)[4][8], int cg, int L) {
     float a[12];
     load12(a, in, L);
     const float4 b = lds4(w + OFF_B1 + 4 * cg);
@@ -97,25 +97,21 @@ INC_DEV void conv_first(const float* w, const float* in, float (*out)[row_len<N>
         wv[4 * i] = q.x; wv[4 * i + 1] = q.y; wv[4 * i + 2] = q.z; wv[4 * i + 3] = q.w;
     }
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        float o[8];
+    for (int c = 0; c < 4; ++c)
 #pragma unroll
         for (int j = 0; j < 8; ++j) {
-            float acc = bias[c];
+            float acc1 = bias[c];
 #pragma unroll
-            for (int k = 0; k < KW; ++k) acc = fmaf(wv[c * KW + k], a[j + k], acc);
-            o[j] = GELU_OUT ? gelu(acc) : acc;
+            for (int k = 0; k < KW; ++k) acc1 = fmaf(wv[c * KW + k], a[j + k], acc1);
+            acc[c][j] = acc1;
         }
-        store8<N>(out[4 * cg + c], L, o);
-    }
 }
 
-// Layers 2 and 3: 32 -> channels 4 cg .. 4 cg + 3, GELU (or the
-// pre-activations).  wt is [ci][co][k].
-template <int N, bool GELU_OUT = true>
-INC_DEV void conv_mid(const float* wt, const float* bias_p, float (*in)[row_len<N>()],
-                      float (*out)[row_len<N>()], int cg, int L) {
-    float acc[4][8];
+// Layers 2 and 3, accumulation: acc[c][j] = pre-activation of channel 4 cg + c
+// at cell 8 L + j.  wt is [ci][co][k].
+template <int N>
+INC_DEV void conv_mid_acc(const float* wt, const float* bias_p, float (*in)[row_len<N>()], float (&acc)[4][8],
+                          int cg, int L) {
     {
         const float4 b = lds4(bias_p + 4 * cg);
         const float bias[4] = {b.x, b.y, b.z, b.w};
@@ -141,6 +137,11 @@ INC_DEV void conv_mid(const float* wt, const float* bias_p, float (*in)[row_len<
 #pragma unroll
                 for (int j = 0; j < 8; ++j) acc[c][j] = fmaf(wv[c * KW + k], a[j + k], acc[c][j]);
     }
+}
+
+// a 4-channel x 8-cell tile into rows 4 cg .. 4 cg + 3 of `out` (GELU applied or not)
+template <int N, bool GELU_OUT>
+INC_DEV void store_tile(float (*out)[row_len<N>()], const float (&acc)[4][8], int cg, int L) {
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         float o[8];
@@ -148,6 +149,25 @@ INC_DEV void conv_mid(const float* wt, const float* bias_p, float (*in)[row_len<
         for (int j = 0; j < 8; ++j) o[j] = GELU_OUT ? gelu(acc[c][j]) : acc[c][j];
         store8<N>(out[4 * cg + c], L, o);
     }
+}
+
+// Layer 1: one input channel -> channels 4 cg .. 4 cg + 3, GELU (or, with
+// GELU_OUT = false, the pre-activations).
+template <int N, bool GELU_OUT = true>
+INC_DEV void conv_first(const float* w, const float* in, float (*out)[row_len<N>()], int cg, int L) {
+    float acc[4][8];
+    conv_first_acc<N>(w, in, acc, cg, L);
+    store_tile<N, GELU_OUT>(out, acc, cg, L);
+}
+
+// Layers 2 and 3: 32 -> channels 4 cg .. 4 cg + 3, GELU (or the
+// pre-activations).
+template <int N, bool GELU_OUT = true>
+INC_DEV void conv_mid(const float* wt, const float* bias_p, float (*in)[row_len<N>()],
+                      float (*out)[row_len<N>()], int cg, int L) {
+    float acc[4][8];
+    conv_mid_acc<N>(wt, bias_p, in, acc, cg, L);
+    store_tile<N, GELU_OUT>(out, acc, cg, L);
 }
 
 // Layer 4: channels 4 cg .. 4 cg + 3 -> partial sums of the single output

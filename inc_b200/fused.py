@@ -5,7 +5,7 @@
 u = solver.step(u); results[:, k] = u``) for a ``PeriodicCNN1D`` corrector in
 one launch of ``inc_burgers_cnn_rollout``: the four convolutions run from
 shared memory before every step, so no per-step corrector launches remain.
-With gradients on (rows of 256 cells), the rollout is one autograd node
+With gradients on (rows of 64, 128, 256 or 512 cells), the rollout is one autograd node
 whose backward is ``inc_burgers_cnn_rollout_bwd``: segment replay from
 checkpoints, the network's activations recomputed in shared memory, the
 solver's adjoint and the network's backward in one kernel, weight gradients
@@ -62,13 +62,19 @@ def pack_cnn_weights(model, device=None) -> torch.Tensor:
     return out
 
 
-CNN_TRAIN_N = 256
+CNN_TRAIN_N = CNN_N
 MAX_CKPT_EVERY = 32
+
+
+def max_ckpt_every(n: int) -> int:
+    """Largest segment length of the fused backward at row width n (its segment
+    states share the SM's 227 KB of shared memory with the activations)."""
+    return 26 if n == 512 else MAX_CKPT_EVERY
 
 
 def cnn_train_supported(model, solver, u) -> bool:
     """True when the fused training kernel (forward + backward) covers this case."""
-    return cnn_supported(model, solver, u) and u.shape[1] == CNN_TRAIN_N
+    return cnn_supported(model, solver, u) and u.shape[1] in CNN_TRAIN_N
 
 
 def unpack_cnn_grads(g: torch.Tensor):
@@ -135,7 +141,7 @@ def burgers_cnn_rollout(model, solver, u0, steps, corrections=True, ckpt_every=8
 
     With gradients enabled (and u0 or the model's parameters requiring them) the
     result is differentiable through the fused backward, which replays
-    ckpt_every-step segments (n = 256).  Advances ``solver.t`` by steps * dt and
+    ckpt_every-step segments (n = 64, 128, 256 or 512).  Advances ``solver.t`` by steps * dt and
     leaves the last correction in ``solver.correction_s``, like the per-step loop."""
     if not cnn_supported(model, solver, u0):
         raise ValueError("burgers_cnn_rollout: needs a PeriodicCNN1D(32, 5, 4) corrector, a fixed-dt "
@@ -144,11 +150,10 @@ def burgers_cnn_rollout(model, solver, u0, steps, corrections=True, ckpt_every=8
     params = [p for c in model.convs for p in (c.weight, c.bias)]
     want = torch.is_grad_enabled() and (u0.requires_grad or any(p.requires_grad for p in params))
     if want and steps > 0:
-        if u0.shape[1] != CNN_TRAIN_N:
-            raise ValueError(f"burgers_cnn_rollout: gradients need rows of {CNN_TRAIN_N} cells")
-        k = int(ckpt_every)
-        if not 1 <= k <= MAX_CKPT_EVERY:
-            raise ValueError(f"burgers_cnn_rollout: ckpt_every must be in [1, {MAX_CKPT_EVERY}]")
+        k, kmax = int(ckpt_every), max_ckpt_every(u0.shape[1])
+        if not 1 <= k <= kmax:
+            raise ValueError(f"burgers_cnn_rollout: ckpt_every must be in [1, {kmax}] for rows of "
+                             f"{u0.shape[1]} cells")
         u0c = u0.contiguous()
         launch = solver.launch_for(u0c)
         frames, corr = BurgersCNNRolloutFn.apply(u0c, launch, steps, k, *params)

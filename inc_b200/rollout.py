@@ -138,7 +138,7 @@ def simulate_rollout(model, solver, u_initial, mstep, correction_term, L=None, c
                 return fused.burgers_cnn_rollout(model, solver, u_initial, mstep)
         elif fused.cnn_train_supported(model, solver, u_initial):  # training: fused forward and backward
             k = int(checkpoint_every or 8)
-            if 1 <= k <= fused.MAX_CKPT_EVERY:
+            if 1 <= k <= fused.max_ckpt_every(u_initial.shape[1]):
                 return fused.burgers_cnn_rollout(model, solver, u_initial, mstep, ckpt_every=k)
 
     model_fn = (lambda u: model(u)) if L is None else (lambda u: model(u, L))

@@ -247,9 +247,10 @@ int inc_burgers_cnn_rollout(const inc_burgers_desc* d, const float* weights,
  * frames and corrections (either may be NULL), it replays each k-step segment,
  * recomputes the network's activations and returns dL/du0 (g_u0 [rows][n]) and
  * dL/dweights (g_weights, INC_CNN_WEIGHT_FLOATS floats in the packed layout).
- * work: rows * INC_CNN_WEIGHT_FLOATS floats of device scratch (per-row weight
- * gradients, summed in a fixed order, so results are deterministic).
- * n = 256 only (else INC_E_UNSUPPORTED); ckpt_every <= 32.                   */
+ * work: rows * INC_CNN_WEIGHT_FLOATS floats of device scratch (the weight
+ * gradients of each CTA's rows, summed in a fixed order, so results are
+ * deterministic).  n: 64, 128, 256 or 512 (else INC_E_UNSUPPORTED);
+ * ckpt_every <= 32, and <= 26 at n = 512 (else INC_E_INVALID).               */
 int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const float* weights,
                                 const float* ckpts, const float* corrections,
                                 const float* t_rows, double t0, int32_t steps,

@@ -163,14 +163,21 @@ def test_fused_matches_per_step_gpu_loop_and_dispatch(cuda):
     assert torch.equal(s1.correction_s, c1[:, -1])
 
 
-@pytest.mark.parametrize("scheme,K,eq", [("ssprk3", 8, "viscosity"), ("ssprk3", 5, "learning"),
-                                         ("euler", 1, "linear"), ("ssprk3", 32, "viscosity")])
-def test_fused_training_gradients_vs_per_step_loop(cuda, scheme, K, eq):
+@pytest.mark.parametrize("N,B,scheme,K,eq", [
+    (256, 5, "ssprk3", 8, "viscosity"), (256, 5, "ssprk3", 5, "learning"), (256, 5, "euler", 1, "linear"),
+    (256, 5, "ssprk3", 32, "viscosity"),
+    # four rows per CTA at n = 64 and two at n = 128: batches that leave the last CTA partly empty
+    (64, 9, "ssprk3", 8, "viscosity"), (64, 6, "euler", 1, "linear"), (128, 5, "ssprk3", 5, "learning"),
+    (128, 4, "ssprk3", 13, "viscosity"),
+    # one CTA of 512 threads per row; 26 is the longest segment that fits beside the activations
+    (512, 3, "ssprk3", 8, "viscosity"), (512, 2, "ssprk3", 26, "learning")])
+def test_fused_training_gradients_vs_per_step_loop(cuda, N, B, scheme, K, eq):
     """Gradients of a loss on frames and corrections w.r.t. u0 and every network parameter:
-    fused backward (segment replay, recomputed activations) vs torch autograd through the loop."""
+    fused backward (segment replay, recomputed activations) vs torch autograd through the loop,
+    at every supported row width."""
     from inc_b200.fused import burgers_cnn_rollout
     from inc_b200.solvers import BurgersSolverTorch
-    N, B, steps = 256, 5, 13
+    steps = 13 if K <= 13 else K + 3
     p = _params(N, eq=eq, B=B, seed=6)
     u0_np = _u0(B, N, seed=7)
     gen = torch.Generator().manual_seed(3)
@@ -277,11 +284,11 @@ def test_fused_rejects_unsupported(cuda):
     assert not cnn_supported(net, solver, u)
     with pytest.raises(ValueError):
         burgers_cnn_rollout(net, solver, u, 4)
-    p128 = _params(128)
-    s128 = BurgersSolverTorch(_sim_params(p128, 2, "euler", cuda))
-    u128 = torch.tensor(_u0(2, 128, 2), dtype=torch.float32, device=cuda)
-    with pytest.raises(ValueError):  # gradients are built for rows of 256 cells
-        burgers_cnn_rollout(net, s128, u128, 4)
+    p512 = _params(512)
+    s512 = BurgersSolverTorch(_sim_params(p512, 2, "euler", cuda))
+    u512 = torch.tensor(_u0(2, 512, 2), dtype=torch.float32, device=cuda, requires_grad=True)
+    with pytest.raises(ValueError):  # at n = 512 a segment of 27 states does not fit in shared memory
+        burgers_cnn_rollout(net, s512, u512, 30, ckpt_every=27)
     small = PeriodicCNN1D(channels=16).to(cuda)
     p = _params(64)
     solver = BurgersSolverTorch(_sim_params(p, 2, "euler", cuda))
@@ -292,12 +299,13 @@ def test_fused_rejects_unsupported(cuda):
     assert f.shape == (2, 3, 64) and c.shape == (2, 3, 64)
 
 
-def test_fused_training_gradients_are_deterministic(cuda):
+@pytest.mark.parametrize("N,B", [(256, 7), (64, 7)])
+def test_fused_training_gradients_are_deterministic(cuda, N, B):
     """Two runs of the fused backward give bit-identical gradients: every weight-gradient
-    sum (across the warps of a row, then across rows) is taken in a fixed order."""
+    sum (across the steps and warps of a CTA, then across CTAs) is taken in a fixed order."""
     from inc_b200.fused import burgers_cnn_rollout
     from inc_b200.solvers import BurgersSolverTorch
-    N, B, steps = 256, 7, 9
+    steps = 9
     p = _params(N, B=B, seed=11)
     u0_np = _u0(B, N, seed=12)
 
