@@ -55,14 +55,13 @@ class RaggedBurgers:
         self.grid_blocks = int(grid_blocks) or self.default_grid()
 
     def default_grid(self) -> int:
-        """Blocks of the persistent launch: about (total cells / widest row) warps, so that a
-        warp's share of the work is about one widest row and the longest-first queue can even
-        out the tail, within 2 to 4 blocks of 4 warps per SM (more warps than that leave the
-        widest rows as the tail; fewer hide less latency)."""
+        """Blocks of the persistent launch: as many as are resident at once.  The kernel
+        keeps up to 255 registers a thread (a row of 512 cells holds 16 cells, their
+        increments, compensation and fluxes per lane), so an SM holds eight of its warps;
+        a larger grid only adds blocks that start once the queue is empty."""
         sms = torch.cuda.get_device_properties(self.device).multi_processor_count
         wpb = self.desc.warps_per_block or 4
-        blocks = int(round(self.total / max(self.ns) / wpb))
-        return max(2 * sms, min(4 * sms, blocks))
+        return sms * max(1, 8 // wpb)
 
     def rollout(self, steps, u0=None, out=None):
         """All rows advanced `steps` steps; returns the packed final state."""

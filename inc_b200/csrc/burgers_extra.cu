@@ -72,7 +72,10 @@ INC_DEV void ragged_dispatch(const RaggedArgs& ra, int n, int row, int lane) {
     }
 }
 
-__global__ void __launch_bounds__(256) k_ragged(RaggedArgs ra) {
+// Registers uncapped (up to 255 a thread: two blocks of four warps per SM): the rows
+// of 512 cells keep 16 cells, their compensation, increments and interface fluxes
+// per lane in registers.
+__global__ void __launch_bounds__(256, 1) k_ragged(RaggedArgs ra) {
     const int lane = threadIdx.x & 31;
     for (;;) {
         int item = 0;

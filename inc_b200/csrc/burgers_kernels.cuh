@@ -265,7 +265,7 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
         for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
         const float alpha = group_max_nonneg<TPR>(m);  // per-row max |u|, solver_1d.py:133
         const float nu_dx2 = nu * inv_dx2;
-        if constexpr (CPT <= 8) {
+        if constexpr (CPT <= 8 || PK) {
             float hs[CPT];
             weno_right_fluxes<CPT, PK>(w, alpha, hs);
             float prev = shfl<TPR>(hs[CPT - 1], left);
@@ -276,10 +276,11 @@ INC_DEV void rhs_core(const float (&u)[CPT], float (&r)[CPT], int conv, float nu
                 prev = hs[c];
             }
         } else {
-            // At 16 cells per lane the handover saves 1/17 of the reconstructions; the
-            // left interface is reconstructed here and the fluxes are consumed as they
-            // are made (two live values, for the register-bound backward and adaptive
-            // kernels).
+            // 16 cells per lane in the register-bound backward and adaptive kernels:
+            // the left interface is reconstructed here (one reconstruction in 17 more
+            // than the handover) and the fluxes are consumed as they are made (two live
+            // values).  The ragged forward (PK) keeps the handover at 16 cells too: with
+            // its registers uncapped that made its rows of 512 cells 9% faster.
             const float ha = 0.5f * alpha;
             float fp[CPT + 6], fm[CPT + 6];
 #pragma unroll
