@@ -60,14 +60,17 @@ INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& 
     w.qg1 = fmaf(-0.1f, g1, fmaf(0.5f, g2, 0.2f * g3));
     w.qg2 = fmaf(0.1f, g2, fmaf(0.25f, g3, -0.05f * g4));
     w.d0 = fmaf(-2.f, g1, g0) + g2;
-    w.e0 = fmaf(-4.f, g1, g0) + 3.f * g2;
+    w.e0 = fmaf(3.f, g2, fmaf(-4.f, g1, g0));
     w.d1 = fmaf(-2.f, g2, g1) + g3;
-    w.e1 = g1 - g3;
+    w.e1 = fmaf(-1.f, g3, g1);
     w.d2 = fmaf(-2.f, g3, g2) + g4;
-    w.e2 = RIGHT ? (fmaf(-4.f, g3, g2) + 3.f * g4) : (fmaf(-4.f, g3, 3.f * g2) + g4);
-    w.s0 = kEpsScaled + fmaf(w.d0, w.d0, (3.f / 13.f) * w.e0 * w.e0);
-    w.s1 = kEpsScaled + fmaf(w.d1, w.d1, (3.f / 13.f) * w.e1 * w.e1);
-    w.s2 = kEpsScaled + fmaf(w.d2, w.d2, (3.f / 13.f) * w.e2 * w.e2);
+    // left (3, -4, 1), right (1, -4, 3) on (g2, g3, g4); -4 g3 is exact, so these are
+    // weno5_pair's values lane for lane
+    w.e2 = RIGHT ? fmaf(3.f, g4, fmaf(-4.f, g3, g2)) : fmaf(3.f, g2, -4.f * g3) + g4;
+    // s'_k = eps' + d^2 + (3/13) e^2 (beta_k scaled by 12/13), eps folded into the FMA chain
+    w.s0 = fmaf(w.d0, w.d0, fmaf((3.f / 13.f) * w.e0, w.e0, kEpsScaled));
+    w.s1 = fmaf(w.d1, w.d1, fmaf((3.f / 13.f) * w.e1, w.e1, kEpsScaled));
+    w.s2 = fmaf(w.d2, w.d2, fmaf((3.f / 13.f) * w.e2, w.e2, kEpsScaled));
     w.r0 = rcp_approx(w.s0 * w.s0);
     w.r1 = rcp_approx(w.s1 * w.s1);
     w.r2 = rcp_approx(w.s2 * w.s2);
@@ -96,16 +99,16 @@ INC_DEV float weno5_pair(float g0, float g1, float g2, float g3, float g4, float
     const float2 qg1 = __ffma2_rn(f2s(-0.1f), G1, __ffma2_rn(f2s(0.5f), G2, __fmul2_rn(f2s(0.2f), G3)));
     const float2 qg2 = __ffma2_rn(f2s(0.1f), G2, __ffma2_rn(f2s(0.25f), G3, __fmul2_rn(f2s(-0.05f), G4)));
     const float2 d0 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G1, G0), G2);
-    const float2 e0 = __fadd2_rn(__ffma2_rn(f2s(-4.f), G1, G0), __fmul2_rn(f2s(3.f), G2));
+    const float2 e0 = __ffma2_rn(f2s(3.f), G2, __ffma2_rn(f2s(-4.f), G1, G0));
     const float2 d1 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G2, G1), G3);
-    const float2 e1 = __fadd2_rn(G1, __fmul2_rn(f2s(-1.f), G3));
+    const float2 e1 = __ffma2_rn(f2s(-1.f), G3, G1);
     const float2 d2 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G3, G2), G4);
-    // left: (-4 g3 + 3 g2) + g4; right: (-4 g3 + g2) + 3 g4
-    const float2 e2 = __fadd2_rn(__ffma2_rn(f2s(-4.f), G3, __fmul2_rn(f2(3.f, 1.f), G2)), __fmul2_rn(f2(1.f, 3.f), G4));
+    // left: fma(1, g4, fma(3, g2, -4 g3)); right: fma(3, g4, fma(1, g2, -4 g3)) (weno5_eval's values)
+    const float2 e2 = __ffma2_rn(f2(1.f, 3.f), G4, __ffma2_rn(f2(3.f, 1.f), G2, __fmul2_rn(f2s(-4.f), G3)));
     const float2 c313 = f2s(3.f / 13.f), eps = f2s(kEpsScaled);
-    const float2 s0 = __fadd2_rn(eps, __ffma2_rn(d0, d0, __fmul2_rn(__fmul2_rn(c313, e0), e0)));
-    const float2 s1 = __fadd2_rn(eps, __ffma2_rn(d1, d1, __fmul2_rn(__fmul2_rn(c313, e1), e1)));
-    const float2 s2 = __fadd2_rn(eps, __ffma2_rn(d2, d2, __fmul2_rn(__fmul2_rn(c313, e2), e2)));
+    const float2 s0 = __ffma2_rn(d0, d0, __ffma2_rn(__fmul2_rn(c313, e0), e0, eps));
+    const float2 s1 = __ffma2_rn(d1, d1, __ffma2_rn(__fmul2_rn(c313, e1), e1, eps));
+    const float2 s2 = __ffma2_rn(d2, d2, __ffma2_rn(__fmul2_rn(c313, e2), e2, eps));
     const float2 q0 = __fmul2_rn(s0, s0), q1 = __fmul2_rn(s1, s1), q2 = __fmul2_rn(s2, s2);
     const float2 r0 = f2(rcp_approx(q0.x), rcp_approx(q0.y)), r1 = f2(rcp_approx(q1.x), rcp_approx(q1.y)),
                  r2 = f2(rcp_approx(q2.x), rcp_approx(q2.y));
