@@ -87,24 +87,31 @@ INC_DEV float weno5(float g0, float g1, float g2, float g3, float g4) {
 
 // weno5<false>(g0..g4) + weno5<true>(h0..h4), the two reconstructions of one
 // interface evaluated together in the two lanes of Blackwell's packed FP32 pairs
-// (fma/add/mul.f32x2: half the issue slots; the reciprocals stay scalar).  Same
-// operations per lane as weno5_eval, so the same values.
+// (fma/add/mul.f32x2: half the issue slots; the reciprocals stay scalar), in the
+// first differences D_j = g_{j+1} - g_j: the candidates as q_k = g2 + dq_k (the
+// weights sum to one, so h = g2 + sum w_k dq_k), the smoothness indicators from
+// d_k, e_k of the D's (e_k enters squared, so its sign is free).  36 packed
+// operations per interface where weno5_eval's form takes 40; the same
+// reconstruction up to FP32 rounding (weno5_eval keeps the form its adjoint,
+// weno5_vjp, differentiates).
 INC_DEV float2 f2(float a, float b) { return make_float2(a, b); }
 INC_DEV float2 f2s(float a) { return make_float2(a, a); }
+INC_DEV float2 sub2(float2 a, float2 b) { return __ffma2_rn(f2s(-1.f), b, a); }  // a - b, exactly rounded
 INC_DEV float weno5_pair(float g0, float g1, float g2, float g3, float g4, float h0, float h1, float h2, float h3,
                          float h4) {
     const float2 G0 = f2(g0, h0), G1 = f2(g1, h1), G2 = f2(g2, h2), G3 = f2(g3, h3), G4 = f2(g4, h4);
-    const float2 qg0 = __ffma2_rn(f2s(0.0333333333f), G0, __ffma2_rn(f2s(-0.1166666667f), G1,
-                                                                      __fmul2_rn(f2s(0.1833333333f), G2)));
-    const float2 qg1 = __ffma2_rn(f2s(-0.1f), G1, __ffma2_rn(f2s(0.5f), G2, __fmul2_rn(f2s(0.2f), G3)));
-    const float2 qg2 = __ffma2_rn(f2s(0.1f), G2, __ffma2_rn(f2s(0.25f), G3, __fmul2_rn(f2s(-0.05f), G4)));
-    const float2 d0 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G1, G0), G2);
-    const float2 e0 = __ffma2_rn(f2s(3.f), G2, __ffma2_rn(f2s(-4.f), G1, G0));
-    const float2 d1 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G2, G1), G3);
-    const float2 e1 = __ffma2_rn(f2s(-1.f), G3, G1);
-    const float2 d2 = __fadd2_rn(__ffma2_rn(f2s(-2.f), G3, G2), G4);
-    // left: fma(1, g4, fma(3, g2, -4 g3)); right: fma(3, g4, fma(1, g2, -4 g3)) (weno5_eval's values)
-    const float2 e2 = __ffma2_rn(f2(1.f, 3.f), G4, __ffma2_rn(f2(3.f, 1.f), G2, __fmul2_rn(f2s(-4.f), G3)));
+    const float2 D0 = sub2(G1, G0), D1 = sub2(G2, G1), D2 = sub2(G3, G2), D3 = sub2(G4, G3);
+    // gamma_k (q_k - g2): gamma = (0.1, 0.6, 0.3); q0 - g2 = -D0/3 + 5 D1/6,
+    // q1 - g2 = D1/6 + D2/3, q2 - g2 = 2 D2/3 - D3/6
+    const float2 qg0 = __ffma2_rn(f2s(-1.f / 30.f), D0, __fmul2_rn(f2s(1.f / 12.f), D1));
+    const float2 qg1 = __ffma2_rn(f2s(0.1f), D1, __fmul2_rn(f2s(0.2f), D2));
+    const float2 qg2 = __ffma2_rn(f2s(0.2f), D2, __fmul2_rn(f2s(-0.05f), D3));
+    // d_k = second differences; e0 = -(g0 - 4 g1 + 3 g2), e1 = -(g1 - g3); e2: left
+    // 3 g2 - 4 g3 + g4 = D3 - 3 D2, right -(g2 - 4 g3 + 3 g4) = D2 - 3 D3
+    const float2 d0 = sub2(D1, D0), d1 = sub2(D2, D1), d2 = sub2(D3, D2);
+    const float2 e0 = __ffma2_rn(f2s(-3.f), D1, D0);
+    const float2 e1 = __fadd2_rn(D1, D2);
+    const float2 e2 = __ffma2_rn(f2(-3.f, 1.f), D2, __fmul2_rn(f2(1.f, -3.f), D3));
     const float2 c313 = f2s(3.f / 13.f), eps = f2s(kEpsScaled);
     const float2 s0 = __ffma2_rn(d0, d0, __ffma2_rn(__fmul2_rn(c313, e0), e0, eps));
     const float2 s1 = __ffma2_rn(d1, d1, __ffma2_rn(__fmul2_rn(c313, e1), e1, eps));
@@ -114,7 +121,7 @@ INC_DEV float weno5_pair(float g0, float g1, float g2, float g3, float g4, float
                  r2 = f2(rcp_approx(q2.x), rcp_approx(q2.y));
     const float2 den = __ffma2_rn(f2s(0.1f), r0, __ffma2_rn(f2s(0.6f), r1, __fmul2_rn(f2s(0.3f), r2)));
     const float2 inv = f2(rcp_approx(den.x), rcp_approx(den.y));
-    const float2 h = __fmul2_rn(__ffma2_rn(qg0, r0, __ffma2_rn(qg1, r1, __fmul2_rn(qg2, r2))), inv);
+    const float2 h = __ffma2_rn(__ffma2_rn(qg0, r0, __ffma2_rn(qg1, r1, __fmul2_rn(qg2, r2))), inv, G2);
     return h.x + h.y;
 }
 
