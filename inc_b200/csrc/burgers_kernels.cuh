@@ -78,22 +78,39 @@ INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& 
     w.h = fmaf(w.qg0, w.r0, fmaf(w.qg1, w.r1, w.qg2 * w.r2)) * w.inv_den;
 }
 
+// The reconstruction alone (the forward kernels), in the first differences
+// D_j = g_{j+1} - g_j: the candidates as q_k = g2 + dq_k (the weights sum to one,
+// so h = g2 + sum w_k dq_k), the smoothness indicators from d_k, e_k of the D's
+// (e_k enters squared, so its sign is free).  Fewer and shorter dependent
+// operations than weno5_eval's form, which the adjoint (weno5_vjp) keeps; the two
+// agree up to FP32 rounding.
 template <bool RIGHT>
 INC_DEV float weno5(float g0, float g1, float g2, float g3, float g4) {
-    Weno w;
-    weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
-    return w.h;
+    const float D0 = g1 - g0, D1 = g2 - g1, D2 = g3 - g2, D3 = g4 - g3;
+    // gamma_k (q_k - g2): gamma = (0.1, 0.6, 0.3); q0 - g2 = -D0/3 + 5 D1/6,
+    // q1 - g2 = D1/6 + D2/3, q2 - g2 = 2 D2/3 - D3/6
+    const float qg0 = fmaf(-1.f / 30.f, D0, (1.f / 12.f) * D1);
+    const float qg1 = fmaf(0.1f, D1, 0.2f * D2);
+    const float qg2 = fmaf(0.2f, D2, -0.05f * D3);
+    // d_k = second differences; e0 = -(g0 - 4 g1 + 3 g2), e1 = -(g1 - g3); e2: left
+    // 3 g2 - 4 g3 + g4 = D3 - 3 D2, right -(g2 - 4 g3 + 3 g4) = D2 - 3 D3
+    const float d0 = D1 - D0, d1 = D2 - D1, d2 = D3 - D2;
+    const float e0 = fmaf(-3.f, D1, D0);
+    const float e1 = D1 + D2;
+    const float e2 = RIGHT ? fmaf(1.f, D2, -3.f * D3) : fmaf(-3.f, D2, D3);
+    const float s0 = fmaf(d0, d0, fmaf((3.f / 13.f) * e0, e0, kEpsScaled));
+    const float s1 = fmaf(d1, d1, fmaf((3.f / 13.f) * e1, e1, kEpsScaled));
+    const float s2 = fmaf(d2, d2, fmaf((3.f / 13.f) * e2, e2, kEpsScaled));
+    const float r0 = rcp_approx(s0 * s0), r1 = rcp_approx(s1 * s1), r2 = rcp_approx(s2 * s2);
+    const float inv = rcp_approx(fmaf(0.1f, r0, fmaf(0.6f, r1, 0.3f * r2)));
+    return fmaf(fmaf(qg0, r0, fmaf(qg1, r1, qg2 * r2)), inv, g2);
 }
 
 // weno5<false>(g0..g4) + weno5<true>(h0..h4), the two reconstructions of one
 // interface evaluated together in the two lanes of Blackwell's packed FP32 pairs
-// (fma/add/mul.f32x2: half the issue slots; the reciprocals stay scalar), in the
-// first differences D_j = g_{j+1} - g_j: the candidates as q_k = g2 + dq_k (the
-// weights sum to one, so h = g2 + sum w_k dq_k), the smoothness indicators from
-// d_k, e_k of the D's (e_k enters squared, so its sign is free).  36 packed
-// operations per interface where weno5_eval's form takes 40; the same
-// reconstruction up to FP32 rounding (weno5_eval keeps the form its adjoint,
-// weno5_vjp, differentiates).
+// (fma/add/mul.f32x2: half the issue slots; the reciprocals stay scalar): 36
+// packed operations per interface.  Same operations per lane as weno5, so the
+// same values.
 INC_DEV float2 f2(float a, float b) { return make_float2(a, b); }
 INC_DEV float2 f2s(float a) { return make_float2(a, a); }
 INC_DEV float2 sub2(float2 a, float2 b) { return __ffma2_rn(f2s(-1.f), b, a); }  // a - b, exactly rounded
