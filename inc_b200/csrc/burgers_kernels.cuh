@@ -32,13 +32,14 @@ constexpr float kEps = 1e-6f;  // solver_1d.py:5
 //   beta'_k = (12/13) beta_k = d_k^2 + (3/13) e_k^2,
 //   s'_k    = (12/13) (eps + beta_k) = (12/13) eps + beta'_k,
 //   r_k     = 1 / s'_k^2  (= (13/12)^2 / (eps + beta_k)^2),
-//   h       = sum_k (gamma_k q_k) r_k / sum_k gamma_k r_k,
-// with gamma_k folded into the candidate polynomials' coefficients (qg_k).
+//   h       = g2 + sum_k (gamma_k dq_k) r_k / sum_k gamma_k r_k,  dq_k = q_k - g2
+// (the weights sum to one), with gamma_k folded into the candidates' coefficients
+// (qg_k) and everything formed from the first differences D_j = g_{j+1} - g_j.
 struct Weno {
-    float qg0, qg1, qg2;  // gamma_k q_k
+    float qg0, qg1, qg2;  // gamma_k (q_k - g2)
     float s0, s1, s2;     // s'_k
     float r0, r1, r2;     // 1 / s'_k^2
-    float inv_den, h;
+    float inv_den, dh;    // dh = h - g2
     float d0, e0, d1, e1, d2, e2;
 };
 
@@ -55,18 +56,20 @@ INC_DEV float rcp_approx(float x) {
 
 template <bool RIGHT>
 INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& w) {
-    // gamma = (0.1, 0.6, 0.3) times q0 = (1/3, -7/6, 11/6), q1 = (-1/6, 5/6, 1/3), q2 = (1/3, 5/6, -1/6)
-    w.qg0 = fmaf(0.0333333333f, g0, fmaf(-0.1166666667f, g1, 0.1833333333f * g2));
-    w.qg1 = fmaf(-0.1f, g1, fmaf(0.5f, g2, 0.2f * g3));
-    w.qg2 = fmaf(0.1f, g2, fmaf(0.25f, g3, -0.05f * g4));
-    w.d0 = fmaf(-2.f, g1, g0) + g2;
-    w.e0 = fmaf(3.f, g2, fmaf(-4.f, g1, g0));
-    w.d1 = fmaf(-2.f, g2, g1) + g3;
-    w.e1 = fmaf(-1.f, g3, g1);
-    w.d2 = fmaf(-2.f, g3, g2) + g4;
-    // left (3, -4, 1), right (1, -4, 3) on (g2, g3, g4); -4 g3 is exact, so these are
-    // weno5_pair's values lane for lane
-    w.e2 = RIGHT ? fmaf(3.f, g4, fmaf(-4.f, g3, g2)) : fmaf(3.f, g2, -4.f * g3) + g4;
+    const float D0 = g1 - g0, D1 = g2 - g1, D2 = g3 - g2, D3 = g4 - g3;
+    // gamma = (0.1, 0.6, 0.3); q0 - g2 = -D0/3 + 5 D1/6, q1 - g2 = D1/6 + D2/3,
+    // q2 - g2 = 2 D2/3 - D3/6
+    w.qg0 = fmaf(-1.f / 30.f, D0, (1.f / 12.f) * D1);
+    w.qg1 = fmaf(0.1f, D1, 0.2f * D2);
+    w.qg2 = fmaf(0.2f, D2, -0.05f * D3);
+    w.d0 = D1 - D0;
+    w.d1 = D2 - D1;
+    w.d2 = D3 - D2;
+    // e0 = g0 - 4 g1 + 3 g2, e1 = g1 - g3, e2 = 3 g2 - 4 g3 + g4 (left) or
+    // g2 - 4 g3 + 3 g4 (right), with their signs (the adjoint differentiates them)
+    w.e0 = fmaf(3.f, D1, -D0);
+    w.e1 = -D1 - D2;
+    w.e2 = RIGHT ? fmaf(3.f, D3, -D2) : fmaf(-3.f, D2, D3);
     // s'_k = eps' + d^2 + (3/13) e^2 (beta_k scaled by 12/13), eps folded into the FMA chain
     w.s0 = fmaf(w.d0, w.d0, fmaf((3.f / 13.f) * w.e0, w.e0, kEpsScaled));
     w.s1 = fmaf(w.d1, w.d1, fmaf((3.f / 13.f) * w.e1, w.e1, kEpsScaled));
@@ -75,15 +78,15 @@ INC_DEV void weno5_eval(float g0, float g1, float g2, float g3, float g4, Weno& 
     w.r1 = rcp_approx(w.s1 * w.s1);
     w.r2 = rcp_approx(w.s2 * w.s2);
     w.inv_den = rcp_approx(fmaf(0.1f, w.r0, fmaf(0.6f, w.r1, 0.3f * w.r2)));
-    w.h = fmaf(w.qg0, w.r0, fmaf(w.qg1, w.r1, w.qg2 * w.r2)) * w.inv_den;
+    w.dh = fmaf(w.qg0, w.r0, fmaf(w.qg1, w.r1, w.qg2 * w.r2)) * w.inv_den;
 }
 
 // The reconstruction alone (the forward kernels), in the first differences
 // D_j = g_{j+1} - g_j: the candidates as q_k = g2 + dq_k (the weights sum to one,
 // so h = g2 + sum w_k dq_k), the smoothness indicators from d_k, e_k of the D's
-// (e_k enters squared, so its sign is free).  Fewer and shorter dependent
-// operations than weno5_eval's form, which the adjoint (weno5_vjp) keeps; the two
-// agree up to FP32 rounding.
+// (e_k enters squared, so its sign is free).  weno5_eval forms the same
+// quantities for the adjoint (weno5_vjp) and keeps them; the two agree up to
+// FP32 rounding.
 template <bool RIGHT>
 INC_DEV float weno5(float g0, float g1, float g2, float g3, float g4) {
     const float D0 = g1 - g0, D1 = g2 - g1, D2 = g3 - g2, D3 = g4 - g3;
@@ -150,12 +153,13 @@ INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float h
     Weno w;
     weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
     const float w0 = 0.1f * w.r0 * w.inv_den, w1 = 0.6f * w.r1 * w.inv_den, w2 = 0.3f * w.r2 * w.inv_den;
+    // q_k - h = dq_k - dh
     const float q0 = 10.f * w.qg0, q1 = w.qg1 * (1.f / 0.6f), q2 = w.qg2 * (1.f / 0.3f);
     const float qb0 = hb * w0, qb1 = hb * w1, qb2 = hb * w2;
     // 1 / (eps + beta_k) = (12/13) / s'_k
-    const float bb0 = (-24.f / 13.f) * qb0 * (q0 - w.h) * rcp_approx(w.s0);
-    const float bb1 = (-24.f / 13.f) * qb1 * (q1 - w.h) * rcp_approx(w.s1);
-    const float bb2 = (-24.f / 13.f) * qb2 * (q2 - w.h) * rcp_approx(w.s2);
+    const float bb0 = (-24.f / 13.f) * qb0 * (q0 - w.dh) * rcp_approx(w.s0);
+    const float bb1 = (-24.f / 13.f) * qb1 * (q1 - w.dh) * rcp_approx(w.s1);
+    const float bb2 = (-24.f / 13.f) * qb2 * (q2 - w.dh) * rcp_approx(w.s2);
     // beta_k = 13/12 d^2 + 1/4 e^2  ->  dbeta = 13/6 d dd + 1/2 e de
     const float A0 = 13.f / 6.f * w.d0 * bb0, E0 = 0.5f * w.e0 * bb0;
     const float A1 = 13.f / 6.f * w.d1 * bb1, E1 = 0.5f * w.e1 * bb1;
