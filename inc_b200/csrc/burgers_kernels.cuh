@@ -13,6 +13,8 @@
 #pragma once
 #include <string.h>
 
+#include <cooperative_groups.h>
+
 #include "common.cuh"
 
 namespace inc {
@@ -145,13 +147,11 @@ INC_DEV float weno5_pair(float g0, float g1, float g2, float g3, float g4, float
     return h.x + h.y;
 }
 
-// Adds hb * d h / d g_m to acc[0..4] (the vector-Jacobian product of weno5).
+// Adds hb * d h / d g_m to acc[0..4] (the vector-Jacobian product of weno5), given
+// the reconstruction's quantities w (weno5_eval of the same g0..g4).
 // With w_k = alpha_k / S:  dh/dq_k = w_k,  dh/dbeta_k = -2 w_k (q_k - h) / (eps + beta_k).
 template <bool RIGHT>
-INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float hb,
-                       float& c0, float& c1, float& c2, float& c3, float& c4) {
-    Weno w;
-    weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
+INC_DEV void weno5_vjp_tail(const Weno& w, float hb, float& c0, float& c1, float& c2, float& c3, float& c4) {
     const float w0 = 0.1f * w.r0 * w.inv_den, w1 = 0.6f * w.r1 * w.inv_den, w2 = 0.3f * w.r2 * w.inv_den;
     // q_k - h = dq_k - dh
     const float q0 = 10.f * w.qg0, q1 = w.qg1 * (1.f / 0.6f), q2 = w.qg2 * (1.f / 0.3f);
@@ -176,6 +176,14 @@ INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float h
     c2 += (1.f / 3.f) * qb2 + A2 + (RIGHT ? 1.f : 3.f) * E2;
     c3 += (5.f / 6.f) * qb2 - 2.f * A2 - 4.f * E2;
     c4 += (-1.f / 6.f) * qb2 + A2 + (RIGHT ? 3.f : 1.f) * E2;
+}
+
+template <bool RIGHT>
+INC_DEV void weno5_vjp(float g0, float g1, float g2, float g3, float g4, float hb,
+                       float& c0, float& c1, float& c2, float& c3, float& c4) {
+    Weno w;
+    weno5_eval<RIGHT>(g0, g1, g2, g3, g4, w);
+    weno5_vjp_tail<RIGHT>(w, hb, c0, c1, c2, c3, c4);
 }
 
 // Lax-Friedrichs flux splitting of f = u^2 / 2 (solver_1d.py:134-137):
@@ -679,6 +687,7 @@ template <int CPT, int TPR>
 struct WideSmem {
     float row[2][CPT * TPR];
     float wmax[2][TPR / 32];
+    int warg[2][TPR / 32];  // (ARG) each warp's first cell of its max |u|
     float flux[2][TPR];  // each thread's last right-interface flux sum, read by its right neighbour
 };
 
@@ -692,18 +701,34 @@ INC_DEV void row_sync() {
     else asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(NT) : "memory");
 }
 
-template <int CPT, int TPR, int BAR = 0>
+// ARG: also the row's first cell of max |u| (as the adjoint picks it); thread 0
+// writes alpha and that cell (as int bits) to arg_out[0], arg_out[1] (WENO only).
+template <int CPT, int TPR, int BAR = 0, bool ARG = false>
 INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, float nu, float inv_dx, float inv_dx2,
-                           float inv_2dx, WideSmem<CPT, TPR>& sh, int parity, int g) {
+                           float inv_2dx, WideSmem<CPT, TPR>& sh, int parity, int g, float* arg_out = nullptr) {
     constexpr int N = CPT * TPR;
     float* row = sh.row[parity];
 #pragma unroll
     for (int c = 0; c < CPT; ++c) row[g * CPT + c] = u[c];
     float m = 0.f;
+    if constexpr (ARG) {  // as fmaxf: a NaN cell is passed over
+        int mi = g * CPT;
 #pragma unroll
-    for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
-    m = group_max_nonneg<32>(m);
-    if ((g & 31) == 0) sh.wmax[parity][g >> 5] = m;
+        for (int c = 0; c < CPT; ++c) {
+            const float av = fabsf(u[c]);
+            if (av > m) { m = av; mi = g * CPT + c; }
+        }
+        group_argmax_nonneg<32>(m, mi);
+        if ((g & 31) == 0) {
+            sh.wmax[parity][g >> 5] = m;
+            sh.warg[parity][g >> 5] = mi;
+        }
+    } else {
+#pragma unroll
+        for (int c = 0; c < CPT; ++c) m = fmaxf(m, fabsf(u[c]));
+        m = group_max_nonneg<32>(m);
+        if ((g & 31) == 0) sh.wmax[parity][g >> 5] = m;
+    }
     row_sync<BAR, TPR>();
     float w[CPT + 6];
 #pragma unroll
@@ -712,6 +737,20 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
         float alpha = 0.f;
 #pragma unroll
         for (int i = 0; i < TPR / 32; ++i) alpha = fmaxf(alpha, sh.wmax[parity][i]);
+        if constexpr (ARG) {
+            if (g == 0) {
+                float best = sh.wmax[parity][0];
+                int am = sh.warg[parity][0];
+#pragma unroll
+                for (int i = 1; i < TPR / 32; ++i)
+                    if (sh.wmax[parity][i] > best) {
+                        best = sh.wmax[parity][i];
+                        am = sh.warg[parity][i];
+                    }
+                arg_out[0] = alpha;
+                arg_out[1] = __int_as_float(am);
+            }
+        }
         // the first cell's left interface from the previous thread, after one barrier
         float hs[CPT];
         weno_right_fluxes<CPT>(w, alpha, hs);
@@ -730,10 +769,10 @@ INC_DEV void rhs_core_wide(const float (&u)[CPT], float (&r)[CPT], int conv, flo
     }
 }
 
-template <int CPT, int TPR, int BAR = 0>
+template <int CPT, int TPR, int BAR = 0, bool ARG = false>
 INC_DEV void full_rhs_wide(const Args& a, const Ctx<CPT>& cx, const float (&x)[CPT], float (&r)[CPT], float t,
-                           WideSmem<CPT, TPR>& sh, int& parity, int g) {
-    rhs_core_wide<CPT, TPR, BAR>(x, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, sh, parity, g);
+                           WideSmem<CPT, TPR>& sh, int& parity, int g, float* arg_out = nullptr) {
+    rhs_core_wide<CPT, TPR, BAR, ARG>(x, r, a.conv, cx.nu, a.inv_dx, a.inv_dx2, a.inv_2dx, sh, parity, g, arg_out);
     parity ^= 1;
     add_source<CPT>(a, cx, x, r, t);
 }
@@ -864,6 +903,93 @@ INC_DEV void rhs_vjp_wide(const Args& a, const Ctx<1>& cx, float u, float v, flo
         }
     } else {  // R_i = -u_i (u_{i+1} - u_{i-1}) / (2 dx)
         out = -v * ((w[4] - w[2]) * a.inv_2dx) - v_l * w[2] * a.inv_2dx + v_r * w[4] * a.inv_2dx;
+    }
+    out += cx.nu * ((v_l - 2.f * v + v_r) * a.inv_dx2);
+    if (a.src == INC_SRC_LINEAR) out = fmaf(cx.beta, v, out);
+}
+
+// rhs_vjp_wide with its v-independent part done ahead.  At one cell the WENO part
+// of J(u)^T v is linear in hb = (v[g+1] - v[g]) / dx, the adjoint of the
+// interface flux g + 1/2 this cell owns: the contributions to cells g-2 .. g+3
+// are hb * m[e] and to alpha hb * pa.  vjp_pre forms m, pa from the stage input's
+// window and its alpha / first argmax (recorded by the segment replay); the
+// stage then scales and scatters them.
+struct VjpPre {
+    float m[6];  // d(hp + hm)/du at cells g-2 .. g+3 through the flux split
+    float pa;    // d(hp + hm)/dalpha
+    float u_l, u, u_r;  // the stage input at cells g-1, g, g+1
+    int am;
+};
+
+// stage input row `row` (in shared memory, read with the row's period) and its
+// recorded alpha / argmax al[0], al[1]
+template <int TPR>
+INC_DEV void vjp_pre(const Args& a, const float* row, const float* al, int g, VjpPre& p) {
+    constexpr int N = TPR;
+    float w[7];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) w[k] = row[(g - 3 + k + N) & (N - 1)];
+    p.u_l = w[2];
+    p.u = w[3];
+    p.u_r = w[4];
+    if (a.conv == INC_CONV_WENO) {
+        const float alpha = al[0];
+        p.am = __float_as_int(al[1]);
+        float fp[7], fm[7];
+#pragma unroll
+        for (int k = 0; k < 7; ++k) flux_split(w[k], 0.5f * alpha, fp[k], fm[k]);
+        Weno wl, wr;
+        weno5_eval<false>(fp[1], fp[2], fp[3], fp[4], fp[5], wl);
+        weno5_eval<true>(fm[2], fm[3], fm[4], fm[5], fm[6], wr);
+        float kp[6], km[6];  // dh+/df+ and dh-/df- at cells g-2 .. g+3 (hb = 1)
+#pragma unroll
+        for (int e = 0; e < 6; ++e) { kp[e] = 0.f; km[e] = 0.f; }
+        weno5_vjp_tail<false>(wl, 1.f, kp[0], kp[1], kp[2], kp[3], kp[4]);
+        weno5_vjp_tail<true>(wr, 1.f, km[1], km[2], km[3], km[4], km[5]);
+        float pa = 0.f;
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+            const float uj = w[e + 1];  // f+- = u (u/4 +- alpha/2)
+            p.m[e] = kp[e] * (0.5f * (uj + alpha)) + km[e] * (0.5f * (uj - alpha));
+            pa += 0.5f * uj * (kp[e] - km[e]);
+        }
+        p.pa = pa;
+    }
+}
+
+// out = J(u)^T v at this thread's cell from the precomputed p (rhs_vjp_wide's
+// values up to FP32 rounding).  `ahead` runs between the two barriers, beside
+// this stage's arithmetic: the caller's precomputation for the next stage.
+template <int TPR, int BAR, typename AHEAD>
+INC_DEV void rhs_vjp_wide_pre(const Args& a, const Ctx<1>& cx, const VjpPre& p, float v, float& out,
+                              WideAdjSmem<TPR>& sh, int g, AHEAD&& ahead) {
+    constexpr int N = TPR, NW = TPR / 32;
+    const int lane = g & 31, warp = g >> 5;
+    sh.vrow[g] = v;
+    row_sync<BAR, TPR>();
+    const float v_r = sh.vrow[(g + 1) & (N - 1)], v_l = sh.vrow[(g + N - 1) & (N - 1)];
+    const bool weno = a.conv == INC_CONV_WENO;
+    if (weno) {
+        const float hb = (v_r - v) * a.inv_dx;
+#pragma unroll
+        for (int e = 0; e < 6; ++e) sh.ub[e][g] = hb * p.m[e];
+        const float abar = group_sum<32>(hb * p.pa);
+        if (lane == 0) sh.wsum[warp] = abar;
+    }
+    ahead();
+    row_sync<BAR, TPR>();
+    if (weno) {
+        out = sh.ub[0][(g + 2) & (N - 1)] + sh.ub[1][(g + 1) & (N - 1)] + sh.ub[2][g] +
+              sh.ub[3][(g + N - 1) & (N - 1)] + sh.ub[4][(g + N - 2) & (N - 1)] + sh.ub[5][(g + N - 3) & (N - 1)];
+        if (g == p.am) {  // alpha = |u[argmax]|: d|u|/du = sign(u)
+            float abar = 0.f;
+#pragma unroll
+            for (int i = 0; i < NW; ++i) abar += sh.wsum[i];
+            const float sg = p.u > 0.f ? 1.f : (p.u < 0.f ? -1.f : 0.f);
+            out = fmaf(abar, sg, out);
+        }
+    } else {
+        out = -v * ((p.u_r - p.u_l) * a.inv_2dx) - v_l * p.u_l * a.inv_2dx + v_r * p.u_r * a.inv_2dx;
     }
     out += cx.nu * ((v_l - 2.f * v + v_r) * a.inv_dx2);
     if (a.src == INC_SRC_LINEAR) out = fmaf(cx.beta, v, out);
@@ -1010,12 +1136,16 @@ __global__ void __launch_bounds__(TPR, 1) k_rollout_bwd_wide(Args a) {
 // one half of a double buffer) while threads [TPR, 2 TPR) differentiate segment s
 // from the other half, so the replay leaves the adjoint's critical path.  Each
 // group syncs on its own named barrier (1: replay, 2: adjoint); the two meet at
-// one CTA barrier per segment, where the halves change hands.
+// one CTA barrier per segment, where the halves change hands.  Rows up to 128
+// cells: the replay also records each stage input's alpha and first argmax, and
+// the adjoint forms the next stage's reconstruction quantities (vjp_pre) while
+// it differentiates this one, between the stage's two barriers.
 template <int TPR>
 __global__ void __launch_bounds__(2 * TPR, 1) k_rollout_bwd_wide2(Args a) {
+    constexpr bool AHEAD = TPR <= 128;  // wider rows keep 128 registers a thread (512 threads)
     __shared__ WideSmem<1, TPR> shr;
     __shared__ WideAdjSmem<TPR> sha;
-    extern __shared__ float segbuf[];  // [2][3 ckpt_every][TPR]
+    extern __shared__ float segbuf[];  // [2][3 ckpt_every][TPR], then (AHEAD) [2][3 ckpt_every][2] alpha, argmax
     const int row = blockIdx.x;
     const bool rep = threadIdx.x < TPR;
     const int g = rep ? threadIdx.x : threadIdx.x - TPR;
@@ -1028,11 +1158,13 @@ __global__ void __launch_bounds__(2 * TPR, 1) k_rollout_bwd_wide2(Args a) {
     const float dt = cx.dt;
     const int64_t base = (int64_t)row * TPR + g;
     const int half = 3 * K * TPR;
+    float* alph = segbuf + 2 * half;
     const float* ckr = a.ckpts + (int64_t)row * nseg * TPR + g;
     int parity = 0;
     // segment sidx replayed into its half of the buffer (replay group)
     auto replay = [&](int sidx) {
         float* seg = segbuf + (sidx & 1) * half;
+        float* al = alph + (sidx & 1) * 6 * K;
         const int k0 = sidx * K;
         const int len = min(K, a.steps - k0);
         float x[1] = {__ldg(ckr + (int64_t)sidx * TPR)}, r[1];
@@ -1040,10 +1172,16 @@ __global__ void __launch_bounds__(2 * TPR, 1) k_rollout_bwd_wide2(Args a) {
             const float t = cx.t + (k0 + j) * dt;
             const float u0 = x[0];
             seg[3 * j * TPR + g] = u0;
-            const int run = j + 1 < len ? stages : stages - 1;
+            // with AHEAD every stage input's right-hand side runs (its alpha is recorded),
+            // the last step's last one included
+            const int run = (AHEAD || j + 1 < len) ? stages : stages - 1;
             float d = 0.f;
             for (int k = 0; k < run; ++k) {  // as advance_wide
-                full_rhs_wide<1, TPR, 1>(a, cx, x, r, t + rk3_c(k) * dt, shr, parity, g);
+                if constexpr (AHEAD)
+                    full_rhs_wide<1, TPR, 1, true>(a, cx, x, r, t + rk3_c(k) * dt, shr, parity, g,
+                                                   al + 2 * (3 * j + k));
+                else
+                    full_rhs_wide<1, TPR, 1>(a, cx, x, r, t + rk3_c(k) * dt, shr, parity, g);
                 d = rk3_b(k) * fmaf(dt, r[0], d);
                 x[0] = u0 + d;
                 if (k + 1 < stages) seg[(3 * j + 1 + k) * TPR + g] = x[0];
@@ -1065,17 +1203,143 @@ __global__ void __launch_bounds__(2 * TPR, 1) k_rollout_bwd_wide2(Args a) {
             const float* seg = segbuf + (sidx & 1) * half;
             const int k0 = sidx * K;
             const int len = min(K, a.steps - k0);
+            if constexpr (AHEAD) {
+                const float* al = alph + (sidx & 1) * 6 * K;
+                VjpPre cur, nxt;
+                vjp_pre<TPR>(a, seg + (3 * (len - 1) + stages - 1) * TPR, al + 2 * (3 * (len - 1) + stages - 1), g,
+                             cur);
+                for (int j = len - 1; j >= 0; --j) {
+                    const int k = k0 + j;
+                    if (gfr) {
+                        gu += gf;
+                        if (k > 0) gf = __ldg(gfr + (int64_t)(k - 1) * TPR);
+                    }
+                    float acc = 0.f;
+                    for (int st = stages - 1; st >= 0; --st) {  // as stages_bwd_wide
+                        const int jn = st > 0 ? j : j - 1, sn = st > 0 ? st - 1 : stages - 1;
+                        float rv;
+                        rhs_vjp_wide_pre<TPR, 2>(a, cx, cur, gu, rv, sha, g, [&] {
+                            if (jn >= 0) vjp_pre<TPR>(a, seg + (3 * jn + sn) * TPR, al + 2 * (3 * jn + sn), g, nxt);
+                        });
+                        const float ka = rk3_a(st), kb = rk3_b(st);
+                        gs += kb * dt * gu;
+                        acc += ka * gu;
+                        gu = kb * (gu + dt * rv);
+                        cur = nxt;
+                    }
+                    gu += acc;
+                }
+            } else {
+                for (int j = len - 1; j >= 0; --j) {
+                    const int k = k0 + j;
+                    if (gfr) {
+                        gu += gf;
+                        if (k > 0) gf = __ldg(gfr + (int64_t)(k - 1) * TPR);
+                    }
+                    stages_bwd_wide<TPR, 2>(a, cx, seg[3 * j * TPR + g], seg[(3 * j + 1) * TPR + g],
+                                            seg[(3 * j + 2) * TPR + g], gu, gs, sha, g);
+                }
+            }
+        }
+        __syncthreads();  // segment sidx - 1 replayed, segment sidx's half free
+    }
+    if (!rep) {
+        a.g_u[base] = gu;
+        if (a.g_s) a.g_s[base] = gs;
+    }
+}
+
+// The same backward on a cluster of two CTAs per row, for small batches (two
+// CTAs per row fit on the GPU's SMs): CTA 0 replays segment s - 1 and writes its
+// stage inputs, alphas and argmaxes straight into CTA 1's shared memory
+// (distributed shared memory); CTA 1 differentiates segment s with the stage
+// quantities formed one stage ahead.  Each CTA has an SM's schedulers to itself;
+// they meet at one cluster barrier per segment, where the buffer halves change
+// hands (the barrier orders the remote stores before CTA 1's reads).
+template <int TPR>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TPR, 1) k_rollout_bwd_cl(Args a) {
+    namespace cg = cooperative_groups;
+    __shared__ WideSmem<1, TPR> shr;   // CTA 0
+    __shared__ WideAdjSmem<TPR> sha;   // CTA 1
+    extern __shared__ float segbuf[];  // (CTA 1) [2][3 ckpt_every][TPR], then [2][3 ckpt_every][2] alpha, argmax
+    cg::cluster_group cl = cg::this_cluster();
+    const bool rep = cl.block_rank() == 0;
+    const int row = blockIdx.x >> 1;
+    const int g = threadIdx.x;
+    Ctx<1> cx;
+    make_ctx<1, TPR>(a, row, g, true, cx);
+    if (cx.has_s) cx.s[0] = __ldg(a.s + (int64_t)row * TPR + g);
+    const int K = a.ckpt_every;
+    const int nseg = (a.steps + K - 1) / K;
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
+    const float dt = cx.dt;
+    const int64_t base = (int64_t)row * TPR + g;
+    const int half = 3 * K * TPR;
+    float* dseg = rep ? cl.map_shared_rank(segbuf, 1) : segbuf;  // CTA 1's buffer
+    float* dalph = dseg + 2 * half;
+    const float* ckr = a.ckpts + (int64_t)row * nseg * TPR + g;
+    int parity = 0;
+    auto replay = [&](int sidx) {  // CTA 0: segment sidx into its half of CTA 1's buffer
+        float* seg = dseg + (sidx & 1) * half;
+        float* al = dalph + (sidx & 1) * 6 * K;
+        const int k0 = sidx * K;
+        const int len = min(K, a.steps - k0);
+        float x[1] = {__ldg(ckr + (int64_t)sidx * TPR)}, r[1];
+        for (int j = 0; j < len; ++j) {
+            const float t = cx.t + (k0 + j) * dt;
+            const float u0 = x[0];
+            seg[3 * j * TPR + g] = u0;
+            float d = 0.f;
+            for (int k = 0; k < stages; ++k) {  // every stage input's alpha is recorded, the last one's too
+                full_rhs_wide<1, TPR, 0, true>(a, cx, x, r, t + rk3_c(k) * dt, shr, parity, g, al + 2 * (3 * j + k));
+                d = rk3_b(k) * fmaf(dt, r[0], d);
+                x[0] = u0 + d;
+                if (k + 1 < stages) seg[(3 * j + 1 + k) * TPR + g] = x[0];
+            }
+        }
+    };
+    if (rep) replay(nseg - 1);
+    cl.sync();
+    const float* gfr = a.g_frames ? a.g_frames + (int64_t)row * a.steps * TPR + g : nullptr;
+    float gu = 0.f, gf = 0.f, gs = 0.f;
+    if (!rep) {
+        gu = a.g_final ? __ldg(a.g_final + base) : 0.f;
+        gf = gfr ? __ldg(gfr + (int64_t)(a.steps - 1) * TPR) : 0.f;
+    }
+    for (int sidx = nseg - 1; sidx >= 0; --sidx) {
+        if (rep) {
+            if (sidx > 0) replay(sidx - 1);
+        } else {
+            const float* seg = segbuf + (sidx & 1) * half;
+            const float* al = dalph + (sidx & 1) * 6 * K;
+            const int k0 = sidx * K;
+            const int len = min(K, a.steps - k0);
+            VjpPre cur, nxt;
+            vjp_pre<TPR>(a, seg + (3 * (len - 1) + stages - 1) * TPR, al + 2 * (3 * (len - 1) + stages - 1), g,
+                         cur);
             for (int j = len - 1; j >= 0; --j) {
                 const int k = k0 + j;
                 if (gfr) {
                     gu += gf;
                     if (k > 0) gf = __ldg(gfr + (int64_t)(k - 1) * TPR);
                 }
-                stages_bwd_wide<TPR, 2>(a, cx, seg[3 * j * TPR + g], seg[(3 * j + 1) * TPR + g],
-                                        seg[(3 * j + 2) * TPR + g], gu, gs, sha, g);
+                float acc = 0.f;
+                for (int st = stages - 1; st >= 0; --st) {  // as stages_bwd_wide
+                    const int jn = st > 0 ? j : j - 1, sn = st > 0 ? st - 1 : stages - 1;
+                    float rv;
+                    rhs_vjp_wide_pre<TPR, 0>(a, cx, cur, gu, rv, sha, g, [&] {
+                        if (jn >= 0) vjp_pre<TPR>(a, seg + (3 * jn + sn) * TPR, al + 2 * (3 * jn + sn), g, nxt);
+                    });
+                    const float ka = rk3_a(st), kb = rk3_b(st);
+                    gs += kb * dt * gu;
+                    acc += ka * gu;
+                    gu = kb * (gu + dt * rv);
+                    cur = nxt;
+                }
+                gu += acc;
             }
         }
-        __syncthreads();  // segment sidx - 1 replayed, segment sidx's half free
+        cl.sync();  // segment sidx - 1 written, segment sidx's half free
     }
     if (!rep) {
         a.g_u[base] = gu;
@@ -1176,14 +1440,25 @@ int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
     }
     const size_t smem = (size_t)3 * b.ckpt_every * TPR * sizeof(float);
     const int nseg = (b.steps + b.ckpt_every - 1) / b.ckpt_every;
+    // few rows: two CTAs per row (replay and adjoint each on an SM of their own)
+    if constexpr (TPR <= 256) {
+        const size_t dyn = 2 * smem + (size_t)2 * 3 * b.ckpt_every * 2 * sizeof(float);
+        if (nseg >= 2 && 2 * b.rows <= sm_count() && dyn + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
+            if (dyn + bwd_wide2_static_smem<TPR>() > 48 * 1024)
+                cudaFuncSetAttribute(k_rollout_bwd_cl<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+            k_rollout_bwd_cl<TPR><<<2 * b.rows, TPR, dyn, st>>>(b);
+            return check_launch("burgers_bwd_cluster");
+        }
+    }
     // several segments: the warp-specialised form overlaps each replay with the adjoint
     // before it (two thread groups; rows up to 256 cells keep 128 registers a thread)
     if constexpr (TPR <= 256) {
-        if (nseg >= 2 && 2 * smem + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
-            if (2 * smem + bwd_wide2_static_smem<TPR>() > 48 * 1024)
+        const size_t dyn = 2 * smem + (size_t)2 * 3 * b.ckpt_every * 2 * sizeof(float);  // + alpha, argmax
+        if (nseg >= 2 && dyn + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
+            if (dyn + bwd_wide2_static_smem<TPR>() > 48 * 1024)
                 cudaFuncSetAttribute(k_rollout_bwd_wide2<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     (int)(2 * smem));
-            k_rollout_bwd_wide2<TPR><<<b.rows, 2 * TPR, 2 * smem, st>>>(b);
+                                     (int)dyn);
+            k_rollout_bwd_wide2<TPR><<<b.rows, 2 * TPR, dyn, st>>>(b);
             return check_launch("burgers_bwd_wide2");
         }
     }

@@ -22,6 +22,17 @@ inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s
 
 inline bool is_pow2(int64_t v) { return v > 0 && (v & (v - 1)) == 0; }
 
+// SMs of the current device, looked up once per device
+inline int sm_count() {
+    static int cache[64] = {0};
+    int dev = 0, n = 0;
+    cudaGetDevice(&dev);
+    if (dev >= 0 && dev < 64 && cache[dev] > 0) return cache[dev];
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (dev >= 0 && dev < 64) cache[dev] = n;
+    return n;
+}
+
 // ---- warp helpers ------------------------------------------------------------
 // All shuffles are issued by the full warp: every kernel here keeps all 32 lanes
 // on the same control path (rows past the end are masked, never skipped).
