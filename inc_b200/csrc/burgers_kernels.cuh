@@ -1347,6 +1347,138 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TPR, 1) k_rollout_bw
     }
 }
 
+// Per cell and stage input, what the precompute CTA hands the adjoint CTA:
+// m[0..5], pa (VjpPre) and the stage input u.
+constexpr int kPreVals = 8;
+
+// The same backward on a cluster of three CTAs per row (2 TPR threads each), a
+// pipeline over segments: CTA 0 replays segment s - 2 into CTA 1's shared memory
+// (stage inputs, alphas, argmaxes); CTA 1's two thread groups form segment s - 1's
+// per-cell stage quantities (vjp_pre, one stage input per group at a time) into
+// CTA 2's shared memory; CTA 2 differentiates segment s, each stage only scaling
+// and scattering them.  One cluster barrier per pipeline step orders the remote
+// stores before their readers and frees the double buffers' halves.
+template <int TPR>
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(2 * TPR, 1) k_rollout_bwd_cl3(Args a) {
+    namespace cg = cooperative_groups;
+    __shared__ WideSmem<1, TPR> shr;   // CTA 0
+    __shared__ WideAdjSmem<TPR> sha;   // CTA 2
+    extern __shared__ float dsm[];     // CTA 1: seg [2][3K][TPR], alpha/argmax [2][3K][2];
+                                       // CTA 2: pre [2][3K][kPreVals][TPR], argmax [2][3K]
+    cg::cluster_group cl = cg::this_cluster();
+    const int role = (int)cl.block_rank();  // 0 replay, 1 precompute, 2 adjoint
+    const int row = blockIdx.x / 3;
+    const int t = threadIdx.x;
+    const int g = t % TPR;
+    const bool lead = t < TPR;  // CTAs 0 and 2 run one group of TPR threads
+    Ctx<1> cx;
+    make_ctx<1, TPR>(a, row, g, true, cx);
+    if (cx.has_s) cx.s[0] = __ldg(a.s + (int64_t)row * TPR + g);
+    const int K = a.ckpt_every;
+    const int nseg = (a.steps + K - 1) / K;
+    const int stages = a.scheme == INC_TS_EULER ? 1 : 3;
+    const float dt = cx.dt;
+    const int64_t base = (int64_t)row * TPR + g;
+    const int half_seg = 3 * K * TPR, half_pre = 3 * K * kPreVals * TPR;
+    float* seg1 = role == 0 ? cl.map_shared_rank(dsm, 1) : dsm;   // CTA 1's buffers
+    float* alph1 = seg1 + 2 * half_seg;
+    float* pre2 = role == 1 ? cl.map_shared_rank(dsm, 2) : dsm;   // CTA 2's buffers
+    int* am2 = reinterpret_cast<int*>(pre2 + 2 * half_pre);
+    const float* ckr = a.ckpts + (int64_t)row * nseg * TPR + g;
+    int parity = 0;
+    auto seg_len = [&](int sidx) { return min(K, a.steps - sidx * K); };
+    auto replay = [&](int sidx) {  // CTA 0, threads [0, TPR)
+        float* seg = seg1 + (sidx & 1) * half_seg;
+        float* al = alph1 + (sidx & 1) * 6 * K;
+        const int k0 = sidx * K, len = seg_len(sidx);
+        float x[1] = {__ldg(ckr + (int64_t)sidx * TPR)}, r[1];
+        for (int j = 0; j < len; ++j) {
+            const float tt = cx.t + (k0 + j) * dt;
+            const float u0 = x[0];
+            seg[3 * j * TPR + g] = u0;
+            float d = 0.f;
+            for (int k = 0; k < stages; ++k) {
+                full_rhs_wide<1, TPR, 1, true>(a, cx, x, r, tt + rk3_c(k) * dt, shr, parity, g, al + 2 * (3 * j + k));
+                d = rk3_b(k) * fmaf(dt, r[0], d);
+                x[0] = u0 + d;
+                if (k + 1 < stages) seg[(3 * j + 1 + k) * TPR + g] = x[0];
+            }
+        }
+    };
+    auto precompute = [&](int sidx) {  // CTA 1, group t / TPR takes every other stage input
+        const float* seg = dsm + (sidx & 1) * half_seg;
+        const float* al = dsm + 2 * half_seg + (sidx & 1) * 6 * K;
+        float* out = pre2 + (sidx & 1) * half_pre;
+        int* amo = am2 + (sidx & 1) * 3 * K;
+        const int len = seg_len(sidx);
+        for (int j = 0; j < len; ++j)
+            for (int k = 0; k < stages; ++k) {
+                const int i = 3 * j + k;
+                if ((j * stages + k) % 2 != t / TPR) continue;
+                VjpPre p;
+                vjp_pre<TPR>(a, seg + i * TPR, al + 2 * i, g, p);
+                float* o = out + i * kPreVals * TPR + g;
+#pragma unroll
+                for (int e = 0; e < 6; ++e) o[e * TPR] = p.m[e];
+                o[6 * TPR] = p.pa;
+                o[7 * TPR] = p.u;
+                if (g == 0) amo[i] = p.am;
+            }
+    };
+    const float* gfr = a.g_frames ? a.g_frames + (int64_t)row * a.steps * TPR + g : nullptr;
+    float gu = 0.f, gf = 0.f, gs = 0.f;
+    if (role == 2 && lead) {
+        gu = a.g_final ? __ldg(a.g_final + base) : 0.f;
+        gf = gfr ? __ldg(gfr + (int64_t)(a.steps - 1) * TPR) : 0.f;
+    }
+    auto adjoint = [&](int sidx) {  // CTA 2, threads [0, TPR)
+        const float* pre = dsm + (sidx & 1) * half_pre;
+        const int* am = reinterpret_cast<const int*>(dsm + 2 * half_pre) + (sidx & 1) * 3 * K;
+        const int k0 = sidx * K, len = seg_len(sidx);
+        for (int j = len - 1; j >= 0; --j) {
+            const int k = k0 + j;
+            if (gfr) {
+                gu += gf;
+                if (k > 0) gf = __ldg(gfr + (int64_t)(k - 1) * TPR);
+            }
+            float acc = 0.f;
+            for (int st = stages - 1; st >= 0; --st) {  // as stages_bwd_wide
+                const int i = 3 * j + st;
+                const float* q = pre + i * kPreVals * TPR;
+                VjpPre p;
+#pragma unroll
+                for (int e = 0; e < 6; ++e) p.m[e] = q[e * TPR + g];
+                p.pa = q[6 * TPR + g];
+                p.u = q[7 * TPR + g];
+                p.u_l = q[7 * TPR + ((g + TPR - 1) & (TPR - 1))];
+                p.u_r = q[7 * TPR + ((g + 1) & (TPR - 1))];
+                p.am = am[i];
+                float rv;
+                rhs_vjp_wide_pre<TPR, 2>(a, cx, p, gu, rv, sha, g, [] {});
+                const float ka = rk3_a(st), kb = rk3_b(st);
+                gs += kb * dt * gu;
+                acc += ka * gu;
+                gu = kb * (gu + dt * rv);
+            }
+            gu += acc;
+        }
+    };
+    for (int it = 0; it < nseg + 2; ++it) {
+        if (role == 0) {
+            if (lead && nseg - 1 - it >= 0) replay(nseg - 1 - it);
+        } else if (role == 1) {
+            if (nseg - it >= 0 && nseg - it < nseg) precompute(nseg - it);
+        } else if (lead && nseg + 1 - it >= 0 && nseg + 1 - it < nseg) {
+            adjoint(nseg + 1 - it);
+        }
+        cl.sync();
+    }
+    if (role == 2 && lead) {
+        a.g_u[base] = gu;
+        if (a.g_s) a.g_s[base] = gs;
+    }
+}
+
 // weno_reconstruction(f, direction) as a standalone op (solver_1d.py:4-42).
 template <int CPT, int TPR>
 __global__ void __launch_bounds__(256) k_weno(const float* __restrict__ f, float* __restrict__ out, int rows,
@@ -1440,7 +1572,19 @@ int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
     }
     const size_t smem = (size_t)3 * b.ckpt_every * TPR * sizeof(float);
     const int nseg = (b.steps + b.ckpt_every - 1) / b.ckpt_every;
-    // few rows: two CTAs per row (replay and adjoint each on an SM of their own)
+    // few rows: three CTAs per row (replay, the stages' precomputation and the
+    // adjoint each on an SM of their own), or two (replay, adjoint)
+    if constexpr (TPR <= 128) {
+        const size_t seg1 = (size_t)(2 * 3 * b.ckpt_every * TPR + 2 * 3 * b.ckpt_every * 2) * sizeof(float);
+        const size_t pre2 = (size_t)(2 * 3 * b.ckpt_every * kPreVals * TPR + 2 * 3 * b.ckpt_every) * sizeof(float);
+        const size_t dyn = seg1 > pre2 ? seg1 : pre2;
+        if (3 * b.rows <= sm_count() && dyn + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
+            if (dyn + bwd_wide2_static_smem<TPR>() > 48 * 1024)
+                cudaFuncSetAttribute(k_rollout_bwd_cl3<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
+            k_rollout_bwd_cl3<TPR><<<3 * b.rows, 2 * TPR, dyn, st>>>(b);
+            return check_launch("burgers_bwd_cluster3");
+        }
+    }
     if constexpr (TPR <= 256) {
         const size_t dyn = 2 * smem + (size_t)2 * 3 * b.ckpt_every * 2 * sizeof(float);
         if (nseg >= 2 && 2 * b.rows <= sm_count() && dyn + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
