@@ -258,6 +258,35 @@ def test_wide_adjoint_matches_warp_adjoint(cuda, n, scheme, conv, eq):
         assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 2e-5
 
 
+@pytest.mark.parametrize("n,B", [(128, 40), (128, 60), (128, 100), (256, 40), (256, 100), (64, 49)])
+def test_wide_adjoint_forms_by_batch(cuda, n, B):
+    """The one-cell-per-thread adjoint takes one of three forms by batch size (three
+    CTAs per row up to 49 rows at n <= 128, two CTAs per row up to 74, two thread
+    groups on one CTA above); each against the warp-layout adjoint of the same
+    checkpointed rollout (three segments), gradients w.r.t. u0 and s."""
+    from inc_b200.rollout import burgers_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    L = 2 * math.pi
+    g = torch.Generator().manual_seed(7 * n + B)
+    u0 = torch.tensor(_rand_u0(B, n, n + B), dtype=torch.float32, device=cuda)
+    s0 = 0.05 * (torch.rand(B, n, generator=g) - 0.5).to(cuda)
+    nu = (0.005 + 0.02 * torch.rand(B, 1, generator=g)).to(cuda)
+    wf = torch.cos(torch.arange(11 * n, device=cuda).reshape(11, n) * 0.01)
+    out = []
+    for cpt in (1, _WARP_CPT[n]):
+        sp = SimpleNamespace(resolution=n, dt=0.2 / n, x=None, adaptive_CFL=None, L=L, nu=nu, device=cuda,
+                             convection_term="WENO", equation_type="viscosity", batch_size=B,
+                             time_scheme="ssprk3", cells_per_thread=cpt)
+        slv = BurgersSolverTorch(sp)
+        u = u0.clone().requires_grad_(True)
+        s = s0.clone().requires_grad_(True)
+        fr = burgers_rollout(slv, u, 11, s=s, ckpt_every=4)
+        out.append(torch.autograd.grad((fr * wf).sum(), (u, s)))
+    for a, b in zip(*out):
+        assert torch.isfinite(a).all()
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 2e-5
+
+
 def test_fd_check_fp64_oracle(cuda):
     """GPU adjoint vs FP64 central differences (h=1e-6) of the oracle, 3 SSP-RK3 steps."""
     from inc_b200.solvers import BurgersSolverTorch
