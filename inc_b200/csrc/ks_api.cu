@@ -269,7 +269,10 @@ extern "C" int64_t inc_ks_rollout_bwd_work_size(const inc_ks_plan* p, int32_t ck
     // one [ckpt_every][3][n] float2 slot per launched group (the launch's grid x groups per block)
     const int gpb = pick_block(Kind::RolloutBwd, p->npairs, T, n, ckpt_every) / T;
     const int64_t groups = (int64_t)((p->npairs + gpb - 1) / gpb) * gpb;
-    return groups * 3 * ckpt_every * n * (int64_t)sizeof(float2);
+    // 32 lanes and up to 8 values per lane in the common case (ETRK2, one domain size
+    // per pair): the warp-specialised backward keeps two segments per pair
+    const int64_t segs = (T == 32 && n / T <= 8 && p->scheme == INC_KS_ETRK2 && !p->split) ? 2 : 1;
+    return segs * groups * 3 * ckpt_every * n * (int64_t)sizeof(float2);
 }
 
 static int ks_rollout_bwd(const inc_ks_plan* p, const float* ckpts, const float* s, int32_t steps,

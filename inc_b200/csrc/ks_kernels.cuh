@@ -1203,6 +1203,79 @@ __global__ void __launch_bounds__(128) k_rollout_bwd(Args a) {
     adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
 }
 
+// The same backward with the segment replay on a second warp: one row pair per
+// CTA of 2 T threads (T = 32, P <= 8, the common case).  Warp 0 replays segment s - 1 from
+// its checkpoint into one half of a double buffer (every step's start state in
+// shared memory, its substep states in the global scratch, which holds two
+// segments per pair) while warp 1 differentiates segment s from the other half, so
+// only the adjoint's transforms stay on the critical path.  The two warps meet at
+// one block barrier per segment, which also orders the replay's scratch stores
+// before the adjoint's loads.
+template <int P, int T, int FAST>
+__global__ void __launch_bounds__(2 * T) k_rollout_bwd_ws(Args a) {
+    static_assert(T == 32, "one warp per role");
+    extern __shared__ float2 sm[];
+    constexpr int N = P * T;
+    const int t = threadIdx.x % T;
+    const bool rep = threadIdx.x < T;
+    const Twiddles<P, T> tw = setup_twiddles<P, T>(a, sm, t);
+    const int K = a.ckpt_every;
+    constexpr int GS = group_stride<T>(2 * buf_len<P, T>());
+    float2* base = sm + tw_size<P, T>();
+    const Buf<P, T> buf = group_buf<P, T>(base + (rep ? 0 : GS), t);
+    float2* st = base + 2 * GS;  // the adjoint's state slots
+    float2* segb = st + 5 * N;   // [2][K][N] step start states
+    const int pair = blockIdx.x;
+    Ctx c;
+    make_ctx(a, pair, t, pair < a.npairs, c);
+    SlotCache<P, T> cc;
+    cc.load(a, c);
+    const int nseg = (a.steps + K - 1) / K;
+    float2* stgb = a.stage + (size_t)pair * 2 * 3 * K * N;  // [2][3K][N] substep states
+    auto replay = [&](int sidx) {
+        float2 x[P];
+        load_pair_strided<P, T>(x, a.ckpts, c, N, (int64_t)nseg * N, (int64_t)sidx * N);
+        forward_program<P, T, FAST>(a, c, x, min(K, a.steps - sidx * K), buf, tw, false, nseg, false,
+                                    segb + (sidx & 1) * K * N, stgb + (size_t)(sidx & 1) * 3 * K * N, 1);
+    };
+    float2 G[P], Sacc[P], SS[P], gf[P];
+    const int64_t gf_stride = (int64_t)a.steps * N;
+    if (!rep) {
+        adjoint_prologue<P, T>(a, c, cc, a.g_final, SS, G, buf, tw);
+#pragma unroll
+        for (int m = 0; m < P; ++m) Sacc[m] = make_float2(0.f, 0.f);
+        if (a.g_frames) load_pair_strided<P, T>(gf, a.g_frames, c, N, gf_stride, (int64_t)(a.steps - 1) * N);
+    }
+    if (rep) replay(nseg - 1);
+    __syncthreads();
+    for (int sidx = nseg - 1; sidx >= 0; --sidx) {
+        if (rep) {
+            if (sidx > 0) replay(sidx - 1);
+        } else {
+            const float2* seg = segb + (sidx & 1) * K * N;
+            const float2* stg = stgb + (size_t)(sidx & 1) * 3 * K * N;
+            const int k0 = sidx * K;
+            const int len = min(K, a.steps - k0);
+            for (int j = len - 1; j >= 0; --j) {
+                const int k = k0 + j;
+                if (a.g_frames) {  // G += FFT(dL/dframe_k)/N, the next step's frame adjoint loaded meanwhile
+                    float2 v[P];
+#pragma unroll
+                    for (int m = 0; m < P; ++m) v[m] = gf[m];
+                    if (k > 0) load_pair_strided<P, T>(gf, a.g_frames, c, N, gf_stride, (int64_t)(k - 1) * N);
+                    fft_fwd<P, T>(v, buf, tw, t);
+#pragma unroll
+                    for (int m = 0; m < P; ++m) G[m] = cadd(G[m], cscale(v[m], a.invN));
+                }
+                step_bwd_program<P, T, true, FAST>(a, c, cc, SS, G, Sacc, nullptr, gf_stride, (int64_t)k * N,
+                                                   seg + j * N, st, buf, tw, stg + (size_t)j * 3 * N);
+            }
+        }
+        __syncthreads();  // segment sidx - 1 replayed, segment sidx's half free
+    }
+    if (!rep) adjoint_epilogue<P, T>(a, c, G, Sacc, buf, tw);
+}
+
 // Asynchronous 8-byte copies global -> shared (cp.async), in commit groups.
 INC_DEV void cp_async8(float2* smem_dst, const float2* gsrc) {
     const unsigned sa = (unsigned)__cvta_generic_to_shared(smem_dst);
@@ -1317,11 +1390,23 @@ int launch_fwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     return launch_with_smem(k_rollout<P, T>, grid, block, smem, st, a);
 }
 
+// Shared memory of k_rollout_bwd_ws (one row pair per CTA).
+template <int P, int T>
+size_t ws_smem_bytes(int K) {
+    return (tw_size<P, T>() + 2 * group_stride<T>(2 * buf_len<P, T>()) + (size_t)(5 + 2 * K) * P * T) *
+           sizeof(float2);
+}
+
 template <int P, int T>
 int launch_bwd_impl(Kind kind, const Args& a, cudaStream_t st, int block) {
     const int gpb = block / T;
     const int grid = (a.npairs + gpb - 1) / gpb;
     const size_t smem = smem_bytes<P, T>(kind, block, a.ckpt_every);
+    if constexpr (T == 32 && P <= 8) {  // the scratch then holds two segments per pair (inc_ks_rollout_bwd_work_size)
+        if (kind == Kind::RolloutBwd && a.stage && fast_case(a) && ws_smem_bytes<P, T>(a.ckpt_every) <= 227 * 1024)
+            return launch_with_smem(k_rollout_bwd_ws<P, T, 1>, a.npairs, 2 * T, ws_smem_bytes<P, T>(a.ckpt_every),
+                                    st, a);
+    }
     if (fast_case(a)) {
         if (kind == Kind::StepBwd) return launch_with_smem(k_step_bwd<P, T, 1>, grid, block, smem, st, a);
         if (kind == Kind::TapeBwd) return launch_with_smem(k_rollout_bwd_tape<P, T, 1>, grid, block, smem, st, a);

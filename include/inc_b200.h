@@ -295,7 +295,10 @@ int inc_ks_rollout_bwd(const inc_ks_plan* plan, const float* ckpts, const float*
  * inc_ks_rollout_bwd_work_size(plan, ckpt_every) bytes (16-byte aligned; -1 for
  * a bad plan or ckpt_every).  The segment replay keeps every step's substep
  * states there, so the adjoint does not rebuild them: 17 instead of 24 row-pair
- * transforms per step() (ETRK2).  Same results to rounding.                    */
+ * transforms per step() (ETRK2).  With 32 lanes and up to 8 values per lane per
+ * row pair, ETRK2 and one domain size per pair, a second warp replays the next
+ * segment while the first differentiates this one, and the scratch holds two
+ * segments per pair.  Same results to rounding.                                */
 int64_t inc_ks_rollout_bwd_work_size(const inc_ks_plan* plan, int32_t ckpt_every);
 int inc_ks_rollout_bwd_ws(const inc_ks_plan* plan, const float* ckpts, const float* s,
                           int32_t steps, int32_t ckpt_every, const float* g_frames,

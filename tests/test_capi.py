@@ -71,12 +71,15 @@ def test_struct_layouts():
 
 def test_ks_rollout_bwd_work_size_needs_no_gpu(lib):
     """The KS backward's scratch size: one [ckpt_every][3][n] complex slot per
-    launched row-pair group, computed on the host from the plan's shape."""
+    launched row-pair group (two for the warp-specialised form: ETRK2, 32 lanes and
+    up to 8 values per lane), computed on the host from the plan's shape."""
     from inc_b200 import _native as nat
     p = nat.KSPlan()
-    p.rows, p.n, p.npairs, p.threads_per_pair = 1024, 256, 512, 32
+    p.rows, p.n, p.npairs, p.threads_per_pair, p.scheme = 1024, 256, 512, 32, nat.INC_KS_ETD1
     # 512 pairs of 32 lanes launch one group per 32-thread block: 512 groups
     assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 8) == 512 * 3 * 8 * 256 * 8
+    p.scheme = nat.INC_KS_ETRK2  # the replay runs one segment ahead: two slots per pair
+    assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 8) == 2 * 512 * 3 * 8 * 256 * 8
     assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 0) == -1
     p.threads_per_pair = 64  # a pair spans two warps, one group per block
     assert lib.inc_ks_rollout_bwd_work_size(C.byref(p), 4) == 512 * 3 * 4 * 256 * 8
