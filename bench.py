@@ -1130,10 +1130,13 @@ def diff_line(args, world, cfg, cells, times, extra):
                    "scheme": cfg["scheme"], "corrector": cfg["corrector"],
                    "checkpoint_every": extra.get("graph_ckpt"),
                    "checkpoint_note": ("solver adjoint replays its own states; the corrector's activations "
-                                       "are kept (None) or recomputed every 8 steps"),
+                                       "are kept (None) or recomputed every 8 steps" if cfg["name"] == "ks_diff"
+                                       else "solver adjoint replays its states from checkpoints every 8 steps; "
+                                       "the fused forward records the CNN's hidden pre-activations (537 MB) "
+                                       "and the fused backward reads them"),
                    "value_is": "whole training step (rollout, loss, backward, Adam) in one CUDA graph",
                    "l2": "inputs and activations exceed L2 (not flushed)" if cfg["name"] == "ks_diff"
-                   else "not flushed (the 64 MB step keeps its activations in L2)",
+                   else "not flushed (the recorded pre-activations, 537 MB, exceed L2)",
                    "parallelism": (f"data-parallel over {world} GPUs: per-rank trajectories, corrector "
                                    "gradients averaged by one all-reduce per step" if world > 1
                                    else "single GPU")},

@@ -98,6 +98,10 @@ SIGNATURES = {
                                           _vp, C.c_int32, _vp, _vp]),
     "inc_burgers_cnn_rollout_bwd": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, _vp, C.c_double, C.c_int32,
                                               C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
+    "inc_burgers_cnn_rollout_acts": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, C.c_double, C.c_int32, _vp,
+                                               _vp, _vp, C.c_int32, _vp, _vp, _vp]),
+    "inc_burgers_cnn_rollout_bwd_acts": (C.c_int, [C.POINTER(BurgersDesc), _vp, _vp, _vp, _vp, C.c_double,
+                                                   C.c_int32, C.c_int32, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp]),
 }
 INC_NOALLOC_CKPT_FLOATS = 2 * 1024 * 1024
 INC_CNN_WEIGHT_FLOATS = 10657

@@ -26,7 +26,7 @@ namespace cnn {
 
 template <int N>
 __global__ void __launch_bounds__(512) k_cnn_rollout(Args a, const float* __restrict__ wts,
-                                                     float* __restrict__ corr) {
+                                                     float* __restrict__ corr, float* __restrict__ acts) {
     extern __shared__ __align__(16) unsigned char smraw[];
     Smem<N>& S = *reinterpret_cast<Smem<N>*>(smraw);
     constexpr int R = rows_per_cta<N>();
@@ -54,9 +54,20 @@ __global__ void __launch_bounds__(512) k_cnn_rollout(Args a, const float* __rest
         __syncthreads();  // also: the weights are in place (first step)
         conv_first<N>(S.w, act0[0], act1, cg, L);
         __syncthreads();
-        conv_mid<N>(S.w + OFF_W2, S.w + OFF_B2, act1, act0, cg, L);
-        __syncthreads();
-        conv_mid<N>(S.w + OFF_W3, S.w + OFF_B3, act0, act1, cg, L);
+        if (acts) {  // training: the hidden layers' pre-activations recorded for the backward
+            float acc[4][8];
+            conv_mid_acc<N>(S.w + OFF_W2, S.w + OFF_B2, act1, acc, cg, L);
+            if (valid) put_acts(acts, row, a.steps, k, 0, acc, cg, L, N);
+            store_tile<N, true>(act0, acc, cg, L);
+            __syncthreads();
+            conv_mid_acc<N>(S.w + OFF_W3, S.w + OFF_B3, act0, acc, cg, L);
+            if (valid) put_acts(acts, row, a.steps, k, 1, acc, cg, L, N);
+            store_tile<N, true>(act1, acc, cg, L);
+        } else {
+            conv_mid<N>(S.w + OFF_W2, S.w + OFF_B2, act1, act0, cg, L);
+            __syncthreads();
+            conv_mid<N>(S.w + OFF_W3, S.w + OFF_B3, act0, act1, cg, L);
+        }
         __syncthreads();
         conv_last_partial<N>(S.w + OFF_W4, act1, act0, cg, L);
         __syncthreads();
@@ -74,12 +85,12 @@ __global__ void __launch_bounds__(512) k_cnn_rollout(Args a, const float* __rest
 }
 
 template <int N>
-int launch(const Args& a, const float* w, float* corr, cudaStream_t st) {
+int launch(const Args& a, const float* w, float* corr, float* acts, cudaStream_t st) {
     constexpr int R = rows_per_cta<N>();
     const size_t smem = sizeof(Smem<N>);
     static_assert(sizeof(Smem<N>) <= 227 * 1024, "shared memory");
     cudaFuncSetAttribute(k_cnn_rollout<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    k_cnn_rollout<N><<<(a.rows + R - 1) / R, R * N, smem, st>>>(a, w, corr);
+    k_cnn_rollout<N><<<(a.rows + R - 1) / R, R * N, smem, st>>>(a, w, corr, acts);
     return check_launch("burgers_cnn_rollout");
 }
 
@@ -90,10 +101,9 @@ int launch(const Args& a, const float* w, float* corr, cudaStream_t st) {
 using namespace inc;
 using namespace inc::burgers;
 
-extern "C" int inc_burgers_cnn_rollout(const inc_burgers_desc* d, const float* weights, const float* u0,
-                                       const float* t_rows, double t0, int32_t steps, float* frames,
-                                       float* corrections, float* u_final, int32_t ckpt_every, float* ckpts,
-                                       void* stream) {
+static int cnn_rollout(const inc_burgers_desc* d, const float* weights, const float* u0, const float* t_rows,
+                       double t0, int32_t steps, float* frames, float* corrections, float* u_final,
+                       int32_t ckpt_every, float* ckpts, float* acts, void* stream) {
     Args a;
     int rc = fill_args(d, a);
     if (rc) return rc;
@@ -105,15 +115,36 @@ extern "C" int inc_burgers_cnn_rollout(const inc_burgers_desc* d, const float* w
         set_error("cnn_rollout: weights must be 16-byte aligned");
         return INC_E_INVALID;
     }
+    if (acts && ((reinterpret_cast<uintptr_t>(acts)) & 15u) != 0) {
+        set_error("cnn_rollout: acts must be 16-byte aligned");
+        return INC_E_INVALID;
+    }
     a.u = u0; a.s = nullptr; a.t_rows = t_rows; a.t0 = (float)t0; a.steps = steps; a.frames = frames; a.out = u_final;
     cudaStream_t st = as_stream(stream);
     switch (d->n) {
-        case 64: return cnn::launch<64>(a, weights, corrections, st);
-        case 128: return cnn::launch<128>(a, weights, corrections, st);
-        case 256: return cnn::launch<256>(a, weights, corrections, st);
-        case 512: return cnn::launch<512>(a, weights, corrections, st);
+        case 64: return cnn::launch<64>(a, weights, corrections, acts, st);
+        case 128: return cnn::launch<128>(a, weights, corrections, acts, st);
+        case 256: return cnn::launch<256>(a, weights, corrections, acts, st);
+        case 512: return cnn::launch<512>(a, weights, corrections, acts, st);
         default:
             set_error("cnn_rollout: n must be 64, 128, 256 or 512 (got %d)", d->n);
             return INC_E_UNSUPPORTED;
     }
+}
+
+extern "C" int inc_burgers_cnn_rollout(const inc_burgers_desc* d, const float* weights, const float* u0,
+                                       const float* t_rows, double t0, int32_t steps, float* frames,
+                                       float* corrections, float* u_final, int32_t ckpt_every, float* ckpts,
+                                       void* stream) {
+    return cnn_rollout(d, weights, u0, t_rows, t0, steps, frames, corrections, u_final, ckpt_every, ckpts, nullptr,
+                       stream);
+}
+
+extern "C" int inc_burgers_cnn_rollout_acts(const inc_burgers_desc* d, const float* weights, const float* u0,
+                                            const float* t_rows, double t0, int32_t steps, float* frames,
+                                            float* corrections, float* u_final, int32_t ckpt_every, float* ckpts,
+                                            float* acts, void* stream) {
+    if (!acts) { set_error("cnn_rollout_acts: acts must not be NULL"); return INC_E_INVALID; }
+    return cnn_rollout(d, weights, u0, t_rows, t0, steps, frames, corrections, u_final, ckpt_every, ckpts, acts,
+                       stream);
 }

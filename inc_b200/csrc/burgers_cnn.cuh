@@ -170,6 +170,34 @@ INC_DEV void conv_mid(const float* wt, const float* bias_p, float (*in)[row_len<
     store_tile<N, GELU_OUT>(out, acc, cg, L);
 }
 
+// The hidden layers' pre-activations of every step, recorded by the forward for
+// its backward: acts[row][step][layer: 0 = z2, 1 = z3][channel][cell].
+INC_DEV float* acts_tile(float* acts, int64_t row, int steps, int k, int layer, int ch, int n) {
+    return acts + ((((row * steps + k) * 2 + layer) * C + ch) * (int64_t)n);
+}
+
+// this thread's 4-channel x 8-cell tile to / from the record (two float4 a channel)
+INC_DEV void put_acts(float* acts, int64_t row, int steps, int k, int layer, const float (&acc)[4][8], int cg,
+                      int L, int n) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        float4* p = reinterpret_cast<float4*>(acts_tile(acts, row, steps, k, layer, 4 * cg + c, n) + 8 * L);
+        p[0] = make_float4(acc[c][0], acc[c][1], acc[c][2], acc[c][3]);
+        p[1] = make_float4(acc[c][4], acc[c][5], acc[c][6], acc[c][7]);
+    }
+}
+INC_DEV void get_acts(const float* __restrict__ acts, int64_t row, int steps, int k, int layer, float (&acc)[4][8],
+                      int cg, int L, int n) {
+#pragma unroll
+    for (int c = 0; c < 4; ++c) {
+        const float4* p = reinterpret_cast<const float4*>(
+            acts_tile(const_cast<float*>(acts), row, steps, k, layer, 4 * cg + c, n) + 8 * L);
+        const float4 v0 = __ldg(p), v1 = __ldg(p + 1);
+        acc[c][0] = v0.x; acc[c][1] = v0.y; acc[c][2] = v0.z; acc[c][3] = v0.w;
+        acc[c][4] = v1.x; acc[c][5] = v1.y; acc[c][6] = v1.z; acc[c][7] = v1.w;
+    }
+}
+
 // Layer 4: channels 4 cg .. 4 cg + 3 -> partial sums of the single output
 // channel, stored in row cg of `part` (the other buffer); no bias, no GELU.
 template <int N>

@@ -220,7 +220,7 @@ INC_DEV void wgrad_part(float (&acc)[KW], const float* dr, const float* ar, int 
 template <int N>
 __global__ void __launch_bounds__(BwdCfg<N>::T, 256 / N > 0 ? 2 : 1)
     k_cnn_rollout_bwd(Args a, const float* __restrict__ wts, const float* __restrict__ corr,
-                      const float* __restrict__ g_corr, float* __restrict__ work) {
+                      const float* __restrict__ g_corr, float* __restrict__ work, const float* __restrict__ acts) {
     using Cfg = BwdCfg<N>;
     constexpr int T = Cfg::T, R = Cfg::R, RL = Cfg::RL, NW = Cfg::NW, CO = Cfg::CO;
     constexpr int LPG = N / 8;  // lanes per channel group in the tile map
@@ -268,16 +268,23 @@ __global__ void __launch_bounds__(BwdCfg<N>::T, 256 / N > 0 ? 2 : 1)
             float acc[4][8];
             // ---- the network's activations at u_k
             put_cell<N>(S.u[rl], g, seg[j][rl][g]);
-            __syncthreads();
-            conv_first<N, true>(wts, S.u[rl], S.A[rl], cg, L);  // A = gelu(z1)
-            __syncthreads();
-            conv_mid<N, false>(wts + OFF_W2, wts + OFF_B2, S.A[rl], S.B[rl], cg, L);  // B = z2
-            __syncthreads();
-            gelu_buf<N>(&S.A[0][0][0], &S.B[0][0][0]);  // A = gelu(z2)
-            __syncthreads();
-            conv_mid_acc<N>(wts + OFF_W3, wts + OFF_B3, S.A[rl], acc, cg, L);
-            __syncthreads();
-            store_tile<N, false>(S.A[rl], acc, cg, L);  // A = z3
+            if (acts) {  // z2, z3 as the forward recorded them (this thread's tiles)
+                get_acts(acts, src, a.steps, k, 0, acc, cg, L, N);
+                store_tile<N, false>(S.B[rl], acc, cg, L);  // B = z2
+                get_acts(acts, src, a.steps, k, 1, acc, cg, L, N);
+                store_tile<N, false>(S.A[rl], acc, cg, L);  // A = z3
+            } else {
+                __syncthreads();
+                conv_first<N, true>(wts, S.u[rl], S.A[rl], cg, L);  // A = gelu(z1)
+                __syncthreads();
+                conv_mid<N, false>(wts + OFF_W2, wts + OFF_B2, S.A[rl], S.B[rl], cg, L);  // B = z2
+                __syncthreads();
+                gelu_buf<N>(&S.A[0][0][0], &S.B[0][0][0]);  // A = gelu(z2)
+                __syncthreads();
+                conv_mid_acc<N>(wts + OFF_W3, wts + OFF_B3, S.A[rl], acc, cg, L);
+                __syncthreads();
+                store_tile<N, false>(S.A[rl], acc, cg, L);  // A = z3
+            }
             // ---- the solver step's adjoint: u_bar through S and s_bar
             {
                 const int64_t at = ((int64_t)src * a.steps + k) * N + g;
@@ -469,8 +476,8 @@ int max_ckpt_every() {
 
 // the backward kernel; *slots = the number of work slots it fills
 template <int N>
-int launch_bwd(const Args& a, const float* w, const float* corr, const float* g_corr, float* work, cudaStream_t st,
-               int* slots) {
+int launch_bwd(const Args& a, const float* w, const float* corr, const float* g_corr, float* work,
+               const float* acts, cudaStream_t st, int* slots) {
     constexpr int R = BwdCfg<N>::R, T = BwdCfg<N>::T;
     if (a.ckpt_every > max_ckpt_every<N>()) {
         set_error("cnn_rollout_bwd: ckpt_every must be <= %d for n = %d (got %d)", max_ckpt_every<N>(), N,
@@ -480,7 +487,7 @@ int launch_bwd(const Args& a, const float* w, const float* corr, const float* g_
     const size_t smem = bwd_smem_bytes<N>(a.ckpt_every);
     cudaFuncSetAttribute(k_cnn_rollout_bwd<N>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     *slots = (a.rows + R - 1) / R;
-    k_cnn_rollout_bwd<N><<<*slots, T, smem, st>>>(a, w, corr, g_corr, work);
+    k_cnn_rollout_bwd<N><<<*slots, T, smem, st>>>(a, w, corr, g_corr, work, acts);
     return check_launch("burgers_cnn_rollout_bwd");
 }
 
@@ -491,11 +498,11 @@ int launch_bwd(const Args& a, const float* w, const float* corr, const float* g_
 using namespace inc;
 using namespace inc::burgers;
 
-extern "C" int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const float* weights, const float* ckpts,
-                                           const float* corrections, const float* t_rows, double t0, int32_t steps,
-                                           int32_t ckpt_every, const float* g_frames, const float* g_corrections,
-                                           const float* g_final, float* g_u0, float* g_weights, float* work,
-                                           void* stream) {
+static int cnn_rollout_bwd(const inc_burgers_desc* d, const float* weights, const float* ckpts,
+                           const float* corrections, const float* t_rows, double t0, int32_t steps,
+                           int32_t ckpt_every, const float* g_frames, const float* g_corrections,
+                           const float* g_final, float* g_u0, float* g_weights, float* work, const float* acts,
+                           void* stream) {
     Args a;
     int rc = fill_args(d, a);
     if (rc) return rc;
@@ -507,8 +514,8 @@ extern "C" int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const floa
         set_error("cnn_rollout_bwd: ckpt_every must be <= %d (got %d)", cnn::BKMAX, ckpt_every);
         return INC_E_INVALID;
     }
-    if ((reinterpret_cast<uintptr_t>(weights) & 15u) != 0) {
-        set_error("cnn_rollout_bwd: weights must be 16-byte aligned");
+    if ((reinterpret_cast<uintptr_t>(weights) & 15u) != 0 || (reinterpret_cast<uintptr_t>(acts) & 15u) != 0) {
+        set_error("cnn_rollout_bwd: weights and acts must be 16-byte aligned");
         return INC_E_INVALID;
     }
     a.t_rows = t_rows; a.t0 = (float)t0; a.steps = steps; a.ckpt_every = ckpt_every;
@@ -516,10 +523,10 @@ extern "C" int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const floa
     cudaStream_t st = as_stream(stream);
     int slots = 0;
     switch (d->n) {
-        case 64: rc = cnn::launch_bwd<64>(a, weights, corrections, g_corrections, work, st, &slots); break;
-        case 128: rc = cnn::launch_bwd<128>(a, weights, corrections, g_corrections, work, st, &slots); break;
-        case 256: rc = cnn::launch_bwd<256>(a, weights, corrections, g_corrections, work, st, &slots); break;
-        case 512: rc = cnn::launch_bwd<512>(a, weights, corrections, g_corrections, work, st, &slots); break;
+        case 64: rc = cnn::launch_bwd<64>(a, weights, corrections, g_corrections, work, acts, st, &slots); break;
+        case 128: rc = cnn::launch_bwd<128>(a, weights, corrections, g_corrections, work, acts, st, &slots); break;
+        case 256: rc = cnn::launch_bwd<256>(a, weights, corrections, g_corrections, work, acts, st, &slots); break;
+        case 512: rc = cnn::launch_bwd<512>(a, weights, corrections, g_corrections, work, acts, st, &slots); break;
         default:
             set_error("cnn_rollout_bwd: n must be 64, 128, 256 or 512 (got %d)", d->n);
             return INC_E_UNSUPPORTED;
@@ -527,4 +534,23 @@ extern "C" int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const floa
     if (rc) return rc;
     cnn::k_sum_rows<<<(cnn::W_FLOATS + 255) / 256, 256, 0, st>>>(work, g_weights, slots);
     return check_launch("burgers_cnn_rollout_bwd (sum)");
+}
+
+extern "C" int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const float* weights, const float* ckpts,
+                                           const float* corrections, const float* t_rows, double t0, int32_t steps,
+                                           int32_t ckpt_every, const float* g_frames, const float* g_corrections,
+                                           const float* g_final, float* g_u0, float* g_weights, float* work,
+                                           void* stream) {
+    return cnn_rollout_bwd(d, weights, ckpts, corrections, t_rows, t0, steps, ckpt_every, g_frames, g_corrections,
+                           g_final, g_u0, g_weights, work, nullptr, stream);
+}
+
+extern "C" int inc_burgers_cnn_rollout_bwd_acts(const inc_burgers_desc* d, const float* weights, const float* ckpts,
+                                                const float* corrections, const float* t_rows, double t0,
+                                                int32_t steps, int32_t ckpt_every, const float* g_frames,
+                                                const float* g_corrections, const float* g_final, float* g_u0,
+                                                float* g_weights, float* work, const float* acts, void* stream) {
+    if (!acts) { set_error("cnn_rollout_bwd_acts: acts must not be NULL"); return INC_E_INVALID; }
+    return cnn_rollout_bwd(d, weights, ckpts, corrections, t_rows, t0, steps, ckpt_every, g_frames, g_corrections,
+                           g_final, g_u0, g_weights, work, acts, stream);
 }

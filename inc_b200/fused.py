@@ -64,6 +64,9 @@ def pack_cnn_weights(model, device=None) -> torch.Tensor:
 
 CNN_TRAIN_N = CNN_N
 MAX_CKPT_EVERY = 32
+# Largest record of the hidden layers' pre-activations the training path keeps (bytes):
+# 2 x 32 x n floats per row and step, 537 MB for 256 rows x 256 cells x 32 steps.
+ACTS_BYTES_MAX = 4 << 30
 
 
 def max_ckpt_every(n: int) -> int:
@@ -109,14 +112,19 @@ class BurgersCNNRolloutFn(torch.autograd.Function):
         corr = torch.empty_like(frames)
         nseg = (steps + ckpt_every - 1) // ckpt_every
         ckpts = torch.empty(B, nseg, N, device=u0.device, dtype=torch.float32)
-        launch.cnn_rollout(w, u0, steps, frames, corr, None, ckpt_every, ckpts)
-        ctx.save_for_backward(ckpts, corr, w)
+        # the hidden layers' pre-activations of every step, kept for the backward when they
+        # fit ACTS_BYTES_MAX (else the backward recomputes them)
+        acts = None
+        if B * steps * 2 * 32 * N * 4 <= ACTS_BYTES_MAX:
+            acts = torch.empty(B, steps, 2, 32, N, device=u0.device, dtype=torch.float32)
+        launch.cnn_rollout(w, u0, steps, frames, corr, None, ckpt_every, ckpts, acts=acts)
+        ctx.save_for_backward(ckpts, corr, w, acts)
         ctx.launch, ctx.steps, ctx.ckpt_every, ctx.shape = launch, steps, ckpt_every, (B, N)
         return frames, corr
 
     @staticmethod
     def backward(ctx, g_frames, g_corr):
-        ckpts, corr, w = ctx.saved_tensors
+        ckpts, corr, w, acts = ctx.saved_tensors
         B, N = ctx.shape
         dev = ckpts.device
         g_u0 = torch.empty(B, N, device=dev, dtype=torch.float32)
@@ -124,7 +132,8 @@ class BurgersCNNRolloutFn(torch.autograd.Function):
         work = torch.empty(B, nat.INC_CNN_WEIGHT_FLOATS, device=dev, dtype=torch.float32)
         gf = None if g_frames is None else g_frames.contiguous()
         gc = None if g_corr is None else g_corr.contiguous()
-        ctx.launch.cnn_rollout_bwd(w, ckpts, corr, ctx.steps, ctx.ckpt_every, gf, gc, None, g_u0, g_w, work)
+        ctx.launch.cnn_rollout_bwd(w, ckpts, corr, ctx.steps, ctx.ckpt_every, gf, gc, None, g_u0, g_w, work,
+                                   acts=acts)
         return (g_u0, None, None, None) + unpack_cnn_grads(g_w)
 
 

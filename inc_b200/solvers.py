@@ -151,21 +151,31 @@ class _BurgersLaunch:
                                                nat.ptr(ckpts), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_rollout")
 
-    def cnn_rollout(self, weights, u0, steps, frames, corrections, u_final, ckpt_every=0, ckpts=None):
+    def cnn_rollout(self, weights, u0, steps, frames, corrections, u_final, ckpt_every=0, ckpts=None, acts=None):
+        """The fused CNN-corrected rollout; with ``acts`` ([rows, steps, 2, 32, n] float32) it
+        also records the hidden layers' pre-activations for cnn_rollout_bwd."""
+        lib = nat.lib()
+        args = (C.byref(self.desc), weights.data_ptr(), u0.data_ptr(), nat.ptr(self.t_rows), self.t0, steps,
+                nat.ptr(frames), nat.ptr(corrections), nat.ptr(u_final), int(ckpt_every), nat.ptr(ckpts))
         with nat.on_device(self.dev):
-            rc = nat.lib().inc_burgers_cnn_rollout(C.byref(self.desc), weights.data_ptr(), u0.data_ptr(),
-                                                   nat.ptr(self.t_rows), self.t0, steps, nat.ptr(frames),
-                                                   nat.ptr(corrections), nat.ptr(u_final), int(ckpt_every),
-                                                   nat.ptr(ckpts), nat.stream_of(self.dev))
+            if acts is None:
+                rc = lib.inc_burgers_cnn_rollout(*args, nat.stream_of(self.dev))
+            else:
+                rc = lib.inc_burgers_cnn_rollout_acts(*args, acts.data_ptr(), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_cnn_rollout")
 
     def cnn_rollout_bwd(self, weights, ckpts, corrections, steps, ckpt_every, g_frames, g_corrections, g_final,
-                        g_u0, g_weights, work):
-        with nat.on_device(self.dev):
-            rc = nat.lib().inc_burgers_cnn_rollout_bwd(
-                C.byref(self.desc), weights.data_ptr(), ckpts.data_ptr(), corrections.data_ptr(),
+                        g_u0, g_weights, work, acts=None):
+        """Its backward; ``acts`` (the forward's record) replaces recomputing z2 and z3."""
+        lib = nat.lib()
+        args = (C.byref(self.desc), weights.data_ptr(), ckpts.data_ptr(), corrections.data_ptr(),
                 nat.ptr(self.t_rows), self.t0, steps, ckpt_every, nat.ptr(g_frames), nat.ptr(g_corrections),
-                nat.ptr(g_final), g_u0.data_ptr(), g_weights.data_ptr(), work.data_ptr(), nat.stream_of(self.dev))
+                nat.ptr(g_final), g_u0.data_ptr(), g_weights.data_ptr(), work.data_ptr())
+        with nat.on_device(self.dev):
+            if acts is None:
+                rc = lib.inc_burgers_cnn_rollout_bwd(*args, nat.stream_of(self.dev))
+            else:
+                rc = lib.inc_burgers_cnn_rollout_bwd_acts(*args, acts.data_ptr(), nat.stream_of(self.dev))
         nat.check(rc, "inc_burgers_cnn_rollout_bwd")
 
     def rollout_bwd(self, ckpts, s, steps, ckpt_every, g_frames, g_final, g_u0, g_s):

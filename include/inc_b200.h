@@ -259,6 +259,24 @@ int inc_burgers_cnn_rollout_bwd(const inc_burgers_desc* d, const float* weights,
                                 float* g_u0, float* g_weights, float* work,
                                 void* stream);
 
+/* The same pair with the hidden layers' pre-activations recorded: the forward
+ * also writes z2 and z3 (the two 32-channel convolutions before their GELU) of
+ * every step to acts [rows][steps][2][32][n] floats (16-byte aligned), and the
+ * backward reads them there instead of recomputing them, a third of its
+ * convolution work.  acts must not be NULL (INC_E_INVALID).                    */
+int inc_burgers_cnn_rollout_acts(const inc_burgers_desc* d, const float* weights,
+                                 const float* u0, const float* t_rows, double t0,
+                                 int32_t steps, float* frames, float* corrections,
+                                 float* u_final, int32_t ckpt_every, float* ckpts,
+                                 float* acts, void* stream);
+int inc_burgers_cnn_rollout_bwd_acts(const inc_burgers_desc* d, const float* weights,
+                                     const float* ckpts, const float* corrections,
+                                     const float* t_rows, double t0, int32_t steps,
+                                     int32_t ckpt_every, const float* g_frames,
+                                     const float* g_corrections, const float* g_final,
+                                     float* g_u0, float* g_weights, float* work,
+                                     const float* acts, void* stream);
+
 /* ---- Kuramoto-Sivashinsky --------------------------------------------- */
 /* Bytes of device memory a plan needs.                                       */
 int64_t inc_ks_plan_size(int32_t rows, int32_t n);

@@ -206,6 +206,36 @@ def test_fused_training_gradients_vs_per_step_loop(cuda, N, B, scheme, K, eq):
     assert max(np.abs(b).max() for b in pr) > 0
 
 
+@pytest.mark.parametrize("N,B", [(64, 9), (256, 5), (512, 2)])
+def test_fused_training_recorded_activations_match_recompute(cuda, monkeypatch, N, B):
+    """The training path keeps the hidden layers' pre-activations from the forward
+    (inc_burgers_cnn_rollout_acts / _bwd_acts) when they fit, else the backward
+    recomputes them from the replayed states: the two agree (the record holds the
+    forward's own states, the replay its recomputation, equal to FP32 rounding)."""
+    from inc_b200 import fused
+    from inc_b200.solvers import BurgersSolverTorch
+    steps = 11
+    p = _params(N, B=B, seed=13)
+    u0_np = _u0(B, N, seed=14)
+    gen = torch.Generator().manual_seed(5)
+    wf = torch.randn(B, steps, N, generator=gen).to(cuda)
+    wc = torch.randn(B, steps, N, generator=gen).to(cuda)
+
+    def run(acts_max):
+        monkeypatch.setattr(fused, "ACTS_BYTES_MAX", acts_max)
+        net = _net(3).float().to(cuda)
+        solver = BurgersSolverTorch(_sim_params(p, B, "ssprk3", cuda))
+        u0 = torch.tensor(u0_np, dtype=torch.float32, device=cuda, requires_grad=True)
+        f, c = fused.burgers_cnn_rollout(net, solver, u0, steps, ckpt_every=4)
+        ((f * wf).sum() + (c * wc).sum()).backward()
+        return [u0.grad.cpu().numpy()] + [q.grad.cpu().numpy() for q in net.parameters()]
+
+    rec, recomp = run(4 << 30), run(0)
+    for a, b in zip(rec, recomp):
+        assert np.isfinite(a).all()
+        assert rel_l2(a, b) < 1e-5
+
+
 def test_fused_training_frames_only_loss_and_graph_capture(cuda):
     """A loss on the frames alone (the corrections' adjoint is zero) and the whole training
     step (fused forward + backward + optimizer) replayed from a CUDA graph."""
