@@ -1092,7 +1092,8 @@ def reference_arm(args, rank, world):
             "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": 1e3 * sum(walls) / len(walls), "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-            "config": {"workload": cfg["name"]},
+            "config": {"workload": cfg["name"], "batch": cfg["B"], "n": cfg["N"], "steps_per_rollout": cfg["steps"],
+                       "scheme": cfg["scheme"]},
             "cpu_baseline": {"value": v, "unit": "cell-steps/s", "cores": cpu.cores, "kind": "port",
                              "sample": sample},
             "e2e": {"value": v, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
