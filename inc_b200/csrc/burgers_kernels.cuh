@@ -1351,25 +1351,30 @@ __global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(TPR, 1) k_rollout_bw
 // m[0..5], pa (VjpPre) and the stage input u.
 constexpr int kPreVals = 8;
 
-// The same backward on a cluster of three CTAs per row (2 TPR threads each), a
+// The same backward on a cluster of three CTAs per row (3 TPR threads each), a
 // pipeline over segments: CTA 0 replays segment s - 2 into CTA 1's shared memory
-// (stage inputs, alphas, argmaxes); CTA 1's two thread groups form segment s - 1's
-// per-cell stage quantities (vjp_pre, one stage input per group at a time) into
-// CTA 2's shared memory; CTA 2 differentiates segment s, each stage only scaling
-// and scattering them.  One cluster barrier per pipeline step orders the remote
-// stores before their readers and frees the double buffers' halves.
+// (every step's stage inputs); CTA 1's three thread groups take one stage input
+// each at a time, find its alpha and first argmax and form its per-cell stage
+// quantities (vjp_pre) into CTA 2's shared memory (segment s - 1); CTA 2
+// differentiates segment s, each stage only scaling and scattering them.  One
+// cluster barrier per pipeline step orders the remote stores before their
+// readers and frees the double buffers' halves.
+constexpr int kPreGroups = 3;
+
 template <int TPR>
-__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(2 * TPR, 1) k_rollout_bwd_cl3(Args a) {
+__global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(kPreGroups * TPR, 1) k_rollout_bwd_cl3(Args a) {
     namespace cg = cooperative_groups;
+    constexpr int NW = TPR / 32;
     __shared__ WideSmem<1, TPR> shr;   // CTA 0
     __shared__ WideAdjSmem<TPR> sha;   // CTA 2
-    extern __shared__ float dsm[];     // CTA 1: seg [2][3K][TPR], alpha/argmax [2][3K][2];
-                                       // CTA 2: pre [2][3K][kPreVals][TPR], argmax [2][3K]
+    __shared__ float rmax[kPreGroups][2][NW];  // CTA 1: each group's per-warp max |u| (double-buffered)
+    __shared__ int rarg[kPreGroups][2][NW];    //        and its first cell
+    extern __shared__ float dsm[];     // CTA 1: seg [2][3K][TPR];  CTA 2: pre [2][3K][kPreVals][TPR], argmax [2][3K]
     cg::cluster_group cl = cg::this_cluster();
     const int role = (int)cl.block_rank();  // 0 replay, 1 precompute, 2 adjoint
     const int row = blockIdx.x / 3;
     const int t = threadIdx.x;
-    const int g = t % TPR;
+    const int g = t % TPR, q = t / TPR;
     const bool lead = t < TPR;  // CTAs 0 and 2 run one group of TPR threads
     Ctx<1> cx;
     make_ctx<1, TPR>(a, row, g, true, cx);
@@ -1380,8 +1385,7 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(2 * TPR, 1) k_rollou
     const float dt = cx.dt;
     const int64_t base = (int64_t)row * TPR + g;
     const int half_seg = 3 * K * TPR, half_pre = 3 * K * kPreVals * TPR;
-    float* seg1 = role == 0 ? cl.map_shared_rank(dsm, 1) : dsm;   // CTA 1's buffers
-    float* alph1 = seg1 + 2 * half_seg;
+    float* seg1 = role == 0 ? cl.map_shared_rank(dsm, 1) : dsm;   // CTA 1's buffer
     float* pre2 = role == 1 ? cl.map_shared_rank(dsm, 2) : dsm;   // CTA 2's buffers
     int* am2 = reinterpret_cast<int*>(pre2 + 2 * half_pre);
     const float* ckr = a.ckpts + (int64_t)row * nseg * TPR + g;
@@ -1389,34 +1393,59 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(2 * TPR, 1) k_rollou
     auto seg_len = [&](int sidx) { return min(K, a.steps - sidx * K); };
     auto replay = [&](int sidx) {  // CTA 0, threads [0, TPR)
         float* seg = seg1 + (sidx & 1) * half_seg;
-        float* al = alph1 + (sidx & 1) * 6 * K;
         const int k0 = sidx * K, len = seg_len(sidx);
         float x[1] = {__ldg(ckr + (int64_t)sidx * TPR)}, r[1];
         for (int j = 0; j < len; ++j) {
             const float tt = cx.t + (k0 + j) * dt;
             const float u0 = x[0];
             seg[3 * j * TPR + g] = u0;
+            const int run = j + 1 < len ? stages : stages - 1;
             float d = 0.f;
-            for (int k = 0; k < stages; ++k) {
-                full_rhs_wide<1, TPR, 1, true>(a, cx, x, r, tt + rk3_c(k) * dt, shr, parity, g, al + 2 * (3 * j + k));
+            for (int k = 0; k < run; ++k) {
+                full_rhs_wide<1, TPR, 1>(a, cx, x, r, tt + rk3_c(k) * dt, shr, parity, g);
                 d = rk3_b(k) * fmaf(dt, r[0], d);
                 x[0] = u0 + d;
                 if (k + 1 < stages) seg[(3 * j + 1 + k) * TPR + g] = x[0];
             }
         }
     };
-    auto precompute = [&](int sidx) {  // CTA 1, group t / TPR takes every other stage input
+    int rpar = 0;  // CTA 1: which half of the group's max buffers this stage input uses
+    auto precompute = [&](int sidx) {  // CTA 1, group q takes every kPreGroups-th stage input
         const float* seg = dsm + (sidx & 1) * half_seg;
-        const float* al = dsm + 2 * half_seg + (sidx & 1) * 6 * K;
         float* out = pre2 + (sidx & 1) * half_pre;
         int* amo = am2 + (sidx & 1) * 3 * K;
         const int len = seg_len(sidx);
         for (int j = 0; j < len; ++j)
             for (int k = 0; k < stages; ++k) {
+                if ((j * stages + k) % kPreGroups != q) continue;
                 const int i = 3 * j + k;
-                if ((j * stages + k) % 2 != t / TPR) continue;
+                const float* rowp = seg + i * TPR;
+                // alpha = max |u| and its first cell, as the forward's row max (a NaN cell is passed over)
+                float al[2] = {0.f, 0.f};
+                if (a.conv == INC_CONV_WENO) {
+                    const float au = fabsf(rowp[g]);
+                    float m = au > 0.f ? au : 0.f;
+                    int mi = g;
+                    group_argmax_nonneg<32>(m, mi);
+                    if ((g & 31) == 0) {
+                        rmax[q][rpar][g >> 5] = m;
+                        rarg[q][rpar][g >> 5] = mi;
+                    }
+                    asm volatile("bar.sync %0, %1;\n" ::"r"(3 + q), "n"(TPR) : "memory");
+                    float best = rmax[q][rpar][0];
+                    int am = rarg[q][rpar][0];
+#pragma unroll
+                    for (int w = 1; w < NW; ++w)
+                        if (rmax[q][rpar][w] > best) {
+                            best = rmax[q][rpar][w];
+                            am = rarg[q][rpar][w];
+                        }
+                    al[0] = best;
+                    al[1] = __int_as_float(am);
+                    rpar ^= 1;
+                }
                 VjpPre p;
-                vjp_pre<TPR>(a, seg + i * TPR, al + 2 * i, g, p);
+                vjp_pre<TPR>(a, rowp, al, g, p);
                 float* o = out + i * kPreVals * TPR + g;
 #pragma unroll
                 for (int e = 0; e < 6; ++e) o[e * TPR] = p.m[e];
@@ -1444,14 +1473,14 @@ __global__ void __cluster_dims__(3, 1, 1) __launch_bounds__(2 * TPR, 1) k_rollou
             float acc = 0.f;
             for (int st = stages - 1; st >= 0; --st) {  // as stages_bwd_wide
                 const int i = 3 * j + st;
-                const float* q = pre + i * kPreVals * TPR;
+                const float* qv = pre + i * kPreVals * TPR;
                 VjpPre p;
 #pragma unroll
-                for (int e = 0; e < 6; ++e) p.m[e] = q[e * TPR + g];
-                p.pa = q[6 * TPR + g];
-                p.u = q[7 * TPR + g];
-                p.u_l = q[7 * TPR + ((g + TPR - 1) & (TPR - 1))];
-                p.u_r = q[7 * TPR + ((g + 1) & (TPR - 1))];
+                for (int e = 0; e < 6; ++e) p.m[e] = qv[e * TPR + g];
+                p.pa = qv[6 * TPR + g];
+                p.u = qv[7 * TPR + g];
+                p.u_l = qv[7 * TPR + ((g + TPR - 1) & (TPR - 1))];
+                p.u_r = qv[7 * TPR + ((g + 1) & (TPR - 1))];
                 p.am = am[i];
                 float rv;
                 rhs_vjp_wide_pre<TPR, 2>(a, cx, p, gu, rv, sha, g, [] {});
@@ -1575,13 +1604,13 @@ int launch_bwd_wide_impl(Kind kind, const Args& a, cudaStream_t st) {
     // few rows: three CTAs per row (replay, the stages' precomputation and the
     // adjoint each on an SM of their own), or two (replay, adjoint)
     if constexpr (TPR <= 128) {
-        const size_t seg1 = (size_t)(2 * 3 * b.ckpt_every * TPR + 2 * 3 * b.ckpt_every * 2) * sizeof(float);
+        const size_t seg1 = (size_t)2 * 3 * b.ckpt_every * TPR * sizeof(float);
         const size_t pre2 = (size_t)(2 * 3 * b.ckpt_every * kPreVals * TPR + 2 * 3 * b.ckpt_every) * sizeof(float);
         const size_t dyn = seg1 > pre2 ? seg1 : pre2;
         if (3 * b.rows <= sm_count() && dyn + bwd_wide2_static_smem<TPR>() <= 227 * 1024) {
             if (dyn + bwd_wide2_static_smem<TPR>() > 48 * 1024)
                 cudaFuncSetAttribute(k_rollout_bwd_cl3<TPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn);
-            k_rollout_bwd_cl3<TPR><<<3 * b.rows, 2 * TPR, dyn, st>>>(b);
+            k_rollout_bwd_cl3<TPR><<<3 * b.rows, kPreGroups * TPR, dyn, st>>>(b);
             return check_launch("burgers_bwd_cluster3");
         }
     }
