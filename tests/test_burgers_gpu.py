@@ -287,6 +287,34 @@ def test_wide_adjoint_forms_by_batch(cuda, n, B):
         assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 2e-5
 
 
+@pytest.mark.parametrize("B,n,steps,K,scheme", [
+    (3, 64, 1, 1, "ssprk3"), (3, 64, 5, 8, "ssprk3"), (7, 128, 9, 1, "euler"), (7, 128, 17, 16, "ssprk3"),
+    (30, 256, 6, 4, "euler"), (60, 128, 13, 5, "ssprk3"), (100, 64, 7, 3, "ssprk3")])
+def test_wide_adjoint_segment_corner_cases(cuda, B, n, steps, K, scheme):
+    """The small-batch adjoint's forms at segment corner cases (a single step, one
+    segment shorter than ckpt_every, ckpt_every = 1, a partial last segment, Euler)
+    against the warp-layout adjoint: gradients w.r.t. u0 and s of a frame loss."""
+    from inc_b200.rollout import burgers_rollout
+    from inc_b200.solvers import BurgersSolverTorch
+    L = 2 * math.pi
+    g = torch.Generator().manual_seed(B * 1000 + n + steps)
+    u0 = torch.tensor(_rand_u0(B, n, B + steps), dtype=torch.float32, device=cuda)
+    s0 = 0.05 * (torch.rand(B, n, generator=g) - 0.5).to(cuda)
+    wf = torch.randn(B, steps, n, generator=g).to(cuda)
+    out = []
+    for cpt in (1, _WARP_CPT[n]):
+        sp = SimpleNamespace(resolution=n, dt=0.2 / n, x=None, adaptive_CFL=None, L=L, nu=0.01, device=cuda,
+                             convection_term="WENO", equation_type="viscosity", batch_size=B,
+                             time_scheme=scheme, cells_per_thread=cpt)
+        u = u0.clone().requires_grad_(True)
+        s = s0.clone().requires_grad_(True)
+        fr = burgers_rollout(BurgersSolverTorch(sp), u, steps, s=s, ckpt_every=K)
+        out.append(torch.autograd.grad((fr * wf).sum(), (u, s)))
+    for a, b in zip(*out):
+        assert torch.isfinite(a).all()
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 2e-5
+
+
 def test_fd_check_fp64_oracle(cuda):
     """GPU adjoint vs FP64 central differences (h=1e-6) of the oracle, 3 SSP-RK3 steps."""
     from inc_b200.solvers import BurgersSolverTorch

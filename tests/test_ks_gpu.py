@@ -216,6 +216,35 @@ def test_rollout_backward_scratch_matches_rebuild(cuda, N, tpp, scheme):
         plan.rollout_bwd(ck, s, steps, K, gf, gfin, gu, gs, work=small)
 
 
+@pytest.mark.parametrize("N,B,steps,K", [(256, 7, 1, 4), (256, 5, 3, 4), (256, 9, 11, 4), (256, 3, 9, 1),
+                                          (128, 11, 13, 8)])
+def test_rollout_backward_two_warp_form(cuda, N, B, steps, K):
+    """The checkpointed backward with its replay on a second warp (32 lanes, ETRK2, one
+    domain size per pair) against the one-warp rebuilding form: a single step, one
+    segment shorter than ckpt_every, ckpt_every = 1, partial last segments, a lone row."""
+    dt = 0.2
+    Ls = [56.0] * B
+    solver = _solver(N, dt, "ETRK2", Ls, tpp=32)
+    u0 = torch.tensor(_u0(B, N, Ls, 9), dtype=torch.float32, device=cuda)
+    g = torch.Generator(device=cuda).manual_seed(N + B + steps)
+    s = 0.01 * torch.randn(B, N, device=cuda, generator=g)
+    ds = torch.tensor(Ls, device=cuda)
+    plan = solver.plan_for(u0, ds)
+    frames = torch.empty(B, steps, N, device=cuda)
+    ck = torch.empty(B, (steps + K - 1) // K, N, device=cuda)
+    plan.rollout(u0, s, steps, frames, None, K, ck)
+    gf = torch.randn(B, steps, N, device=cuda, generator=g)
+    gfin = torch.randn(B, N, device=cuda, generator=g)
+    out = []
+    for work in (None, False):
+        gu, gs = torch.empty_like(u0), torch.empty_like(u0)
+        plan.rollout_bwd(ck, s, steps, K, gf, gfin, gu, gs, work=work)
+        out.append((gu, gs))
+    for a, b in zip(*out):
+        assert torch.isfinite(a).all()
+        assert rel_l2(a.cpu().numpy(), b.cpu().numpy()) < 1e-5
+
+
 @pytest.mark.parametrize("B,tpp", [(1031, 16), (4101, 32)])
 def test_rollout_backward_scratch_many_groups(cuda, B, tpp):
     """The scratch backward on grids of many blocks with several row pairs per block
